@@ -1,0 +1,377 @@
+"""Search benchmark: plain BM25 Search on a resident 10M-doc index, bit-exact top-K.
+
+Workload (one "step" = one Search of one query batch): seeded synthetic corpus of
+10,000,000 documents, vocabulary 1,000,000 with Zipf(1.1) token ranks, lognormal
+lengths with mean 60 (sigma 0.5), k1 1.5, b 0.75, eager FP32 posting scores in
+CSC resident in HBM; batches of 8 queries x 3 distinct terms drawn by document
+frequency, K = 10; two batches A/B alternate as in the reference's benchmark.
+
+  value   queries/s of the device-resident Search (inputs already in HBM), timed
+          per step with CUDA events on the launching stream, L2 flushed between
+          steps (a 256 MiB write), summed over the K timed steps; max over ranks.
+  e2e     queries/s of the public C-ABI call bm25_search with host buffers
+          (pack, graph replay with H2D + kernel + D2H, synchronise, validate),
+          host wall-clock per call, L2 flushed between calls.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--impl reference times the reference's own CPU search (oracle/_ref, compiled from
+the reference's sources; the oracle's C restatement where that was not built) on
+the same corpus and batches with every host thread.
+"""
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = 'Search QPS + p50/p95 ms, 10M docs K10: plain vs learned-pruned, bit-exact top-K'
+UNIT = 'queries/s'
+WORKLOAD = 'synthetic_10m'
+Q, TERMS, K = 8, 3, 10
+SEED_A, SEED_B = 20261014, 20261015
+FALLBACK_HBM_GBS = 6650.0
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def percentile(values, p):
+    v = sorted(values)
+    return v[min(len(v) - 1, max(0, int(round(p / 100.0 * (len(v) - 1)))))]
+
+
+def hbm_peak():
+    path = ROOT / 'MEASURED_PEAKS.json'
+    try:
+        peaks = json.loads(path.read_text())
+        return float(peaks['hbm_gbs']), 'measured'
+    except Exception:
+        return FALLBACK_HBM_GBS, 'fallback'
+
+
+def algorithmic_bytes(df, vocab, offsets, words, k):
+    """Posting bytes the Search must read: per in-vocabulary query word df*8 (int32 id + f32 score)
+    + 16 B of indptr, plus the Q*K*8 B result."""
+    total = 0
+    for w in words:
+        if 0 <= w < vocab:
+            total += int(df[w]) * 8 + 16
+    return total + (offsets.size - 1) * k * 8
+
+
+def traffic_from_profile(name='tile_search_kernel_synthetic_10m.txt'):
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    path = ROOT / 'profiles' / name
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        if line.startswith('traffic_bytes_per_launch:'):
+            try:
+                return float(line.split(':', 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        import tempfile
+        self.path = tempfile.NamedTemporaryFile(prefix='clocks_', suffix='.csv', delete=False).name
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', f'--id={self.device}', f'--query-gpu={self.FIELDS}', '--format=csv,noheader,nounits',
+                 '-lms', '200'], stdout=open(self.path, 'w'), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in line.split(',')]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == 'active'})
+        return {'sm_mhz': statistics.median(sm) if sm else None,
+                'sm_max_mhz': float(rows[0][2]) if rows[0][2].replace('.', '').isdigit() else None,
+                'reasons': reasons, 'samples': len(rows)}
+
+
+def setup_dist(gpus):
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world != gpus:
+        log(f'warning: --gpus {gpus} but WORLD_SIZE {world}')
+    return rank, world, local
+
+
+def build_corpus(pkg):
+    spec = pkg.CONFIG_SHAPES[WORKLOAD]
+    t = time.perf_counter()
+    index = pkg.synthetic_index(spec)
+    log(f'corpus: N={index.num_docs} V={index.vocab} M={index.postings} in {time.perf_counter() - t:.1f}s')
+    return spec, index
+
+
+def batches(pkg, index, rank):
+    a = pkg.synthetic_queries(index.offsets, Q, TERMS, TERMS, SEED_A + 1000 * rank)
+    b = pkg.synthetic_queries(index.offsets, Q, TERMS, TERMS, SEED_B + 1000 * rank)
+    return [a, b]
+
+
+def cpu_search_leg(index, sets, k, budget_s, max_steps, warmup=1):
+    """The reference's CPU search (oracle/_ref) or the oracle's restatement, all host threads."""
+    from oracle import oracle
+    threads = os.cpu_count() or 1
+    if oracle.reference_available():
+        session = oracle.ReferenceCpuSession(index, k, threads, shards=threads, query_capacity=Q,
+                                             word_capacity=Q * TERMS)
+
+        def run(i):
+            return session.search(*sets[i % 2])[:2]
+
+        kind, cores = 'reference', session.threads
+        note = ('reference bm25cpu::CpuSearchSession (cpu_index_search.h) compiled from its sources; '
+                'its contribution uses the hard-coded k1=1.2 (2.2F) on the same postings, same work')
+    else:
+        data = oracle.contributions(index, 1.5)
+
+        def run(i):
+            return oracle.search(index.offsets, index.docs, data, index.num_docs, *sets[i % 2], k, threads=threads)
+
+        kind, cores = 'port', min(threads, Q)
+        note = 'oracle C restatement (term-order scatter + bounded heap), OpenMP over queries'
+    for i in range(warmup):
+        run(i)
+    times = []
+    t_start = time.perf_counter()
+    i = 0
+    while i < max_steps and (time.perf_counter() - t_start) < budget_s:
+        t0 = time.perf_counter()
+        run(i)
+        times.append(time.perf_counter() - t0)
+        i += 1
+    total = sum(times)
+    return {'value': Q * len(times) / total, 'unit': UNIT, 'cores': cores, 'kind': kind,
+            'sample': f'{len(times)} full Searches of {Q} queries x {TERMS} terms (A/B alternating) on the same '
+                      f'10M-doc corpus; {note}',
+            'p50_ms': percentile(times, 50) * 1e3, 'p95_ms': percentile(times, 95) * 1e3}
+
+
+def run_reference(args):
+    rank, world, _ = setup_dist(args.gpus)
+    if rank != 0:
+        return 0
+    pkg = importlib.import_module('bm25-npu_b200')
+    spec, index = build_corpus(pkg)
+    sets = batches(pkg, index, 0)
+    res = cpu_search_leg(index, sets, K, budget_s=1e9, max_steps=args.steps, warmup=args.warmup)
+    line = {
+        'impl': 'reference', 'metric': METRIC, 'value': res['value'], 'unit': UNIT, 'n_gpus': args.gpus,
+        'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': Q * 1e3 / res['value'],
+        'p50_ms': res['p50_ms'], 'p95_ms': res['p95_ms'], 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+        'config': {'workload': WORKLOAD, 'docs': spec.docs, 'vocab': spec.vocab, 'zipf_s': spec.zipf_s,
+                   'len_mean': spec.len_mean, 'k1': spec.k1, 'b': spec.b, 'queries': Q, 'terms': TERMS, 'k': K},
+        'cpu_baseline': {k2: res[k2] for k2 in ('value', 'unit', 'cores', 'kind', 'sample')},
+        'e2e': {'value': res['value'], 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=60)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--tile-docs', type=int, default=0)
+    ap.add_argument('--fan-in', type=int, default=0)
+    args = ap.parse_args()
+    if args.impl == 'reference':
+        return run_reference(args)
+    if args.warmup < 3:
+        args.warmup = 3
+
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = setup_dist(args.gpus)
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group('nccl', timeout=timedelta(seconds=600), device_id=torch.device('cuda', local))
+    pkg = importlib.import_module('bm25-npu_b200')
+    spec, index = build_corpus(pkg)
+    df = index.df()
+    sets = batches(pkg, index, rank)
+    t = time.perf_counter()
+    session = pkg.Bm25Session.from_lazy(index.offsets, index.docs, index.tf, index.norm, index.idf, k1=spec.k1,
+                                        query_capacity=Q, word_capacity=Q * TERMS, max_k=K, device_id=local,
+                                        tile_docs=args.tile_docs, merge_fan_in=args.fan_in)
+    info = session.info()
+    log(f'engine ready in {time.perf_counter() - t:.1f}s: {info}')
+
+    # Parity of both batches against the CPU oracle (outside every timer).
+    parity = None
+    if rank == 0:
+        from oracle import oracle
+        data = oracle.contributions(index, spec.k1)
+        ok = True
+        for qs in sets:
+            rs, ri = oracle.search(index.offsets, index.docs, data, index.num_docs, *qs, K)
+            gs, gi = session.search(qs, K)
+            ok &= bool(np.array_equal(gi, ri) and np.array_equal(gs.view(np.uint32), rs.view(np.uint32)))
+        parity = {'batches': len(sets), 'bit_exact': ok, 'against': 'oracle (C restatement, eager FP32)'}
+        del data
+        log(f'parity vs oracle: {parity}')
+
+    stream = torch.cuda.Stream()
+    dev_sets = [(torch.from_numpy(o).cuda(), torch.from_numpy(w).cuda()) for o, w in sets]
+    d_scores = torch.empty((Q, K), dtype=torch.float32, device='cuda')
+    d_ids = torch.empty((Q, K), dtype=torch.int32, device='cuda')
+    flush = torch.empty(64 << 20, dtype=torch.float32, device='cuda')  # 256 MiB > 126 MB L2
+    bytes_per = [algorithmic_bytes(df, index.vocab, o, w, K) for o, w in sets]
+
+    def device_step(i):
+        o, w = dev_sets[i % 2]
+        session.search_device(o.data_ptr(), w.data_ptr(), Q, K, d_scores.data_ptr(), d_ids.data_ptr(),
+                              stream.cuda_stream)
+
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            device_step(i)
+        stream.synchronize()
+        if session.device_status() != 0:
+            raise RuntimeError('device status set during warm-up')
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        clocks = Clocks(local)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clocks.start()
+        for i in range(args.steps):
+            flush.zero_()
+            starts[i].record(stream)
+            device_step(i)
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+        clock_info = clocks.stop()
+    if session.device_status() != 0:
+        raise RuntimeError('device status set during the timed region')
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    if world > 1:
+        tt = torch.tensor([total_ms], device='cuda', dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    value = world * Q * args.steps / (total_ms / 1e3)
+
+    # End to end through the C ABI with host buffers (pinned arenas, H2D/D2H inside the call).
+    host_ms = []
+    out = (np.empty((Q, K), np.float32), np.empty((Q, K), np.int32))
+    for i in range(args.warmup):
+        session.search(sets[i % 2], K, out=out)
+    if world > 1:
+        dist.barrier()
+    for i in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        session.search(sets[i % 2], K, out=out)
+        host_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_total = sum(host_ms)
+    if world > 1:
+        tt = torch.tensor([e2e_total], device='cuda', dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_total = float(tt.item())
+    e2e_value = world * Q * args.steps / (e2e_total / 1e3)
+    word_offset = -(-((Q + 1) * 8) // 32) * 32
+    h2d = -(-(word_offset + Q * TERMS * 4) // 32) * 32
+    id_off = -(-(Q * K * 4) // 32) * 32
+    d2h = -(-(id_off + Q * K * 4) // 32) * 32 + 32
+
+    # Roofline of the fused kernel: algorithmic bytes / event-timed duration, step by step.
+    bytes_avg = sum(bytes_per[i % 2] for i in range(args.steps)) / args.steps
+    achieved = sum(bytes_per[i % 2] for i in range(args.steps)) / (sum(step_ms) / 1e3) / 1e9
+    peak, peak_kind = hbm_peak()
+    traffic = traffic_from_profile()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        res = cpu_search_leg(index, sets, K, budget_s=20.0, max_steps=40)
+        cpu = {k2: res[k2] for k2 in ('value', 'unit', 'cores', 'kind', 'sample')}
+
+    if rank == 0:
+        line = {
+            'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': total_ms / args.steps,
+            'p50_ms': percentile(step_ms, 50), 'p95_ms': percentile(step_ms, 95),
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+            'config': {'workload': WORKLOAD, 'docs': spec.docs, 'vocab': spec.vocab, 'zipf_s': spec.zipf_s,
+                       'len_mean': spec.len_mean, 'len_sigma': spec.len_sigma, 'k1': spec.k1, 'b': spec.b,
+                       'postings': index.postings, 'queries': Q, 'terms': TERMS, 'k': K,
+                       'batches': 'A/B alternating, terms drawn by df', 'l2': 'flushed between steps (256 MiB write)',
+                       'tile_docs': info['tile_docs'], 'tiles': info['tiles'], 'merge_fan_in': info['merge_fan_in'],
+                       'merge_levels': info['merge_levels'], 'parallelism': f'replicas x{world} (queries sharded)'},
+            'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
+                    'p50_ms': percentile(host_ms, 50), 'p95_ms': percentile(host_ms, 95),
+                    'path': 'bm25_search (C ABI, host buffers): pack + CUDA graph (H2D, kernel, D2H) + validate'},
+            'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                         'frac': achieved / peak, 'traffic': traffic, 'peak_source': peak_kind,
+                         'algorithmic_bytes_per_launch': bytes_avg, 'kernel': 'bm25k::TileSearchKernel'},
+            'gpu_launches': args.steps,
+            'clocks': clock_info,
+            'parity': parity,
+        }
+        if cpu is not None:
+            line['cpu_baseline'] = cpu
+        print(json.dumps(line), flush=True)
+    session.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == '__main__':
+    sys.exit(main())

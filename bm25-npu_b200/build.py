@@ -1,0 +1,66 @@
+"""Build recipe of the native libraries, in-tree (the built .so files travel with the repository).
+
+  libbm25_b200.so   CUDA engine + C ABI (nvcc, sm_100a only)
+  libbm25_synth.so  seeded synthetic corpus -> resident-index arrays (gcc + OpenMP)
+
+Run as ``python bm25-npu_b200/build.py`` or through ``__graft_entry__.build()``.
+"""
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+PACKAGE = Path(__file__).resolve().parent
+ROOT = PACKAGE.parent
+CSRC = PACKAGE / 'csrc'
+INCLUDE = ROOT / 'include'
+NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
+ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
+
+ENGINE_SOURCES = ['engine.cu']
+ENGINE_HEADERS = ['tile_kernels.cuh']
+
+
+def _stale(target, sources):
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(s.stat().st_mtime > t for s in sources)
+
+
+def _run(cmd):
+    print(' '.join(str(c) for c in cmd), flush=True)
+    subprocess.run([str(c) for c in cmd], check=True)
+
+
+def build_engine(force=False, verbose_ptxas=False):
+    target = PACKAGE / 'libbm25_b200.so'
+    sources = [CSRC / s for s in ENGINE_SOURCES]
+    deps = sources + [CSRC / h for h in ENGINE_HEADERS] + [INCLUDE / 'bm25_b200.h', Path(__file__)]
+    if not force and not _stale(target, deps):
+        return target
+    cmd = [NVCC, *ARCH, '-lineinfo', '-O3', '-std=c++17', '-shared', '-Xcompiler', '-fPIC,-fopenmp',
+           '-I', INCLUDE, '-I', CSRC, '-o', target, *sources, '-lgomp']
+    if verbose_ptxas:
+        cmd[1:1] = ['-Xptxas', '-v']
+    _run(cmd)
+    return target
+
+
+def build_synth(force=False):
+    target = PACKAGE / 'libbm25_synth.so'
+    src = CSRC / 'synth.c'
+    if not force and not _stale(target, [src, Path(__file__)]):
+        return target
+    _run(['gcc', '-O3', '-std=c11', '-fopenmp', '-ffp-contract=off', '-fno-fast-math', '-fPIC', '-shared',
+          '-o', target, src, '-lm'])
+    return target
+
+
+def build_all(force=False):
+    return build_engine(force), build_synth(force)
+
+
+if __name__ == '__main__':
+    build_all(force='--force' in sys.argv)

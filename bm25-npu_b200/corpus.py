@@ -1,0 +1,129 @@
+"""Resident-index arrays: seeded synthetic corpora and the reference's on-disk index files.
+
+``LazyIndex`` holds the reference's index layout (common/bm25/index_data.h:9-42,
+files of standalone/resident_index.py:12-18).  ``synthetic_index`` builds one
+with the native two-pass generator (csrc/synth.c, the counterpart of
+standalone/large_corpus.py:95-297); ``read_index_dir`` / ``write_index_dir`` use
+the reference's file names and little-endian dtypes.
+"""
+
+import ctypes
+from ctypes import c_float, c_int32, c_int64
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+from . import _native as n
+
+INDEX_FILES = {
+    'term_offsets.bin': np.dtype('<i8'),
+    'posting_doc_ids.bin': np.dtype('<i4'),
+    'posting_tf.bin': np.dtype('<f4'),
+    'doc_norm.bin': np.dtype('<f4'),
+    'idf.bin': np.dtype('<f4'),
+}
+
+
+@dataclass
+class LazyIndex:
+    offsets: np.ndarray  # int64 [V+1]
+    docs: np.ndarray     # int32 [M]
+    tf: np.ndarray       # float32 [M]
+    norm: np.ndarray     # float32 [N]
+    idf: np.ndarray      # float32 [V]
+    doc_len: np.ndarray = None  # int32 [N] (synthetic corpora only)
+
+    @property
+    def num_docs(self):
+        return int(self.norm.size)
+
+    @property
+    def vocab(self):
+        return int(self.idf.size)
+
+    @property
+    def postings(self):
+        return int(self.docs.size)
+
+    def df(self):
+        return np.diff(self.offsets)
+
+
+@dataclass
+class CorpusSpec:
+    """Seeded synthetic corpus shape: Zipf(s) token ranks, lognormal lengths (mean, sigma)."""
+
+    docs: int
+    vocab: int
+    zipf_s: float = 1.1
+    len_mean: float = 60.0
+    len_sigma: float = 0.5
+    seed: int = 20261203
+    k1: float = 1.5
+    b: float = 0.75
+
+
+# Workload shapes: 8192 docs / V 30k; 10M docs / V 1M; 8.8M passages / V 2.5M; 4.2M docs / V 1M.
+CONFIG_SHAPES = {
+    'synthetic_8192': CorpusSpec(docs=8192, vocab=30000),
+    'synthetic_10m': CorpusSpec(docs=10_000_000, vocab=1_000_000),
+    'passages_8p8m': CorpusSpec(docs=8_800_000, vocab=2_500_000, zipf_s=1.05, len_mean=56.0),
+    'blockmax_4p2m': CorpusSpec(docs=4_200_000, vocab=1_000_000, len_mean=80.0),
+}
+
+
+def synthetic_index(spec, threads=0):
+    """Builds the lazy index of a seeded synthetic corpus (deterministic for any thread count)."""
+    lib = n.synth_library()
+    h = lib.synth_create(spec.docs, spec.vocab, spec.zipf_s, spec.len_mean, spec.len_sigma, spec.seed, threads)
+    if not h:
+        raise ValueError('synthetic corpus: invalid shape or out of memory')
+    try:
+        m = lib.synth_postings(h)
+        offsets = np.empty(spec.vocab + 1, dtype=np.int64)
+        docs = np.empty(m, dtype=np.int32)
+        tf = np.empty(m, dtype=np.float32)
+        norm = np.empty(spec.docs, dtype=np.float32)
+        idf = np.empty(spec.vocab, dtype=np.float32)
+        doc_len = np.empty(spec.docs, dtype=np.int32)
+        rc = lib.synth_fill(h, spec.k1, spec.b, n.ptr(offsets, c_int64), n.ptr(docs, c_int32), n.ptr(tf, c_float),
+                            n.ptr(norm, c_float), n.ptr(idf, c_float), n.ptr(doc_len, c_int32))
+        if rc != 0:
+            raise MemoryError('synthetic corpus: pass 2 failed')
+    finally:
+        lib.synth_destroy(h)
+    return LazyIndex(offsets, docs, tf, norm, idf, doc_len)
+
+
+def synthetic_queries(offsets, count, lo, hi, seed, distinct=True):
+    """Seeded query batch, terms drawn with probability df / M; returns (offsets int64, words int32)."""
+    lib = n.synth_library()
+    offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+    qoff = np.empty(count + 1, dtype=np.int64)
+    words = np.empty(max(1, count * hi), dtype=np.int32)
+    w = lib.synth_queries(n.ptr(offsets, c_int64), offsets.size - 1, count, lo, hi, int(distinct), seed,
+                          n.ptr(qoff, c_int64), n.ptr(words, c_int32))
+    if w < 0:
+        raise ValueError('synthetic queries: invalid arguments')
+    return qoff, words[:w].copy()
+
+
+def unpack_queries(qoffsets, words):
+    return [words[qoffsets[i]:qoffsets[i + 1]].tolist() for i in range(qoffsets.size - 1)]
+
+
+def read_index_dir(path):
+    """Reads the reference's index directory (term_offsets.bin, posting_doc_ids.bin, posting_tf.bin, ...)."""
+    path = Path(path)
+    arrays = {name: np.fromfile(path / name, dtype=dt) for name, dt in INDEX_FILES.items()}
+    return LazyIndex(arrays['term_offsets.bin'].astype(np.int64), arrays['posting_doc_ids.bin'].astype(np.int32),
+                     arrays['posting_tf.bin'].astype(np.float32), arrays['doc_norm.bin'].astype(np.float32),
+                     arrays['idf.bin'].astype(np.float32))
+
+
+def write_index_dir(index, path):
+    path = Path(path)
+    path.mkdir(parents=True, exist_ok=True)
+    for (name, dt), values in zip(INDEX_FILES.items(), (index.offsets, index.docs, index.tf, index.norm, index.idf)):
+        np.ascontiguousarray(values, dtype=dt).tofile(path / name)

@@ -1,0 +1,806 @@
+// Host runtime of the B200 BM25 engine and its C ABI (include/bm25_b200.h).
+//
+// Replaces the reference's ACL session layer
+//   feature_retrieval/src/ascendfaiss/ascendhost/src/bm25/large_search.cpp:107-212
+//   feature_retrieval/src/ascendfaiss/ascendhost/src/bm25/planned_search.{h,cpp}
+//   feature_retrieval/src/ascendfaiss/ascendhost/src/bm25/runtime.cpp
+// with the CUDA runtime: a resident index in HBM, a per-tile posting directory
+// built on the device, pinned host arenas for the query packet and the result,
+// and one CUDA graph per (Q, K) holding H2D -> fused scoring/selection/merge ->
+// D2H.  Search = validate + pack, graph replay, synchronise, validate result.
+#include "bm25_b200.h"
+#include "tile_kernels.cuh"
+
+#include <cuda_runtime.h>
+#include <omp.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace bm25b200 {
+
+// Exception classes of common/bm25/error.h:8-31.
+struct InvalidArgument : std::runtime_error {
+    explicit InvalidArgument(const std::string &m) : std::runtime_error(m) {}
+};
+struct InvalidState : std::runtime_error {
+    explicit InvalidState(const std::string &m) : std::runtime_error(m) {}
+};
+struct DeviceError : std::runtime_error {
+    DeviceError(int64_t c, const std::string &m) : std::runtime_error(m), code(c) {}
+    int64_t code;
+};
+
+static void Check(bool ok, const std::string &message)
+{
+    if (!ok)
+        throw InvalidArgument(message);
+}
+
+static void Cuda(cudaError_t e, const char *what)
+{
+    if (e != cudaSuccess)
+        throw DeviceError((int64_t)e, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+static size_t Align32(size_t n) { return (n + 31) & ~size_t(31); }
+
+constexpr int kPad = 256; // zero elements after the posting arrays for 128-bit tail loads
+
+// ---------------------------------------------------------------------------
+// Index validation (host, OpenMP over terms).
+
+// Eager CSC rules: bm25s layout with sorted unique ids and finite non-negative scores.
+static void ValidateEager(const int64_t *indptr, const int32_t *indices, const float *data, int64_t vocab,
+                          int64_t docs)
+{
+    Check(indptr && indices && data, "Null index array");
+    Check(vocab >= 1 && vocab < INT32_MAX && docs >= 1 && docs <= INT32_MAX, "Empty or oversized index");
+    Check(indptr[0] == 0, "Index dimensions/endpoints differ");
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic, 1024) reduction(| : bad)
+    for (int64_t t = 0; t < vocab; ++t) {
+        const int64_t b = indptr[t], e = indptr[t + 1];
+        if (b < 0 || e < b) {
+            bad |= 1;
+            continue;
+        }
+        for (int64_t p = b; p < e; ++p) {
+            const int32_t d = indices[p];
+            if (d < 0 || d >= docs || (p > b && indices[p - 1] >= d))
+                bad |= 2;
+            const float v = data[p];
+            if (!(v >= 0.0f && v <= 3.402823466e+38F))
+                bad |= 4;
+        }
+    }
+    Check(!(bad & 1), "Invalid posting bounds");
+    Check(!(bad & 2), "Unsorted/duplicate/out-of-range posting ID");
+    Check(!(bad & 4), "Invalid posting score");
+}
+
+// Lazy index rules of common/bm25/index_data.h:18-40.
+static void ValidateLazy(const int64_t *offsets, const int32_t *docs, const float *tf, const float *norm,
+                         const float *idf, int64_t vocab, int64_t ndocs)
+{
+    Check(offsets && docs && tf && norm && idf, "Null index array");
+    Check(ndocs >= 1 && ndocs <= INT32_MAX && vocab >= 1 && vocab < INT32_MAX, "Empty or oversized index");
+    Check(offsets[0] == 0 && offsets[vocab] >= 0 && offsets[vocab] <= INT32_MAX, "Index dimensions/endpoints differ");
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (int64_t d = 0; d < ndocs; ++d)
+        if (!(std::isfinite(norm[d]) && norm[d] > 0))
+            bad |= 8;
+    Check(!(bad & 8), "Invalid article norm");
+#pragma omp parallel for schedule(dynamic, 1024) reduction(| : bad)
+    for (int64_t t = 0; t < vocab; ++t) {
+        if (!(std::isfinite(idf[t]) && idf[t] >= 0))
+            bad |= 16;
+        const int64_t b = offsets[t], e = offsets[t + 1];
+        if (b < 0 || e < b) {
+            bad |= 1;
+            continue;
+        }
+        for (int64_t p = b; p < e; ++p) {
+            const int32_t d = docs[p];
+            if (d < 0 || d >= ndocs || (p > b && docs[p - 1] >= d))
+                bad |= 2;
+            const float f = tf[p];
+            if (!(std::isfinite(f) && f >= 1 && f <= 16777216.0F && std::floor(f) == f))
+                bad |= 4;
+        }
+    }
+    Check(!(bad & 16), "Invalid IDF");
+    Check(!(bad & 1), "Invalid posting bounds");
+    Check(!(bad & 2), "Unsorted/duplicate/out-of-range posting ID");
+    Check(!(bad & 4), "Invalid posting TF");
+}
+
+// ---------------------------------------------------------------------------
+
+class Engine {
+  public:
+    struct Plan {
+        int tile_docs = 0, tiles = 0, fan_in = 32, levels = 0;
+        std::vector<int> lists;  // lists per query at each level
+        int64_t dir_rows = 0, dir_min_df = 0;
+    };
+
+    Engine(const bm25_options &o, int64_t vocab, int64_t docs, int64_t postings)
+        : opts_(o), vocab_(vocab), docs_(docs), postings_(postings)
+    {
+        Check(o.max_k >= 1 && o.max_k <= bm25k::kMaxSmallK, "max_k must be in [1, 32]");
+        Check(o.max_k <= docs, "max_k exceeds the document count");
+        Check(o.query_capacity >= 1 && o.query_capacity <= 65535, "query_capacity must be in [1, 65535]");
+        Check(o.word_capacity >= 0 && o.word_capacity <= 16777216, "word_capacity must be in [0, 2^24]");
+        Cuda(cudaSetDevice(o.device_id), "cudaSetDevice");
+        device_ = o.device_id;
+        size_t total = 0;
+        Cuda(cudaMemGetInfo(&free_at_start_, &total), "cudaMemGetInfo");
+        if (o.stream) {
+            stream_ = static_cast<cudaStream_t>(o.stream);
+        } else {
+            Cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+            own_stream_ = true;
+        }
+        Cuda(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming), "cudaEventCreate");
+        MakePlan();
+    }
+
+    ~Engine() { Release(); }
+
+    // Uploads an eager CSC index.
+    void UploadEager(const int64_t *indptr, const int32_t *indices, const float *data)
+    {
+        AllocIndex();
+        Cuda(cudaMemcpy(d_indptr_, indptr, (vocab_ + 1) * sizeof(int64_t), cudaMemcpyHostToDevice), "index upload");
+        Cuda(cudaMemcpy(d_indices_, indices, postings_ * sizeof(int32_t), cudaMemcpyHostToDevice), "index upload");
+        Cuda(cudaMemcpy(d_data_, data, postings_ * sizeof(float), cudaMemcpyHostToDevice), "index upload");
+        Finish(indptr);
+    }
+
+    // Uploads the reference's lazy index and builds the eager scores on the device.
+    void UploadLazy(const int64_t *offsets, const int32_t *docs, const float *tf, const float *norm, const float *idf,
+                    float k1)
+    {
+        Check(std::isfinite(k1) && k1 >= 0, "Invalid k1");
+        AllocIndex();
+        Cuda(cudaMemcpy(d_indptr_, offsets, (vocab_ + 1) * sizeof(int64_t), cudaMemcpyHostToDevice), "index upload");
+        Cuda(cudaMemcpy(d_indices_, docs, postings_ * sizeof(int32_t), cudaMemcpyHostToDevice), "index upload");
+        float *d_tf = nullptr, *d_norm = nullptr, *d_idf = nullptr;
+        unsigned *d_status = nullptr;
+        try {
+            Cuda(cudaMalloc(&d_tf, std::max<int64_t>(postings_, 1) * sizeof(float)), "cudaMalloc tf");
+            Cuda(cudaMalloc(&d_norm, docs_ * sizeof(float)), "cudaMalloc norm");
+            Cuda(cudaMalloc(&d_idf, vocab_ * sizeof(float)), "cudaMalloc idf");
+            Cuda(cudaMalloc(&d_status, sizeof(unsigned)), "cudaMalloc status");
+            Cuda(cudaMemcpy(d_tf, tf, postings_ * sizeof(float), cudaMemcpyHostToDevice), "index upload");
+            Cuda(cudaMemcpy(d_norm, norm, docs_ * sizeof(float), cudaMemcpyHostToDevice), "index upload");
+            Cuda(cudaMemcpy(d_idf, idf, vocab_ * sizeof(float), cudaMemcpyHostToDevice), "index upload");
+            Cuda(cudaMemset(d_status, 0, sizeof(unsigned)), "cudaMemset");
+            // f32(k1 + 1) with the sum in double: k1 = 1.2 gives the reference's 2.2F.
+            const float k1p1 = (float)((double)k1 + 1.0);
+            if (postings_ > 0) {
+                const long long chunks = (postings_ + bm25k::kBuildChunk - 1) / bm25k::kBuildChunk;
+                const int grid = (int)std::min<long long>(chunks, 148 * 16);
+                bm25k::BuildContributionsKernel<<<grid, 256, 0, stream_>>>(
+                    (const long long *)d_indptr_, (int)vocab_, postings_, d_indices_, d_tf, d_norm, d_idf, k1p1,
+                    d_data_, d_status);
+                Cuda(cudaGetLastError(), "contribution kernel launch");
+            }
+            unsigned status = 0;
+            Cuda(cudaMemcpyAsync(&status, d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_), "status");
+            Cuda(cudaStreamSynchronize(stream_), "contribution kernel");
+            Check(status == 0, "Posting contribution outside the finite FP32 range");
+        } catch (...) {
+            cudaFree(d_tf);
+            cudaFree(d_norm);
+            cudaFree(d_idf);
+            cudaFree(d_status);
+            throw;
+        }
+        cudaFree(d_tf);
+        cudaFree(d_norm);
+        cudaFree(d_idf);
+        cudaFree(d_status);
+        Finish(offsets);
+    }
+
+    void Search(const int64_t *qoffsets, const int32_t *words, int64_t q, int32_t k, float *out_scores,
+                int32_t *out_ids)
+    {
+        RequireUsable();
+        Check(out_scores && out_ids, "Null output buffer");
+        Pack(qoffsets, words, q, k);  // validates everything before touching the arena
+        try {
+            Cuda(cudaSetDevice(device_), "cudaSetDevice");
+            cudaGraphExec_t exec = GraphFor((int)q, k);
+            Cuda(cudaStreamWaitEvent(stream_, done_, 0), "cudaStreamWaitEvent");
+            ++searches_;
+            Cuda(cudaGraphLaunch(exec, stream_), "cudaGraphLaunch");
+            ++replays_;
+            Cuda(cudaEventRecord(done_, stream_), "cudaEventRecord");
+            Cuda(cudaStreamSynchronize(stream_), "complete Search through result D2H");
+            Receive(q, k, out_scores, out_ids);
+        } catch (...) {
+            failed_ = true;
+            throw;
+        }
+    }
+
+    void SearchDevice(const int64_t *qoffsets, const int32_t *words, int64_t q, int32_t k, float *out_scores,
+                      int32_t *out_ids, cudaStream_t stream)
+    {
+        RequireUsable();
+        Check(q >= 1 && q <= opts_.query_capacity, "Query batch exceeds declared capacity or is empty");
+        Check(k >= 1 && k <= opts_.max_k && k <= docs_, "K outside [1, min(max_k, N)]");
+        Check(qoffsets && words && out_scores && out_ids, "Null device buffer");
+        try {
+            Cuda(cudaSetDevice(device_), "cudaSetDevice");
+            cudaStream_t s = stream ? stream : stream_;
+            Cuda(cudaStreamWaitEvent(s, done_, 0), "cudaStreamWaitEvent");
+            ++searches_;
+            Launch((int)q, k, qoffsets, words, out_scores, out_ids, d_dev_status_, s);
+            Cuda(cudaEventRecord(done_, s), "cudaEventRecord");
+        } catch (...) {
+            failed_ = true;
+            throw;
+        }
+    }
+
+    uint32_t DeviceStatus()
+    {
+        RequireUsable();
+        unsigned status = 0;
+        try {
+            Cuda(cudaSetDevice(device_), "cudaSetDevice");
+            Cuda(cudaStreamWaitEvent(stream_, done_, 0), "cudaStreamWaitEvent");
+            Cuda(cudaMemcpyAsync(&status, d_dev_status_, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_),
+                 "status D2H");
+            Cuda(cudaMemsetAsync(d_dev_status_, 0, sizeof(unsigned), stream_), "status reset");
+            Cuda(cudaStreamSynchronize(stream_), "status sync");
+        } catch (...) {
+            failed_ = true;
+            throw;
+        }
+        return status;
+    }
+
+    void Close()
+    {
+        if (closed_)
+            return;
+        Cuda(cudaSetDevice(device_), "cudaSetDevice");
+        Cuda(cudaStreamSynchronize(stream_), "drain before close");
+        Release();
+        closed_ = true;
+    }
+
+    void Info(bm25_info *info) const
+    {
+        info->num_docs = docs_;
+        info->vocab = vocab_;
+        info->postings = postings_;
+        info->tile_docs = plan_.tile_docs;
+        info->tiles = plan_.tiles;
+        info->merge_fan_in = plan_.fan_in;
+        info->merge_levels = plan_.levels;
+        info->directory_rows = plan_.dir_rows;
+        info->directory_min_df = plan_.dir_min_df;
+        info->index_bytes = index_bytes_;
+        info->device_bytes = device_bytes_;
+        info->graph_replays = replays_;
+        info->searches = searches_;
+    }
+
+  private:
+    void RequireUsable() const
+    {
+        if (closed_ || failed_)
+            throw InvalidState(closed_ ? "BM25 session is closed" : "BM25 session failed; Close and re-create it");
+    }
+
+    void *Alloc(size_t bytes, const char *what)
+    {
+        void *p = nullptr;
+        Cuda(cudaMalloc(&p, std::max<size_t>(bytes, 16)), what);
+        allocations_.push_back(p);
+        device_bytes_ += (int64_t)bytes;
+        return p;
+    }
+
+    void MakePlan()
+    {
+        int t = opts_.tile_docs;
+        if (t == 0) {
+            const int64_t per_sm = (docs_ + 147) / 148;
+            t = 2048;
+            while (t < per_sm && t < 16384)
+                t <<= 1;
+        }
+        Check(t >= 2048 && t <= 32768 && (t & (t - 1)) == 0, "tile_docs must be a power of two in [2048, 32768]");
+        plan_.tile_docs = t;
+        plan_.tiles = (int)((docs_ + t - 1) / t);
+        int f = opts_.merge_fan_in ? opts_.merge_fan_in : 32;
+        Check(f >= 2 && f <= 1024, "merge_fan_in must be in [2, 1024]");
+        for (;;) {
+            plan_.lists.clear();
+            int n = plan_.tiles;
+            plan_.lists.push_back(n);
+            while (n > 1) {
+                n = (n + f - 1) / f;
+                plan_.lists.push_back(n);
+            }
+            if ((int)plan_.lists.size() <= bm25k::kMaxLevels)
+                break;
+            f *= 2;
+        }
+        plan_.fan_in = f;
+        plan_.levels = (int)plan_.lists.size();
+    }
+
+    void AllocIndex()
+    {
+        d_indptr_ = static_cast<int64_t *>(Alloc((vocab_ + 1) * sizeof(int64_t), "cudaMalloc indptr"));
+        d_indices_ = static_cast<int32_t *>(Alloc((postings_ + kPad) * sizeof(int32_t), "cudaMalloc indices"));
+        d_data_ = static_cast<float *>(Alloc((postings_ + kPad) * sizeof(float), "cudaMalloc data"));
+        Cuda(cudaMemset(d_indices_ + postings_, 0, kPad * sizeof(int32_t)), "cudaMemset pad");
+        Cuda(cudaMemset(d_data_ + postings_, 0, kPad * sizeof(float)), "cudaMemset pad");
+        index_bytes_ = (vocab_ + 1) * 8 + postings_ * 8;
+    }
+
+    // Directory, arenas, merge-tree storage and kernel attributes.
+    void Finish(const int64_t *indptr)
+    {
+        const int tiles = plan_.tiles;
+        // Long lists (df >= min_df) get one directory row of tiles + 1 offsets;
+        // shorter lists are counted cooperatively inside the tile CTA.
+        std::vector<int64_t> dfs(vocab_);
+        for (int64_t t = 0; t < vocab_; ++t)
+            dfs[t] = indptr[t + 1] - indptr[t];
+        int64_t min_df = std::max<int64_t>(32, tiles);
+        const int64_t row_bytes = (int64_t)(tiles + 1) * 4;
+        int64_t budget = opts_.directory_bytes;
+        if (budget <= 0)
+            budget = std::max<int64_t>(int64_t(64) << 20, std::min<int64_t>(int64_t(4) << 30, index_bytes_ / 4));
+        int64_t rows = 0;
+        for (int64_t t = 0; t < vocab_; ++t)
+            rows += dfs[t] >= min_df;
+        if (rows * row_bytes > budget) {
+            std::vector<int64_t> sorted(dfs);
+            const int64_t keep = std::max<int64_t>(0, budget / row_bytes);
+            std::nth_element(sorted.begin(), sorted.begin() + keep, sorted.end(), std::greater<int64_t>());
+            min_df = sorted[keep] + 1;
+            rows = 0;
+            for (int64_t t = 0; t < vocab_; ++t)
+                rows += dfs[t] >= min_df;
+        }
+        plan_.dir_min_df = min_df;
+        plan_.dir_rows = rows;
+        std::vector<int32_t> dir_row(vocab_, -1), dir_terms;
+        dir_terms.reserve(rows);
+        for (int64_t t = 0; t < vocab_; ++t)
+            if (dfs[t] >= min_df) {
+                dir_row[t] = (int32_t)dir_terms.size();
+                dir_terms.push_back((int32_t)t);
+            }
+        d_dir_row_ = static_cast<int32_t *>(Alloc(vocab_ * sizeof(int32_t), "cudaMalloc dir_row"));
+        Cuda(cudaMemcpy(d_dir_row_, dir_row.data(), vocab_ * sizeof(int32_t), cudaMemcpyHostToDevice), "dir upload");
+        d_dir_ = static_cast<int32_t *>(Alloc(std::max<int64_t>(rows, 1) * row_bytes, "cudaMalloc directory"));
+        if (rows > 0) {
+            int32_t *d_terms = static_cast<int32_t *>(Alloc(rows * sizeof(int32_t), "cudaMalloc dir terms"));
+            Cuda(cudaMemcpy(d_terms, dir_terms.data(), rows * sizeof(int32_t), cudaMemcpyHostToDevice), "dir upload");
+            const long long total = rows * (long long)(tiles + 1);
+            const int grid = (int)std::min<long long>((total + 255) / 256, 148 * 64);
+            bm25k::BuildDirectoryKernel<<<grid, 256, 0, stream_>>>((const long long *)d_indptr_, d_indices_, d_terms,
+                                                                   rows, plan_.tile_docs, tiles, d_dir_, tiles + 1);
+            Cuda(cudaGetLastError(), "directory kernel launch");
+            Cuda(cudaStreamSynchronize(stream_), "directory kernel");
+        }
+        // Query packet / result arenas (fixed_query_packet.h:15-25 layout).
+        word_offset_ = Align32((opts_.query_capacity + 1) * sizeof(int64_t));
+        in_bytes_ = Align32(word_offset_ + std::max<int64_t>(1, opts_.word_capacity) * sizeof(int32_t));
+        const size_t qk = (size_t)opts_.query_capacity * opts_.max_k;
+        out_bytes_ = Align32(qk * 4) * 2 + 32;
+        Cuda(cudaHostAlloc(&h_in_, in_bytes_, cudaHostAllocDefault), "cudaHostAlloc");
+        Cuda(cudaHostAlloc(&h_out_, out_bytes_, cudaHostAllocDefault), "cudaHostAlloc");
+        std::memset(h_in_, 0, in_bytes_);
+        d_in_ = static_cast<unsigned char *>(Alloc(in_bytes_, "cudaMalloc input arena"));
+        d_out_ = static_cast<unsigned char *>(Alloc(out_bytes_, "cudaMalloc output arena"));
+        d_dev_status_ = static_cast<unsigned *>(Alloc(sizeof(unsigned), "cudaMalloc status"));
+        Cuda(cudaMemset(d_dev_status_, 0, sizeof(unsigned)), "cudaMemset");
+        // Merge tree: level 0 holds tile lists, the root level is the output.
+        for (int l = 0; l < plan_.levels; ++l) {
+            bm25k::Level lv{};
+            lv.n = plan_.lists[l];
+            if (lv.n > 1) {
+                const size_t nodes = (size_t)opts_.query_capacity * lv.n;
+                lv.scores = static_cast<float *>(Alloc(nodes * opts_.max_k * sizeof(float), "cudaMalloc tree"));
+                lv.ids = static_cast<int *>(Alloc(nodes * opts_.max_k * sizeof(int), "cudaMalloc tree"));
+                lv.counts = static_cast<int *>(Alloc(nodes * sizeof(int), "cudaMalloc tree"));
+            }
+            if (l > 0) {
+                const size_t nodes = (size_t)opts_.query_capacity * lv.n;
+                lv.arrivals = static_cast<unsigned *>(Alloc(nodes * sizeof(unsigned), "cudaMalloc arrivals"));
+                Cuda(cudaMemset(lv.arrivals, 0, nodes * sizeof(unsigned)), "cudaMemset arrivals");
+            }
+            levels_.push_back(lv);
+        }
+        smem_bytes_ = (size_t)plan_.tile_docs * sizeof(float) + sizeof(bm25k::TileShared);
+        Cuda(cudaFuncSetAttribute(bm25k::TileSearchKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem_bytes_),
+             "cudaFuncSetAttribute");
+        Cuda(cudaDeviceSynchronize(), "index preparation");
+    }
+
+    void Launch(int q, int k, const int64_t *qoffsets, const int32_t *words, float *out_scores, int32_t *out_ids,
+                unsigned *status, cudaStream_t s)
+    {
+        bm25k::TileArgs a{};
+        a.indptr = (const long long *)d_indptr_;
+        a.indices = d_indices_;
+        a.data = d_data_;
+        a.dir_row = d_dir_row_;
+        a.dir = d_dir_;
+        a.dir_stride = plan_.tiles + 1;
+        a.qoffsets = (const long long *)qoffsets;
+        a.words = words;
+        a.vocab = (int)vocab_;
+        a.num_docs = (int)docs_;
+        a.tile_docs = plan_.tile_docs;
+        a.tiles = plan_.tiles;
+        a.k = k;
+        a.fan_in = plan_.fan_in;
+        a.levels = plan_.levels;
+        for (int l = 0; l < plan_.levels; ++l)
+            a.lv[l] = levels_[l];
+        a.out_scores = out_scores;
+        a.out_ids = out_ids;
+        a.status = status;
+        dim3 grid(plan_.tiles, q);
+        bm25k::TileSearchKernel<<<grid, bm25k::kThreads, smem_bytes_, s>>>(a);
+        Cuda(cudaGetLastError(), "tile kernel launch");
+    }
+
+    size_t IdOffset(int q, int k) const { return Align32((size_t)q * k * 4); }
+    size_t StatusOffset(int q, int k) const { return Align32(IdOffset(q, k) + (size_t)q * k * 4); }
+
+    cudaGraphExec_t GraphFor(int q, int k)
+    {
+        const auto key = std::make_pair(q, k);
+        auto it = graphs_.find(key);
+        if (it != graphs_.end())
+            return it->second;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        Cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin graph capture");
+        try {
+            Cuda(cudaMemcpyAsync(d_in_, h_in_, in_bytes_, cudaMemcpyHostToDevice, stream_), "query H2D");
+            unsigned *status = reinterpret_cast<unsigned *>(d_out_ + StatusOffset(q, k));
+            Cuda(cudaMemsetAsync(status, 0, sizeof(unsigned), stream_), "status reset");
+            Launch(q, k, reinterpret_cast<const int64_t *>(d_in_), reinterpret_cast<const int32_t *>(d_in_ + word_offset_),
+                   reinterpret_cast<float *>(d_out_), reinterpret_cast<int32_t *>(d_out_ + IdOffset(q, k)), status,
+                   stream_);
+            Cuda(cudaMemcpyAsync(h_out_, d_out_, StatusOffset(q, k) + 32, cudaMemcpyDeviceToHost, stream_),
+                 "top-K D2H");
+        } catch (...) {
+            cudaStreamEndCapture(stream_, &graph);
+            if (graph)
+                cudaGraphDestroy(graph);
+            throw;
+        }
+        Cuda(cudaStreamEndCapture(stream_, &graph), "end graph capture");
+        const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        Cuda(e, "cudaGraphInstantiate");
+        graphs_[key] = exec;
+        return exec;
+    }
+
+    // Validates the whole request before writing the arena (fixed_query_packet.h:26-49).
+    void Pack(const int64_t *qoffsets, const int32_t *words, int64_t q, int32_t k)
+    {
+        Check(q >= 1 && q <= opts_.query_capacity, "Query batch exceeds declared capacity or is empty");
+        Check(k >= 1 && k <= opts_.max_k && k <= docs_, "K outside [1, min(max_k, N)]");
+        Check(qoffsets != nullptr && qoffsets[0] == 0, "Query offsets must start at 0");
+        for (int64_t i = 0; i < q; ++i) {
+            const int64_t n = qoffsets[i + 1] - qoffsets[i];
+            Check(n >= 0 && n <= bm25k::kMaxTerms, "Query exceeds fixed word/64-term capacity");
+        }
+        const int64_t total = qoffsets[q];
+        Check(total <= opts_.word_capacity, "Word IDs exceed declared query capacity");
+        Check(total == 0 || words != nullptr, "Null word buffer");
+        for (int64_t w = 0; w < total; ++w)
+            Check(words[w] >= 0 && words[w] < INT32_MAX, "Invalid public word ID");
+        std::memset(h_in_, 0, in_bytes_);
+        std::memcpy(h_in_, qoffsets, (q + 1) * sizeof(int64_t));
+        if (total)
+            std::memcpy(static_cast<unsigned char *>(h_in_) + word_offset_, words, total * sizeof(int32_t));
+    }
+
+    // Host-side result checks of large_search.cpp:153-174.
+    void Receive(int64_t q, int32_t k, float *out_scores, int32_t *out_ids)
+    {
+        const unsigned char *base = static_cast<const unsigned char *>(h_out_);
+        unsigned status = 0;
+        std::memcpy(&status, base + StatusOffset((int)q, k), sizeof(unsigned));
+        if (status)
+            throw DeviceError(0, "Device reported invalid Search state, status=" + std::to_string(status));
+        const float *scores = reinterpret_cast<const float *>(base);
+        const int32_t *ids = reinterpret_cast<const int32_t *>(base + IdOffset((int)q, k));
+        const size_t n = (size_t)q * k;
+        for (size_t i = 0; i < n; ++i) {
+            if (!(ids[i] >= 0 && ids[i] < docs_ && std::isfinite(scores[i]) && scores[i] >= 0))
+                throw DeviceError(0, "Invalid real-document result");
+            if (i % k && !(scores[i - 1] > scores[i] || (scores[i - 1] == scores[i] && ids[i - 1] < ids[i])))
+                throw DeviceError(0, "Strict global ranking failure");
+        }
+        std::memcpy(out_scores, scores, n * sizeof(float));
+        std::memcpy(out_ids, ids, n * sizeof(int32_t));
+    }
+
+    void Release()
+    {
+        for (auto &g : graphs_)
+            cudaGraphExecDestroy(g.second);
+        graphs_.clear();
+        for (void *p : allocations_)
+            cudaFree(p);
+        allocations_.clear();
+        levels_.clear();
+        if (h_in_)
+            cudaFreeHost(h_in_);
+        if (h_out_)
+            cudaFreeHost(h_out_);
+        h_in_ = h_out_ = nullptr;
+        if (done_)
+            cudaEventDestroy(done_);
+        done_ = nullptr;
+        if (own_stream_ && stream_)
+            cudaStreamDestroy(stream_);
+        stream_ = nullptr;
+        own_stream_ = false;
+    }
+
+    bm25_options opts_;
+    int64_t vocab_, docs_, postings_;
+    int device_ = 0;
+    cudaStream_t stream_ = nullptr;
+    bool own_stream_ = false;
+    cudaEvent_t done_ = nullptr;
+    size_t free_at_start_ = 0;
+    Plan plan_;
+    std::vector<void *> allocations_;
+    int64_t device_bytes_ = 0, index_bytes_ = 0;
+    int64_t *d_indptr_ = nullptr;
+    int32_t *d_indices_ = nullptr;
+    float *d_data_ = nullptr;
+    int32_t *d_dir_row_ = nullptr, *d_dir_ = nullptr;
+    std::vector<bm25k::Level> levels_;
+    size_t word_offset_ = 0, in_bytes_ = 0, out_bytes_ = 0, smem_bytes_ = 0;
+    void *h_in_ = nullptr, *h_out_ = nullptr;
+    unsigned char *d_in_ = nullptr, *d_out_ = nullptr;
+    unsigned *d_dev_status_ = nullptr;
+    std::map<std::pair<int, int>, cudaGraphExec_t> graphs_;
+    bool closed_ = false, failed_ = false;
+    int64_t replays_ = 0, searches_ = 0;
+};
+
+} // namespace bm25b200
+
+// ---------------------------------------------------------------------------
+// C ABI
+
+struct bm25_handle {
+    std::mutex mutex;
+    std::unique_ptr<bm25b200::Engine> engine;
+    std::string error;
+    int64_t code = 0;
+};
+
+namespace {
+thread_local std::string g_create_error;
+thread_local int64_t g_create_code = 0;
+
+// Error mapping of Bm25ErrorAdapter.h:11-45.
+template <class F> int Invoke(F &&f, std::string &error, int64_t &code) noexcept
+{
+    error.clear();
+    code = 0;
+    try {
+        f();
+        return BM25_OK;
+    } catch (const bm25b200::InvalidArgument &e) {
+        error = e.what();
+        return BM25_ERR_INVALID_PARAM;
+    } catch (const bm25b200::InvalidState &e) {
+        error = e.what();
+        return BM25_ERR_ILLEGAL_OPERATION;
+    } catch (const bm25b200::DeviceError &e) {
+        error = e.what();
+        code = e.code;
+        return BM25_ERR_INNER_ERROR;
+    } catch (const std::exception &e) {
+        error = e.what();
+        return BM25_ERR_INNER_ERROR;
+    } catch (...) {
+        error = "Unknown BM25 failure";
+        return BM25_ERR_INNER_ERROR;
+    }
+}
+
+template <class Upload>
+int Create(int64_t vocab, int64_t docs, int64_t postings, const bm25_options *options, bm25_handle **out,
+           Upload &&upload)
+{
+    return Invoke(
+        [&] {
+            bm25b200::Check(out != nullptr, "Null handle output");
+            *out = nullptr;
+            bm25_options o;
+            bm25_default_options(&o);
+            if (options)
+                o = *options;
+            auto h = std::make_unique<bm25_handle>();
+            h->engine = std::make_unique<bm25b200::Engine>(o, vocab, docs, postings);
+            upload(*h->engine);
+            *out = h.release();
+        },
+        g_create_error, g_create_code);
+}
+} // namespace
+
+extern "C" {
+
+void bm25_default_options(bm25_options *o)
+{
+    if (!o)
+        return;
+    std::memset(o, 0, sizeof(*o));
+    o->device_id = 0;
+    o->max_k = 10;
+    o->query_capacity = 8;
+    o->word_capacity = 24;
+}
+
+int bm25_create(const int64_t *indptr, const int32_t *indices, const float *data, int64_t vocab, int64_t num_docs,
+                const bm25_options *options, bm25_handle **out)
+{
+    int64_t postings = 0;
+    const int pre = Invoke(
+        [&] {
+            bm25b200::Check(indptr != nullptr && vocab >= 1 && vocab < INT32_MAX, "Empty or oversized index");
+            postings = indptr[vocab];
+            bm25b200::ValidateEager(indptr, indices, data, vocab, num_docs);
+        },
+        g_create_error, g_create_code);
+    if (pre != BM25_OK) {
+        if (out)
+            *out = nullptr;
+        return pre;
+    }
+    return Create(vocab, num_docs, postings, options, out,
+                  [&](bm25b200::Engine &e) { e.UploadEager(indptr, indices, data); });
+}
+
+int bm25_create_lazy(const int64_t *term_offsets, const int32_t *posting_doc_ids, const float *posting_tf,
+                     const float *doc_norm, const float *idf, int64_t vocab, int64_t num_docs, float k1,
+                     const bm25_options *options, bm25_handle **out)
+{
+    int64_t postings = 0;
+    const int pre = Invoke(
+        [&] {
+            bm25b200::Check(term_offsets != nullptr && vocab >= 1 && vocab < INT32_MAX, "Empty or oversized index");
+            postings = term_offsets[vocab];
+            bm25b200::ValidateLazy(term_offsets, posting_doc_ids, posting_tf, doc_norm, idf, vocab, num_docs);
+        },
+        g_create_error, g_create_code);
+    if (pre != BM25_OK) {
+        if (out)
+            *out = nullptr;
+        return pre;
+    }
+    return Create(vocab, num_docs, postings, options, out, [&](bm25b200::Engine &e) {
+        e.UploadLazy(term_offsets, posting_doc_ids, posting_tf, doc_norm, idf, k1);
+    });
+}
+
+int bm25_search(bm25_handle *h, const int64_t *qoffsets, const int32_t *words, int64_t q, int32_t k,
+                float *out_scores, int32_t *out_ids)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            h->engine->Search(qoffsets, words, q, k, out_scores, out_ids);
+        },
+        h->error, h->code);
+}
+
+int bm25_search_device(bm25_handle *h, const int64_t *qoffsets, const int32_t *words, int64_t q, int32_t k,
+                       float *out_scores, int32_t *out_ids, void *stream)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            h->engine->SearchDevice(qoffsets, words, q, k, out_scores, out_ids, static_cast<cudaStream_t>(stream));
+        },
+        h->error, h->code);
+}
+
+int bm25_device_status(bm25_handle *h, uint32_t *status)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            bm25b200::Check(status != nullptr, "Null status output");
+            *status = h->engine->DeviceStatus();
+        },
+        h->error, h->code);
+}
+
+int bm25_close(bm25_handle *h)
+{
+    if (!h)
+        return BM25_OK;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (h->engine) {
+                h->engine->Close();
+                h->engine.reset();
+            }
+        },
+        h->error, h->code);
+}
+
+void bm25_destroy(bm25_handle *h)
+{
+    if (!h)
+        return;
+    bm25_close(h);
+    delete h;
+}
+
+int bm25_last_error(const bm25_handle *h, char *buffer, size_t length, int64_t *code)
+{
+    const std::string &e = h ? h->error : g_create_error;
+    if (code)
+        *code = h ? h->code : g_create_code;
+    if (buffer && length) {
+        std::snprintf(buffer, length, "%s", e.c_str());
+    }
+    return BM25_OK;
+}
+
+int bm25_get_info(const bm25_handle *h, bm25_info *info)
+{
+    if (!h || !info)
+        return BM25_ERR_INVALID_PARAM;
+    if (!h->engine)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    h->engine->Info(info);
+    return BM25_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,285 @@
+"""Python mirror of the engine's Search session (C ABI in include/bm25_b200.h).
+
+``Bm25Session`` corresponds to the reference's ``bm25large::Session``
+(feature_retrieval/src/ascendfaiss/ascendhost/src/bm25/large_search.h:35-86) and
+``AscendIndexBm25`` to the SDK facade
+(feature_retrieval/src/ascendfaiss/ascendhost/include/index/AscendIndexBm25.h:37-57):
+same method names, argument meaning and error behaviour (input errors leave the
+session usable, device errors poison it, Close is idempotent).
+"""
+
+import ctypes
+from ctypes import c_float, c_int32, c_int64, c_void_p
+
+import numpy as np
+
+from . import _native as n
+
+
+class Bm25Error(RuntimeError):
+    """Raised for a non-OK status; ``status`` is the C ABI code, ``code`` the CUDA error (or 0)."""
+
+    def __init__(self, status, message, code=0):
+        super().__init__(message)
+        self.status = status
+        self.code = code
+
+
+class InvalidParam(Bm25Error, ValueError):
+    pass
+
+
+class IllegalOperation(Bm25Error):
+    pass
+
+
+class InnerError(Bm25Error):
+    pass
+
+
+_ERRORS = {
+    n.BM25_ERR_INVALID_PARAM: InvalidParam,
+    n.BM25_ERR_ILLEGAL_OPERATION: IllegalOperation,
+    n.BM25_ERR_INNER_ERROR: InnerError,
+}
+
+
+def _last_error(lib, handle):
+    buf = ctypes.create_string_buffer(1024)
+    code = c_int64(0)
+    lib.bm25_last_error(handle, buf, len(buf), ctypes.byref(code))
+    return buf.value.decode('utf-8', 'replace'), code.value
+
+
+def _raise(lib, status, handle):
+    if status == n.BM25_OK:
+        return
+    message, code = _last_error(lib, handle)
+    raise _ERRORS.get(status, Bm25Error)(status, message or f'BM25 status {status}', code)
+
+
+def pack_queries(queries):
+    """List of word-id lists -> (offsets int64 [Q+1], words int32), common/bm25/search_inputs.h:23-42."""
+    offsets = np.zeros(len(queries) + 1, dtype=np.int64)
+    for i, row in enumerate(queries):
+        offsets[i + 1] = offsets[i] + len(row)
+    words = np.fromiter((w for row in queries for w in row), dtype=np.int64, count=int(offsets[-1]))
+    if words.size and (words.min() < 0 or words.max() >= 2**31 - 1):
+        raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'Invalid public word ID')
+    return offsets, words.astype(np.int32)
+
+
+def _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes, stream):
+    o = n.Options()
+    n.engine_library().bm25_default_options(ctypes.byref(o))
+    o.device_id = device_id
+    o.max_k = max_k
+    o.query_capacity = query_capacity
+    o.word_capacity = word_capacity
+    o.tile_docs = tile_docs
+    o.merge_fan_in = merge_fan_in
+    o.directory_bytes = directory_bytes
+    o.stream = stream
+    return o
+
+
+class Bm25Session:
+    """A resident index on one GPU plus its fixed-capacity Search plan."""
+
+    def __init__(self, handle, num_docs, max_k):
+        self._lib = n.engine_library()
+        self._handle = handle
+        self.num_docs = num_docs
+        self.max_k = max_k
+
+    @classmethod
+    def from_csc(cls, indptr, indices, data, num_docs, *, query_capacity=8, word_capacity=24, max_k=10,
+                 device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0, stream=None):
+        """Eager CSC index (bm25s layout): indptr int64 [V+1], indices int32 [M], data float32 [M]."""
+        lib = n.engine_library()
+        indptr = np.ascontiguousarray(indptr, dtype=np.int64)
+        indices = np.ascontiguousarray(indices, dtype=np.int32)
+        data = np.ascontiguousarray(data, dtype=np.float32)
+        vocab = indptr.size - 1
+        if vocab < 1 or indices.size != indptr[-1] or data.size != indices.size:
+            raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'Index dimensions/endpoints differ')
+        o = _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes,
+                     stream)
+        h = c_void_p()
+        status = lib.bm25_create(n.ptr(indptr, c_int64), n.ptr(indices, c_int32), n.ptr(data, c_float), vocab,
+                                 int(num_docs), ctypes.byref(o), ctypes.byref(h))
+        _raise(lib, status, None)
+        return cls(h, int(num_docs), max_k)
+
+    @classmethod
+    def from_lazy(cls, term_offsets, posting_doc_ids, posting_tf, doc_norm, idf, *, k1=1.2, query_capacity=8,
+                  word_capacity=24, max_k=10, device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0,
+                  stream=None):
+        """The reference's resident index (common/bm25/index_data.h:9-42); posting scores built on the GPU."""
+        lib = n.engine_library()
+        offsets = np.ascontiguousarray(term_offsets, dtype=np.int64)
+        docs = np.ascontiguousarray(posting_doc_ids, dtype=np.int32)
+        tf = np.ascontiguousarray(posting_tf, dtype=np.float32)
+        norm = np.ascontiguousarray(doc_norm, dtype=np.float32)
+        idf = np.ascontiguousarray(idf, dtype=np.float32)
+        vocab = idf.size
+        if offsets.size != vocab + 1 or docs.size != tf.size or offsets[-1] != docs.size:
+            raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'Index dimensions/endpoints differ')
+        o = _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes,
+                     stream)
+        h = c_void_p()
+        status = lib.bm25_create_lazy(n.ptr(offsets, c_int64), n.ptr(docs, c_int32), n.ptr(tf, c_float),
+                                      n.ptr(norm, c_float), n.ptr(idf, c_float), vocab, norm.size, float(k1),
+                                      ctypes.byref(o), ctypes.byref(h))
+        _raise(lib, status, None)
+        return cls(h, norm.size, max_k)
+
+    def search(self, queries, k, *, out=None):
+        """Top-k per query; queries = list of word lists or (offsets, words).  Returns (scores, ids) [Q, k]."""
+        if isinstance(queries, tuple):
+            offsets, words = queries
+            offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+            words = np.ascontiguousarray(words, dtype=np.int32)
+        else:
+            offsets, words = pack_queries(queries)
+        q = offsets.size - 1
+        if out is None:
+            scores = np.empty((q, k), dtype=np.float32)
+            ids = np.empty((q, k), dtype=np.int32)
+        else:
+            scores, ids = out
+        if words.size == 0:
+            words = np.zeros(1, dtype=np.int32)
+        status = self._lib.bm25_search(self._handle, n.ptr(offsets, c_int64), n.ptr(words, c_int32), q, k,
+                                       n.ptr(scores, c_float), n.ptr(ids, c_int32))
+        _raise(self._lib, status, self._handle)
+        return scores, ids
+
+    def search_device(self, qoffsets_ptr, words_ptr, q, k, scores_ptr, ids_ptr, stream_ptr=None):
+        """Device-resident Search on raw device pointers (e.g. torch ``data_ptr()``); asynchronous."""
+        status = self._lib.bm25_search_device(self._handle, c_void_p(qoffsets_ptr), c_void_p(words_ptr), q, k,
+                                              c_void_p(scores_ptr), c_void_p(ids_ptr), c_void_p(stream_ptr))
+        _raise(self._lib, status, self._handle)
+
+    def device_status(self):
+        s = ctypes.c_uint32(0)
+        _raise(self._lib, self._lib.bm25_device_status(self._handle, ctypes.byref(s)), self._handle)
+        return s.value
+
+    def info(self):
+        i = n.Info()
+        _raise(self._lib, self._lib.bm25_get_info(self._handle, ctypes.byref(i)), self._handle)
+        return {name: getattr(i, name) for name, _ in n.Info._fields_}
+
+    def last_error(self):
+        return _last_error(self._lib, self._handle)
+
+    def close(self):
+        if self._handle:
+            _raise(self._lib, self._lib.bm25_close(self._handle), self._handle)
+            self._lib.bm25_destroy(self._handle)
+            self._handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            if self._handle:
+                self._lib.bm25_destroy(self._handle)
+                self._handle = None
+        except Exception:
+            pass
+
+
+# --- SDK-shaped facade -------------------------------------------------------
+
+APP_ERR_OK = 0
+# IndexSDK's numeric APP_ERR values (common/ErrorCode.h) are not part of the
+# reference tree; these local values are unpinned.
+APP_ERR_INVALID_PARAM = 2001
+APP_ERR_ILLEGAL_OPERATION = 2002
+APP_ERR_INNER_ERROR = 2003
+_APP = {n.BM25_ERR_INVALID_PARAM: APP_ERR_INVALID_PARAM, n.BM25_ERR_ILLEGAL_OPERATION: APP_ERR_ILLEGAL_OPERATION,
+        n.BM25_ERR_INNER_ERROR: APP_ERR_INNER_ERROR}
+
+
+class Bm25Config:
+    """AscendIndexBm25.h:17-25 with the ACL context/resources replaced by an optional CUDA stream."""
+
+    def __init__(self, deviceId=0, queryCount=8, maxQueryWords=24, topK=10, k1=1.2, stream=None):
+        self.deviceId = deviceId
+        self.queryCount = queryCount
+        self.maxQueryWords = maxQueryWords
+        self.topK = topK
+        self.k1 = k1
+        self.stream = stream
+
+
+class Bm25SearchResult:
+    def __init__(self):
+        self.scores = []
+        self.labels = []
+
+
+class AscendIndexBm25:
+    """Init/Search/Close/GetLastError returning APP_ERR codes (AscendIndexBm25.cpp:33-84)."""
+
+    def __init__(self):
+        self._session = None
+        self._config = None
+        self._error = ('', 0)
+
+    def _invoke(self, fn):
+        self._error = ('', 0)
+        try:
+            fn()
+            return APP_ERR_OK
+        except Bm25Error as e:
+            self._error = (str(e), e.code)
+            return _APP.get(e.status, APP_ERR_INNER_ERROR)
+        except (ValueError, TypeError) as e:
+            self._error = (str(e), 0)
+            return APP_ERR_INVALID_PARAM
+
+    def Init(self, index, config):
+        """index: object with offsets, docs, tf, norm, idf (the reference's lazy Index)."""
+
+        def run():
+            if self._session is not None:
+                raise IllegalOperation(n.BM25_ERR_ILLEGAL_OPERATION, 'BM25 is already initialized; Close before Init')
+            self._session = Bm25Session.from_lazy(
+                index.offsets, index.docs, index.tf, index.norm, index.idf, k1=config.k1,
+                query_capacity=config.queryCount, word_capacity=config.maxQueryWords, max_k=config.topK,
+                device_id=config.deviceId, stream=config.stream)
+            self._config = config
+
+        return self._invoke(run)
+
+    def Search(self, queries, result):
+        """Output is replaced only on success; the batch must hold queryCount queries."""
+
+        def run():
+            if self._session is None:
+                raise IllegalOperation(n.BM25_ERR_ILLEGAL_OPERATION, 'BM25 is not initialized')
+            if len(queries) != self._config.queryCount:
+                raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'Fixed session requires its declared query count')
+            scores, ids = self._session.search(queries, self._config.topK)
+            result.scores = scores.reshape(-1).tolist()
+            result.labels = [int(x) for x in ids.reshape(-1)]
+
+        return self._invoke(run)
+
+    def Close(self):
+        def run():
+            if self._session is not None:
+                self._session.close()
+                self._session = None
+
+        return self._invoke(run)
+
+    def GetLastError(self):
+        return self._error

@@ -1,0 +1,131 @@
+/*
+ * bm25_b200.h -- C ABI of the B200 BM25 Search engine (libbm25_b200.so).
+ *
+ * Plain pointers and sizes only; no CUDA or C++ types in the signatures, so the
+ * library can be bound from C, C++ (AscendIndexBm25.h), Python ctypes or any FFI.
+ *
+ * Ranking contract (same as the reference): per query the K documents with the
+ * highest FP32 score, ties broken by ascending document id; documents with
+ * score zero tie with each other and fill the remaining ranks by ascending id.
+ * Per-document scores are the FP32 sum of the query terms' posting scores added
+ * in query-term order (duplicates added again, unknown word ids skipped), so
+ * they are bit-identical to the reference's CPU search
+ *   feature_retrieval/src/ascendfaiss/test/ascendhost/bm25/reference/cpu_index_search.h:170-190.
+ *
+ * Status codes mirror the IndexSDK APP_ERR mapping of
+ *   feature_retrieval/src/ascendfaiss/ascendhost/include/impl/Bm25ErrorAdapter.h:11-45
+ * (InvalidArgument -> INVALID_PARAM, InvalidState -> ILLEGAL_OPERATION,
+ *  DeviceError/other -> INNER_ERROR).
+ *
+ * Threading: every call on one handle is serialised by a mutex inside the handle
+ * (the reference serialises AscendIndexBm25 the same way, AscendIndexBm25.cpp:26).
+ */
+#ifndef BM25_B200_H
+#define BM25_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BM25_OK 0
+#define BM25_ERR_INVALID_PARAM 1     /* bad input; the handle stays usable */
+#define BM25_ERR_ILLEGAL_OPERATION 2 /* closed, failed or uninitialised handle */
+#define BM25_ERR_INNER_ERROR 3       /* device / runtime failure; the handle is poisoned */
+
+typedef struct bm25_handle bm25_handle;
+
+/* Session configuration (replaces Bm25Config, AscendIndexBm25.h:17-25). */
+typedef struct bm25_options {
+    int32_t device_id;       /* CUDA device ordinal (Bm25Config::deviceId) */
+    int32_t max_k;           /* largest K a Search may ask for (Bm25Config::topK); 1..32 */
+    int64_t query_capacity;  /* largest query batch (Bm25Config::queryCount) */
+    int64_t word_capacity;   /* largest total word count per batch (Bm25Config::maxQueryWords) */
+    int32_t tile_docs;       /* documents per scoring tile; 0 = automatic (power of two, 2048..32768) */
+    int32_t merge_fan_in;    /* lists merged per tree node; 0 = automatic (2..32) */
+    int64_t directory_bytes; /* byte budget of the per-tile posting directory; 0 = automatic */
+    void *stream;            /* borrowed cudaStream_t, or NULL for an engine-owned stream */
+} bm25_options;
+
+/* Fills defaults: device 0, max_k 10, 8 queries, 24 words (the reference's Bm25Config defaults). */
+void bm25_default_options(bm25_options *options);
+
+/*
+ * Creates a resident index from an eager CSC matrix (the bm25s layout,
+ * reference_only/bm25s_original/bm25s/scoring.py:371-410):
+ *   indptr  int64 [vocab + 1], indptr[0] = 0, non-decreasing, indptr[vocab] = M
+ *   indices int32 [M], doc ids in [0, num_docs), strictly ascending within a term
+ *   data    float [M], finite and >= 0 (precomputed per-posting BM25 scores)
+ * The arrays are validated and copied to the device; the caller keeps ownership.
+ * Replaces Init's index upload (AscendIndexBm25.cpp:33-48, large_search.cpp:107-188).
+ */
+int bm25_create(const int64_t *indptr, const int32_t *indices, const float *data, int64_t vocab, int64_t num_docs,
+                const bm25_options *options, bm25_handle **out);
+
+/*
+ * Creates a resident index from the reference's lazy index
+ * (common/bm25/index_data.h:9-42; files of standalone/resident_index.py:12-18):
+ *   term_offsets int64 [vocab + 1], posting_doc_ids int32 [M], posting_tf float [M],
+ *   doc_norm float [num_docs], idf float [vocab]
+ * validated with the reference's rules, then turned into eager FP32 posting scores
+ * on the GPU with the reference's expression (idf * (tf * f32(k1 + 1))) / (tf + norm)
+ * (ops/ascendc/bm25/fused/op_kernel/bm25_fused_score_top_k.cpp:738-739); k1 = 1.2
+ * reproduces the reference's 2.2F literal.
+ */
+int bm25_create_lazy(const int64_t *term_offsets, const int32_t *posting_doc_ids, const float *posting_tf,
+                     const float *doc_norm, const float *idf, int64_t vocab, int64_t num_docs, float k1,
+                     const bm25_options *options, bm25_handle **out);
+
+/*
+ * Search with host buffers (replaces Session::Search, large_search.cpp:190-212):
+ *   qoffsets int64 [q + 1] (qoffsets[0] = 0, non-decreasing), words int32 [qoffsets[q]]
+ *   (the packed layout of common/bm25/search_inputs.h:23-42), 1 <= q <= query_capacity,
+ *   qoffsets[q] <= word_capacity, at most 64 words per query, every word in [0, INT32_MAX - 1];
+ *   1 <= k <= min(max_k, num_docs).
+ * Writes out_scores[q * k] and out_ids[q * k] only on success.  One CUDA-graph
+ * replay: query H2D, scoring + selection + merge tree, result D2H; then the
+ * result is validated on the host (large_search.cpp:64-85).
+ */
+int bm25_search(bm25_handle *handle, const int64_t *qoffsets, const int32_t *words, int64_t q, int32_t k,
+                float *out_scores, int32_t *out_ids);
+
+/*
+ * Device-resident variant for callers that keep queries and results in HBM:
+ * all four arrays are device pointers; work is enqueued on `stream` (a
+ * cudaStream_t, NULL = the handle's stream) and the call returns without
+ * synchronising.  No host validation of the device inputs: words outside the
+ * vocabulary are skipped, negative words set the device status that
+ * bm25_device_status reports.
+ */
+int bm25_search_device(bm25_handle *handle, const int64_t *qoffsets, const int32_t *words, int64_t q, int32_t k,
+                       float *out_scores, int32_t *out_ids, void *stream);
+
+/* Waits for the handle's device-resident Searches and returns their accumulated device status word
+ * (0 = clean), then clears it.  Device-resident Searches only OR into this word. */
+int bm25_device_status(bm25_handle *handle, uint32_t *status);
+
+/* Releases device and pinned resources; idempotent; a failed close can be retried (planned_search.cpp:22-56). */
+int bm25_close(bm25_handle *handle);
+
+/* Closes (if needed) and frees the handle itself. */
+void bm25_destroy(bm25_handle *handle);
+
+/* Last error message of the handle (ErrorInfo, common/bm25/error_info.h:8-20); code = CUDA error or 0. */
+int bm25_last_error(const bm25_handle *handle, char *buffer, size_t length, int64_t *code);
+
+/* Engine facts for reports and tests. */
+typedef struct bm25_info {
+    int64_t num_docs, vocab, postings;
+    int32_t tile_docs, tiles, merge_fan_in, merge_levels;
+    int64_t directory_rows, directory_min_df;
+    int64_t index_bytes, device_bytes;
+    int64_t graph_replays, searches;
+} bm25_info;
+int bm25_get_info(const bm25_handle *handle, bm25_info *info);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BM25_B200_H */
