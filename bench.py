@@ -141,8 +141,11 @@ def setup_dist(gpus):
     return rank, world, local
 
 
-def build_corpus(pkg):
+def build_corpus(pkg, docs=0, vocab=0):
+    import dataclasses
     spec = pkg.CONFIG_SHAPES[WORKLOAD]
+    if docs or vocab:  # reduced copies of the workload, for ncu captures that must stay small
+        spec = dataclasses.replace(spec, docs=docs or spec.docs, vocab=vocab or spec.vocab)
     t = time.perf_counter()
     index = pkg.synthetic_index(spec)
     log(f'corpus: N={index.num_docs} V={index.vocab} M={index.postings} in {time.perf_counter() - t:.1f}s')
@@ -225,6 +228,10 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--tile-docs', type=int, default=0)
     ap.add_argument('--fan-in', type=int, default=0)
+    ap.add_argument('--kernel', type=int, default=0, help='0 streaming (default), 1 one CTA per (query, tile)')
+    ap.add_argument('--stages', type=int, default=0)
+    ap.add_argument('--docs', type=int, default=0, help='reduced corpus for profiling captures (not a bench line)')
+    ap.add_argument('--vocab', type=int, default=0, help='reduced vocabulary for profiling captures')
     args = ap.parse_args()
     if args.impl == 'reference':
         return run_reference(args)
@@ -240,13 +247,14 @@ def main():
         from datetime import timedelta
         dist.init_process_group('nccl', timeout=timedelta(seconds=600), device_id=torch.device('cuda', local))
     pkg = importlib.import_module('bm25-npu_b200')
-    spec, index = build_corpus(pkg)
+    spec, index = build_corpus(pkg, args.docs, args.vocab)
     df = index.df()
     sets = batches(pkg, index, rank)
     t = time.perf_counter()
     session = pkg.Bm25Session.from_lazy(index.offsets, index.docs, index.tf, index.norm, index.idf, k1=spec.k1,
                                         query_capacity=Q, word_capacity=Q * TERMS, max_k=K, device_id=local,
-                                        tile_docs=args.tile_docs, merge_fan_in=args.fan_in)
+                                        tile_docs=args.tile_docs, merge_fan_in=args.fan_in, kernel=args.kernel,
+                                        ring_stages=args.stages)
     info = session.info()
     log(f'engine ready in {time.perf_counter() - t:.1f}s: {info}')
 
@@ -347,18 +355,21 @@ def main():
             'warmup': args.warmup, 'ms_per_step': total_ms / args.steps,
             'p50_ms': percentile(step_ms, 50), 'p95_ms': percentile(step_ms, 95),
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
-            'config': {'workload': WORKLOAD, 'docs': spec.docs, 'vocab': spec.vocab, 'zipf_s': spec.zipf_s,
+            'config': {'workload': WORKLOAD if not (args.docs or args.vocab) else f'{WORKLOAD}_reduced', 'docs': spec.docs, 'vocab': spec.vocab, 'zipf_s': spec.zipf_s,
                        'len_mean': spec.len_mean, 'len_sigma': spec.len_sigma, 'k1': spec.k1, 'b': spec.b,
                        'postings': index.postings, 'queries': Q, 'terms': TERMS, 'k': K,
                        'batches': 'A/B alternating, terms drawn by df', 'l2': 'flushed between steps (256 MiB write)',
                        'tile_docs': info['tile_docs'], 'tiles': info['tiles'], 'merge_fan_in': info['merge_fan_in'],
-                       'merge_levels': info['merge_levels'], 'parallelism': f'replicas x{world} (queries sharded)'},
+                       'merge_levels': info['merge_levels'], 'kernel': info['kernel'],
+                       'ring_stages': info['ring_stages'], 'grid': info['grid'],
+                       'parallelism': f'replicas x{world} (queries sharded)'},
             'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
                     'p50_ms': percentile(host_ms, 50), 'p95_ms': percentile(host_ms, 95),
                     'path': 'bm25_search (C ABI, host buffers): pack + CUDA graph (H2D, kernel, D2H) + validate'},
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                          'frac': achieved / peak, 'traffic': traffic, 'peak_source': peak_kind,
-                         'algorithmic_bytes_per_launch': bytes_avg, 'kernel': 'bm25k::TileSearchKernel'},
+                         'algorithmic_bytes_per_launch': bytes_avg,
+                         'kernel': 'bm25k::StreamSearchKernel' if info['kernel'] == 0 else 'bm25k::TileSearchKernel'},
             'gpu_launches': args.steps,
             'clocks': clock_info,
             'parity': parity,

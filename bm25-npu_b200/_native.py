@@ -28,6 +28,8 @@ class Options(ctypes.Structure):
         ('merge_fan_in', c_int32),
         ('directory_bytes', c_int64),
         ('stream', c_void_p),
+        ('kernel', c_int32),
+        ('ring_stages', c_int32),
     ]
 
 
@@ -46,6 +48,10 @@ class Info(ctypes.Structure):
         ('device_bytes', c_int64),
         ('graph_replays', c_int64),
         ('searches', c_int64),
+        ('kernel', c_int32),
+        ('ring_stages', c_int32),
+        ('grid', c_int32),
+        ('smem_bytes', c_int32),
     ]
 
 

@@ -9,6 +9,7 @@
 // and one CUDA graph per (Q, K) holding H2D -> fused scoring/selection/merge ->
 // D2H.  Search = validate + pack, graph replay, synchronise, validate result.
 #include "bm25_b200.h"
+#include "stream_kernel.cuh"
 #include "tile_kernels.cuh"
 
 #include <cuda_runtime.h>
@@ -133,6 +134,7 @@ class Engine {
         int tile_docs = 0, tiles = 0, fan_in = 32, levels = 0;
         std::vector<int> lists;  // lists per query at each level
         int64_t dir_rows = 0, dir_min_df = 0;
+        int kernel = 0, stages = 0, grid = 0;
     };
 
     Engine(const bm25_options &o, int64_t vocab, int64_t docs, int64_t postings)
@@ -300,6 +302,10 @@ class Engine {
         info->device_bytes = device_bytes_;
         info->graph_replays = replays_;
         info->searches = searches_;
+        info->kernel = plan_.kernel;
+        info->ring_stages = plan_.stages;
+        info->grid = plan_.grid;
+        info->smem_bytes = (int32_t)smem_bytes_;
     }
 
   private:
@@ -320,11 +326,13 @@ class Engine {
 
     void MakePlan()
     {
+        Check(opts_.kernel == 0 || opts_.kernel == 1, "kernel must be 0 (streaming) or 1 (per-tile)");
+        plan_.kernel = opts_.kernel;
         int t = opts_.tile_docs;
         if (t == 0) {
             const int64_t per_sm = (docs_ + 147) / 148;
             t = 2048;
-            while (t < per_sm && t < 16384)
+            while (t < per_sm && t < (plan_.kernel == 0 ? 8192 : 16384))
                 t <<= 1;
         }
         Check(t >= 2048 && t <= 32768 && (t & (t - 1)) == 0, "tile_docs must be a power of two in [2048, 32768]");
@@ -346,6 +354,11 @@ class Engine {
         }
         plan_.fan_in = f;
         plan_.levels = (int)plan_.lists.size();
+        if (plan_.kernel == 0) {
+            const int st = opts_.ring_stages ? opts_.ring_stages : 4;
+            Check(st >= 2 && st <= bm25k::kMaxStages, "ring_stages must be in [2, 8]");
+            plan_.stages = st;
+        }
     }
 
     void AllocIndex()
@@ -418,8 +431,8 @@ class Engine {
         d_out_ = static_cast<unsigned char *>(Alloc(out_bytes_, "cudaMalloc output arena"));
         d_dev_status_ = static_cast<unsigned *>(Alloc(sizeof(unsigned), "cudaMalloc status"));
         Cuda(cudaMemset(d_dev_status_, 0, sizeof(unsigned)), "cudaMemset");
-        // Merge tree: level 0 holds tile lists, the root level is the output.
-        for (int l = 0; l < plan_.levels; ++l) {
+        // Merge tree of the per-tile kernel: level 0 holds tile lists, the root level is the output.
+        for (int l = 0; l < plan_.levels && plan_.kernel == 1; ++l) {
             bm25k::Level lv{};
             lv.n = plan_.lists[l];
             if (lv.n > 1) {
@@ -435,10 +448,39 @@ class Engine {
             }
             levels_.push_back(lv);
         }
-        smem_bytes_ = (size_t)plan_.tile_docs * sizeof(float) + sizeof(bm25k::TileShared);
-        Cuda(cudaFuncSetAttribute(bm25k::TileSearchKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem_bytes_),
-             "cudaFuncSetAttribute");
+        if (plan_.kernel == 1) {
+            smem_bytes_ = (size_t)plan_.tile_docs * sizeof(float) + sizeof(bm25k::TileShared);
+            Cuda(cudaFuncSetAttribute(bm25k::TileSearchKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem_bytes_),
+                 "cudaFuncSetAttribute");
+        } else {
+            smem_bytes_ = (size_t)plan_.tile_docs * sizeof(float) +
+                          2 * (size_t)plan_.stages * bm25k::kChunk * sizeof(int) + sizeof(bm25k::StreamShared);
+            Cuda(cudaFuncSetAttribute(bm25k::StreamSearchKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem_bytes_),
+                 "cudaFuncSetAttribute");
+            int per_sm = 0, sms = 0;
+            Cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bm25k::StreamSearchKernel,
+                                                               bm25k::kStreamThreads, smem_bytes_),
+                 "occupancy");
+            Cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "SM count");
+            Check(per_sm >= 1, "tile_docs / ring_stages exceed the shared memory of one SM");
+            plan_.grid = per_sm * sms;
+            sms_ = sms;
+            const size_t qc = (size_t)opts_.query_capacity, tiles_z = (size_t)plan_.tiles;
+            // worst case: every warp of every tile appends max_k candidates
+            cand_cap_ = (long long)tiles_z * bm25k::kConsumerWarps * opts_.max_k;
+            ctrl_ = static_cast<bm25k::StreamCtrl *>(Alloc(sizeof(bm25k::StreamCtrl), "cudaMalloc ctrl"));
+            threshold_ = static_cast<unsigned *>(Alloc(qc * sizeof(unsigned), "cudaMalloc threshold"));
+            cand_count_ = static_cast<unsigned *>(Alloc(qc * sizeof(unsigned), "cudaMalloc cand count"));
+            cand_scores_ = static_cast<float *>(Alloc(qc * cand_cap_ * sizeof(float), "cudaMalloc candidates"));
+            cand_ids_ = static_cast<int *>(Alloc(qc * cand_cap_ * sizeof(int), "cudaMalloc candidates"));
+            plan_entries_ = static_cast<bm25k::PlanEntry *>(
+                Alloc(std::max<size_t>(1, opts_.word_capacity) * tiles_z * sizeof(bm25k::PlanEntry), "cudaMalloc plan"));
+            Cuda(cudaMemset(ctrl_, 0, sizeof(bm25k::StreamCtrl)), "cudaMemset");
+            Cuda(cudaMemset(threshold_, 0, qc * sizeof(unsigned)), "cudaMemset");
+            Cuda(cudaMemset(cand_count_, 0, qc * sizeof(unsigned)), "cudaMemset");
+        }
         Cuda(cudaDeviceSynchronize(), "index preparation");
     }
 
@@ -454,6 +496,7 @@ class Engine {
         a.dir_stride = plan_.tiles + 1;
         a.qoffsets = (const long long *)qoffsets;
         a.words = words;
+        a.word_cap = std::max<int64_t>(1, opts_.word_capacity);
         a.vocab = (int)vocab_;
         a.num_docs = (int)docs_;
         a.tile_docs = plan_.tile_docs;
@@ -461,14 +504,52 @@ class Engine {
         a.k = k;
         a.fan_in = plan_.fan_in;
         a.levels = plan_.levels;
-        for (int l = 0; l < plan_.levels; ++l)
+        for (int l = 0; l < (int)levels_.size(); ++l)
             a.lv[l] = levels_[l];
         a.out_scores = out_scores;
         a.out_ids = out_ids;
         a.status = status;
-        dim3 grid(plan_.tiles, q);
-        bm25k::TileSearchKernel<<<grid, bm25k::kThreads, smem_bytes_, s>>>(a);
-        Cuda(cudaGetLastError(), "tile kernel launch");
+        if (plan_.kernel == 1) {
+            dim3 grid(plan_.tiles, q);
+            bm25k::TileSearchKernel<<<grid, bm25k::kThreads, smem_bytes_, s>>>(a);
+        } else {
+            bm25k::StreamArgs sa{};
+            sa.indptr = a.indptr;
+            sa.indices = a.indices;
+            sa.data = a.data;
+            sa.dir_row = a.dir_row;
+            sa.dir = a.dir;
+            sa.dir_stride = a.dir_stride;
+            sa.qoffsets = a.qoffsets;
+            sa.words = a.words;
+            sa.vocab = a.vocab;
+            sa.num_docs = a.num_docs;
+            sa.tile_docs = a.tile_docs;
+            sa.tiles = a.tiles;
+            sa.k = k;
+            sa.q = q;
+            sa.word_cap = a.word_cap;
+            sa.plan = plan_entries_;
+            sa.threshold = threshold_;
+            sa.cand_count = cand_count_;
+            sa.cand_scores = cand_scores_;
+            sa.cand_ids = cand_ids_;
+            sa.cand_cap = cand_cap_;
+            sa.ctrl = ctrl_;
+            sa.stages = plan_.stages;
+            sa.out_scores = out_scores;
+            sa.out_ids = out_ids;
+            sa.status = status;
+            const int plan_grid = (int)std::max<int64_t>(1, std::min<int64_t>(opts_.word_capacity, (int64_t)sms_ * 4));
+            bm25k::PlanKernel<<<plan_grid, bm25k::kPlanThreads, 0, s>>>(sa);
+            Cuda(cudaGetLastError(), "plan kernel launch");
+            const int grid = (int)std::min<long long>(plan_.grid, ((long long)q * plan_.tiles + bm25k::kTaskBatch - 1) /
+                                                                      bm25k::kTaskBatch);
+            bm25k::StreamSearchKernel<<<std::max(grid, 1), bm25k::kStreamThreads, smem_bytes_, s>>>(sa);
+            Cuda(cudaGetLastError(), "stream kernel launch");
+            bm25k::FinalSelectKernel<<<q, bm25k::kFinalThreads, 0, s>>>(sa);
+        }
+        Cuda(cudaGetLastError(), "search kernel launch");
     }
 
     size_t IdOffset(int q, int k) const { return Align32((size_t)q * k * 4); }
@@ -590,6 +671,13 @@ class Engine {
     void *h_in_ = nullptr, *h_out_ = nullptr;
     unsigned char *d_in_ = nullptr, *d_out_ = nullptr;
     unsigned *d_dev_status_ = nullptr;
+    bm25k::StreamCtrl *ctrl_ = nullptr;
+    unsigned *threshold_ = nullptr, *cand_count_ = nullptr;
+    float *cand_scores_ = nullptr;
+    int *cand_ids_ = nullptr;
+    long long cand_cap_ = 0;
+    bm25k::PlanEntry *plan_entries_ = nullptr;
+    int sms_ = 148;
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs_;
     bool closed_ = false, failed_ = false;
     int64_t replays_ = 0, searches_ = 0;

@@ -1,0 +1,867 @@
+// Persistent, warp-specialised BM25 Search kernels for sm_100a (the default path).
+//
+// Contract of the reference's fused scoring + merge operators
+//   feature_retrieval/src/ascendfaiss/ops/ascendc/bm25/fused/op_kernel/bm25_fused_score_top_k.cpp:637-936
+//   feature_retrieval/src/ascendfaiss/ops/ascendc/bm25/merge/op_kernel/bm25_top_k_merge.cpp:10-98
+// (exact per-query top-K, score desc / id asc, zero-score fill by id), organised
+// for a B200 as three launches:
+//
+// PlanKernel -- one CTA per query word resolves the word's posting sub-range in
+//   every tile (per-tile directory for long lists; a shared-memory lower_bound
+//   over short lists), written as absolute [b, e) pairs to plan[word][tile].
+//
+// StreamSearchKernel -- persistent: each CTA has one producer warp and eight
+//   consumer warps.  Tasks are (query, tile) pairs in tile-major order, so every
+//   query has tiles in the first wave and gets a score threshold early.
+//   * The producer takes kTaskBatch tasks per work-counter atomic, reads their
+//     plan entries and the queries' running thresholds lane-parallel, skips
+//     tasks without postings, and streams the postings of the others -- doc ids
+//     and FP32 scores -- as chunks of up to kChunk postings into a shared-memory
+//     ring with 1-D bulk async copies (cp.async.bulk ... mbarrier::complete_tx,
+//     no multicast), up to `stages` chunks ahead, across task boundaries.
+//   * Consumer warp w owns documents [w * R, (w + 1) * R) of the tile
+//     (R = tile_docs / 8).  It waits on each ring stage itself, finds its slice
+//     of the chunk (one term's postings, sorted by document) with a
+//     warp-parallel lower_bound, adds it into its own part of the shared-memory
+//     tile row and releases the stage.  Only warp w touches a document of its
+//     region and it consumes the ring in order, so each document's FP32 sum is
+//     built in query-term order with no CTA barrier at all.
+//   * At the end of a task each warp keeps its region's top-K among scores at
+//     or above max(query threshold, a lower bound on the region's K-th score
+//     from its lanes' maxima), appends them to the query's candidate buffer,
+//     publishes its region's K-th score as the query's new threshold (K region
+//     documents reach it, so the global K-th does too) and clears its region.
+//     A global top-K document is in the top-K of every subset that contains
+//     it, so every filter keeps it.
+//
+// FinalSelectKernel -- one CTA per query ranks the query's candidates exactly,
+//   adds the zero-score fill, writes the K results and resets the query's
+//   buffer and threshold for the next Search.
+//
+// Every wait in the streaming kernel is on an mbarrier and bounded by a clock
+// budget; on expiry the kernel records kStatusTimeout, drains its own copies
+// (bounded) and returns.
+#pragma once
+#include "tile_kernels.cuh"
+
+namespace bm25k {
+
+constexpr int kConsumerWarps = 8;
+constexpr int kConsumerThreads = kConsumerWarps * 32;
+constexpr int kStreamThreads = kConsumerThreads + 32;  // + one producer warp
+constexpr int kChunk = 2048;                           // postings per ring stage
+constexpr int kMaxStages = 8;
+constexpr int kTaskBatch = 8;                          // tasks per work-counter atomic
+constexpr int kPlanCache = 4;                          // plan entries a producer lane keeps in registers
+constexpr int kWarpSurvCap = 64;                       // region candidates ranked exactly per warp
+constexpr int kFinalThreads = 256;
+constexpr int kSurvCap = 512;                          // candidates ranked exactly per query
+constexpr long long kWaitBudget = 4000000000LL;        // cycles (~2 s) before a wait gives up
+constexpr int kPlanThreads = 256;
+constexpr int kPlanSmemIds = 4096;                     // short lists up to this length are searched in smem
+
+enum : uint32_t {
+    kStatusTimeout = 16u,       // a bounded wait gave up
+    kStatusCandOverflow = 32u,  // a query's candidate buffer was too small
+};
+
+enum : int {
+    kFirstOfTask = 1,
+    kLastOfTask = 4,
+    kStop = 8,
+};
+
+struct StreamCtrl {
+    unsigned next;  // next task to hand out
+    unsigned done;  // producers that found no more tasks
+};
+
+struct PlanEntry {
+    long long b, e;
+};
+
+struct StreamArgs {
+    const long long *indptr;
+    const int *indices;
+    const float *data;
+    const int *dir_row;
+    const int *dir;
+    long long dir_stride;
+    const long long *qoffsets;
+    const int *words;
+    int vocab, num_docs, tile_docs, tiles, k, q;
+    long long word_cap;     // rows of `plan`; query words beyond it are rejected
+    PlanEntry *plan;        // [word][tile]
+    unsigned *threshold;    // [Q] running K-th score bits (0 = none yet)
+    unsigned *cand_count;   // [Q] candidates appended
+    float *cand_scores;     // [Q][cand_cap]
+    int *cand_ids;          // [Q][cand_cap]
+    long long cand_cap;
+    StreamCtrl *ctrl;
+    int stages;
+    float *out_scores;
+    int *out_ids;
+    unsigned *status;
+};
+
+struct __align__(16) StageMeta {
+    long long base;  // posting position of ring element 0
+    int lo, hi;      // valid ring elements [lo, hi) of the current term
+    int count;       // elements copied (multiple of 4)
+    int flags;
+    int q, tile;
+    float thr;       // the query's running threshold when the task was fetched
+};
+
+struct StreamShared {
+    unsigned long long full[kMaxStages];
+    unsigned long long empty[kMaxStages];
+    StageMeta meta[kMaxStages];
+    float wbuf_s[kConsumerWarps][kWarpSurvCap];
+    int wbuf_i[kConsumerWarps][kWarpSurvCap];
+    float wsel_s[kConsumerWarps][32];
+    int wsel_i[kConsumerWarps][32];
+    unsigned bad;
+    int abort;
+};
+
+// ---- PTX wrappers ----------------------------------------------------------
+
+__device__ __forceinline__ unsigned SmemAddr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void MbarInit(unsigned long long *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(SmemAddr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void MbarArriveExpectTx(unsigned long long *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(SmemAddr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void MbarArrive(unsigned long long *bar)
+{
+    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(SmemAddr(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool MbarTryWait(unsigned long long *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n"
+        ".reg .pred p;\n"
+        "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n"
+        "selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(ok)
+        : "r"(SmemAddr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait; false when the budget ran out or another role aborted.
+__device__ __forceinline__ bool MbarWait(unsigned long long *bar, unsigned parity, volatile int *abort)
+{
+    if (MbarTryWait(bar, parity))
+        return true;
+    const long long t0 = clock64();
+    for (;;) {
+        if (MbarTryWait(bar, parity))
+            return true;
+        if (*abort)
+            return false;
+        if (clock64() - t0 > kWaitBudget) {
+            *abort = 1;
+            return false;
+        }
+    }
+}
+
+// Whole-warp bounded wait: lane 0 waits, then every lane acquires the completed phase.
+__device__ __forceinline__ bool WarpWait(unsigned long long *bar, unsigned parity, volatile int *abort, int lane)
+{
+    int ok = 1;
+    if (lane == 0)
+        ok = MbarWait(bar, parity, abort) ? 1 : 0;
+    ok = __shfl_sync(kFull, ok, 0);
+    if (ok)
+        (void)MbarTryWait(bar, parity);  // complete already: returns at once, acquiring for this lane
+    return ok != 0;
+}
+
+// 1-D bulk copy global -> shared, completion counted on `bar` (no multicast).
+__device__ __forceinline__ void BulkLoad(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     SmemAddr(dst)),
+                 "l"(src), "r"(bytes), "r"(SmemAddr(bar))
+                 : "memory");
+}
+
+// ---- warp top-K with the K-th entry cached in registers (tie fallbacks) --------
+
+// Lane l holds the l-th best (score, id) seen by the warp (l < k <= 32), best
+// first; empty slots hold (-1, kNoId).  (ts, ti) caches lane k-1's entry so an
+// offer that inserts nothing costs one compare and one ballot.
+struct WarpTopK {
+    float ls, ts;
+    int li, ti;
+    __device__ __forceinline__ void Reset()
+    {
+        ls = ts = -1.0f;
+        li = ti = kNoId;
+    }
+    __device__ __forceinline__ void Offer(float cs, int ci, bool has, int k, int lane)
+    {
+        unsigned pending = __ballot_sync(kFull, has && Better(cs, ci, ts, ti));
+        while (pending) {
+            const int src = __ffs(pending) - 1;
+            pending &= pending - 1;
+            const float s = __shfl_sync(kFull, cs, src);
+            const int id = __shfl_sync(kFull, ci, src);
+            if (Better(s, id, ts, ti)) {  // uniform
+                const bool above = lane < k && Better(ls, li, s, id);
+                const int pos = __popc(__ballot_sync(kFull, above));
+                const float us = __shfl_up_sync(kFull, ls, 1);
+                const int ui = __shfl_up_sync(kFull, li, 1);
+                if (lane < k && lane > pos) {
+                    ls = us;
+                    li = ui;
+                }
+                if (lane == pos) {
+                    ls = s;
+                    li = id;
+                }
+                ts = __shfl_sync(kFull, ls, k - 1);
+                ti = __shfl_sync(kFull, li, k - 1);
+            }
+        }
+    }
+};
+
+// ---- per-warp region selection ---------------------------------------------------
+
+// Descending bitonic sort across the warp; returns this lane's element.
+__device__ __forceinline__ float WarpSortDesc(float v, int lane)
+{
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const float o = __shfl_xor_sync(kFull, v, stride);
+            const bool desc = (lane & size) == 0;
+            const bool lower = (lane & stride) == 0;
+            v = (lower == desc) ? fmaxf(v, o) : fminf(v, o);
+        }
+    }
+    return v;
+}
+
+// Warp w's candidates of the task: its region's top-k among scores >= thr
+// (and > 0), sorted best first into wsel[w] with global ids.  Returns their
+// number; *kth receives the region's k-th score when it is known exactly
+// (k candidates, none filtered below it), else 0.
+__device__ __forceinline__ int WarpRegionSelect(StreamShared &sh, const float *region, int region_docs, float thr,
+                                                int k, int base_id, int lane, int warp, float *kth)
+{
+    const float4 *reg4 = reinterpret_cast<const float4 *>(region);
+    const int r4 = region_docs / 4;  // multiple of 32: warp-uniform trip counts
+    float tmax = 0.0f;
+    int pass = 0;
+    for (int i = lane; i < r4; i += 32) {
+        const float4 x = reg4[i];
+        tmax = fmaxf(tmax, fmaxf(fmaxf(x.x, x.y), fmaxf(x.z, x.w)));
+        pass += (x.x >= thr && x.x > 0.0f) + (x.y >= thr && x.y > 0.0f) + (x.z >= thr && x.z > 0.0f) +
+                (x.w >= thr && x.w > 0.0f);
+    }
+    int total = __reduce_add_sync(kFull, pass);
+    *kth = 0.0f;
+    if (total == 0)
+        return 0;
+    float tau = thr;
+    if (total > k) {
+        // k-th largest lane maximum: k lanes each hold a score >= it
+        const float bound = __shfl_sync(kFull, WarpSortDesc(tmax, lane), k - 1);
+        if (bound > tau) {
+            tau = bound;
+            pass = 0;
+            for (int i = lane; i < r4; i += 32) {
+                const float4 x = reg4[i];
+                pass += (x.x >= tau && x.x > 0.0f) + (x.y >= tau && x.y > 0.0f) + (x.z >= tau && x.z > 0.0f) +
+                        (x.w >= tau && x.w > 0.0f);
+            }
+            total = __reduce_add_sync(kFull, pass);
+        }
+    }
+    int n = 0;
+    if (total <= kWarpSurvCap) {
+        // each lane writes its survivors at its exclusive prefix offset
+        int at = pass;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(kFull, at, o);
+            if (lane >= o)
+                at += v;
+        }
+        at -= pass;
+        if (pass) {
+            for (int i = lane; i < r4; i += 32) {
+                const float4 x = reg4[i];
+                const float xs[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    if (xs[c] >= tau && xs[c] > 0.0f) {
+                        sh.wbuf_s[warp][at] = xs[c];
+                        sh.wbuf_i[warp][at] = base_id + 4 * i + c;
+                        ++at;
+                    }
+            }
+        }
+        __syncwarp();
+        for (int i = lane; i < total; i += 32) {
+            const float s = sh.wbuf_s[warp][i];
+            const int id = sh.wbuf_i[warp][i];
+            int rank = 0;
+            for (int t = 0; t < total; ++t)
+                rank += Better(sh.wbuf_s[warp][t], sh.wbuf_i[warp][t], s, id);
+            if (rank < k) {
+                sh.wsel_s[warp][rank] = s;
+                sh.wsel_i[warp][rank] = id;
+            }
+        }
+        n = min(total, k);
+    } else {
+        // ties at the top overflow the buffer: insertion select over the region
+        WarpTopK top;
+        top.Reset();
+        for (int i = lane; i < r4; i += 32) {
+            const float4 x = reg4[i];
+            const int id0 = base_id + 4 * i;
+            top.Offer(x.x, id0 + 0, x.x > 0.0f && x.x >= tau, k, lane);
+            top.Offer(x.y, id0 + 1, x.y > 0.0f && x.y >= tau, k, lane);
+            top.Offer(x.z, id0 + 2, x.z > 0.0f && x.z >= tau, k, lane);
+            top.Offer(x.w, id0 + 3, x.w > 0.0f && x.w >= tau, k, lane);
+        }
+        n = __popc(__ballot_sync(kFull, lane < k && top.li != kNoId));
+        if (lane < n) {
+            sh.wsel_s[warp][lane] = top.ls;
+            sh.wsel_i[warp][lane] = top.li;
+        }
+    }
+    __syncwarp();
+    if (n == k)
+        *kth = sh.wsel_s[warp][k - 1];
+    return n;
+}
+
+// ---- plan kernel -------------------------------------------------------------
+
+__device__ __forceinline__ long long LowerBoundSmem(const int *ids, long long n, long long target)
+{
+    long long lo = 0, hi = n;
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if ((long long)ids[mid] < target)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ long long LowerBoundGlobal(const int *ids, long long lo, long long hi, long long target)
+{
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if ((long long)__ldg(ids + mid) < target)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// plan[w][tile] = absolute posting range of query word w inside tile (empty for
+// unknown or negative words).  Grid-stride over the batch's words.
+__global__ void __launch_bounds__(kPlanThreads) PlanKernel(const StreamArgs a)
+{
+    __shared__ int ids[kPlanSmemIds];
+    long long total = a.qoffsets[a.q];
+    if (total < 0 || total > a.word_cap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0)
+            atomicOr(a.status, kStatusBadQuery);
+        total = total < 0 ? 0 : a.word_cap;
+    }
+    for (long long w = blockIdx.x; w < total; w += gridDim.x) {
+        const int term = a.words[w];
+        PlanEntry *out = a.plan + w * a.tiles;
+        if (term < 0 || term >= a.vocab) {
+            if (term < 0 && threadIdx.x == 0)
+                atomicOr(a.status, kStatusBadWord);
+            for (int t = threadIdx.x; t < a.tiles; t += kPlanThreads)
+                out[t] = PlanEntry{0, 0};
+            continue;
+        }
+        const long long s = a.indptr[term], e = a.indptr[term + 1];
+        const int r = a.dir_row[term];
+        if (r >= 0) {
+            const int *d = a.dir + (long long)r * a.dir_stride;
+            for (int t = threadIdx.x; t < a.tiles; t += kPlanThreads)
+                out[t] = PlanEntry{s + d[t], s + d[t + 1]};
+        } else if (e - s <= kPlanSmemIds) {
+            const int n = (int)(e - s);
+            __syncthreads();  // the previous word's readers are done with ids[]
+            for (int p = threadIdx.x; p < n; p += kPlanThreads)
+                ids[p] = __ldg(a.indices + s + p);
+            __syncthreads();
+            for (int t = threadIdx.x; t < a.tiles; t += kPlanThreads) {
+                const long long lo = (long long)t * a.tile_docs;
+                out[t] = PlanEntry{s + LowerBoundSmem(ids, n, lo), s + LowerBoundSmem(ids, n, lo + a.tile_docs)};
+            }
+        } else {
+            for (int t = threadIdx.x; t < a.tiles; t += kPlanThreads) {
+                const long long lo = (long long)t * a.tile_docs;
+                out[t] = PlanEntry{LowerBoundGlobal(a.indices, s, e, lo),
+                                   LowerBoundGlobal(a.indices, s, e, lo + a.tile_docs)};
+            }
+        }
+    }
+}
+
+// ---- the streaming kernel -------------------------------------------------------
+
+// First index in ids[a, b) (ascending) whose value is >= target; all lanes.
+__device__ __forceinline__ int WarpLowerBound(const int *ids, int a, int b, long long target, int lane)
+{
+    while (b - a > 32) {
+        const int step = (b - a + 31) >> 5;
+        const int p = a + lane * step;
+        const bool less = p < b && (long long)ids[p] < target;
+        const int c = __popc(__ballot_sync(kFull, less));
+        if (c == 0)
+            return a;
+        const int na = a + (c - 1) * step + 1;
+        b = min(b, a + c * step);
+        a = na;
+    }
+    const bool less = a + lane < b && (long long)ids[a + lane] < target;
+    return a + __popc(__ballot_sync(kFull, less));
+}
+
+__global__ void __launch_bounds__(kStreamThreads, 1) StreamSearchKernel(const StreamArgs a)
+{
+    extern __shared__ __align__(128) unsigned char stream_smem[];
+    float *row = reinterpret_cast<float *>(stream_smem);
+    int *ring_ids = reinterpret_cast<int *>(stream_smem + (size_t)a.tile_docs * 4);
+    float *ring_vals = reinterpret_cast<float *>(ring_ids + (size_t)a.stages * kChunk);
+    StreamShared &sh = *reinterpret_cast<StreamShared *>(ring_vals + (size_t)a.stages * kChunk);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    if (tid == 0) {
+        for (int i = 0; i < a.stages; ++i) {
+            MbarInit(&sh.full[i], 1);
+            MbarInit(&sh.empty[i], kConsumerWarps);
+        }
+        sh.bad = 0;
+        sh.abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    {
+        float4 *row4 = reinterpret_cast<float4 *>(row);
+        for (int i = tid; i < a.tile_docs / 4; i += kStreamThreads)
+            row4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncthreads();
+    volatile int *abort = &sh.abort;
+    const unsigned total = (unsigned)a.q * (unsigned)a.tiles;
+
+    if (warp == kConsumerWarps) {
+        // ================= producer warp =================
+        unsigned long long g = 0;  // ring entries issued
+        unsigned bad = 0;
+        bool dead = false;
+
+        // Claims the next ring stage (lane 0 waits, the warp learns the outcome).
+        auto claim = [&](int &st) -> bool {
+            st = (int)(g % (unsigned long long)a.stages);
+            const unsigned long long k = g / (unsigned long long)a.stages;
+            int ok = 1;
+            if (k > 0 && lane == 0)
+                ok = MbarWait(&sh.empty[st], (unsigned)((k - 1) & 1), abort) ? 1 : 0;
+            return __shfl_sync(kFull, ok, 0) != 0;
+        };
+
+        while (!dead) {
+            unsigned base = 0;
+            if (lane == 0)
+                base = atomicAdd(&a.ctrl->next, (unsigned)kTaskBatch);
+            base = __shfl_sync(kFull, base, 0);
+            if (base >= total)
+                break;
+            const unsigned task = base + lane;
+            const bool valid = lane < kTaskBatch && task < total;
+            int q = 0, tile = 0, nt = 0, last = -1;
+            long long qb = 0;
+            float thr = 0.0f;
+            PlanEntry pc[kPlanCache];
+#pragma unroll
+            for (int s = 0; s < kPlanCache; ++s)
+                pc[s] = PlanEntry{0, 0};
+            if (valid) {
+                tile = (int)(task / (unsigned)a.q);
+                q = (int)(task % (unsigned)a.q);
+                thr = __uint_as_float(__ldcg(a.threshold + q));
+                qb = a.qoffsets[q];
+                long long n = a.qoffsets[q + 1] - qb;
+                if (n < 0 || n > kMaxTerms || qb < 0 || qb + n > a.word_cap) {
+                    bad |= kStatusBadQuery;
+                    n = 0;
+                }
+                nt = (int)n;
+#pragma unroll
+                for (int s = 0; s < kPlanCache; ++s)
+                    if (s < nt)
+                        pc[s] = a.plan[(qb + s) * a.tiles + tile];
+#pragma unroll
+                for (int s = 0; s < kPlanCache; ++s)
+                    if (s < nt && pc[s].e > pc[s].b)
+                        last = s;
+                for (int s = kPlanCache; s < nt; ++s) {
+                    const PlanEntry pe = a.plan[(qb + s) * a.tiles + tile];
+                    if (pe.e > pe.b)
+                        last = s;
+                }
+            }
+            // tasks without postings contribute nothing: skip them
+            unsigned work = __ballot_sync(kFull, valid && last >= 0);
+            while (work && !dead) {
+                const int src = __ffs(work) - 1;
+                work &= work - 1;
+                const int tq = __shfl_sync(kFull, q, src);
+                const int ttile = __shfl_sync(kFull, tile, src);
+                const long long tqb = __shfl_sync(kFull, qb, src);
+                const int tlast = __shfl_sync(kFull, last, src);
+                const float tthr = __shfl_sync(kFull, thr, src);
+                bool first = true;
+                for (int slot = 0; slot <= tlast && !dead; ++slot) {
+                    long long b, e;
+                    if (slot < kPlanCache) {
+                        long long mb = 0, me = 0;
+#pragma unroll
+                        for (int s = 0; s < kPlanCache; ++s)
+                            if (s == slot) {
+                                mb = pc[s].b;
+                                me = pc[s].e;
+                            }
+                        b = __shfl_sync(kFull, mb, src);
+                        e = __shfl_sync(kFull, me, src);
+                    } else {
+                        const PlanEntry pe = a.plan[(tqb + slot) * a.tiles + ttile];
+                        b = pe.b;
+                        e = pe.e;
+                    }
+                    if (b >= e)
+                        continue;
+                    const long long a0 = b & ~3LL, a1 = (e + 3) & ~3LL;
+                    for (long long c0 = a0; c0 < a1;) {
+                        const long long c1 = min(c0 + (long long)kChunk, a1);
+                        int st;
+                        if (!claim(st)) {
+                            dead = true;
+                            break;
+                        }
+                        if (lane == 0) {
+                            StageMeta &m = sh.meta[st];
+                            m.base = c0;
+                            m.count = (int)(c1 - c0);
+                            m.lo = (int)max(0LL, b - c0);
+                            m.hi = (int)min((long long)m.count, e - c0);
+                            m.flags = (first ? kFirstOfTask : 0) | (slot == tlast && c1 == a1 ? kLastOfTask : 0);
+                            m.q = tq;
+                            m.tile = ttile;
+                            m.thr = tthr;
+                            const unsigned bytes = (unsigned)(c1 - c0) * 4u;
+                            MbarArriveExpectTx(&sh.full[st], 2u * bytes);
+                            BulkLoad(ring_ids + (size_t)st * kChunk, a.indices + c0, bytes, &sh.full[st]);
+                            BulkLoad(ring_vals + (size_t)st * kChunk, a.data + c0, bytes, &sh.full[st]);
+                        }
+                        __syncwarp();
+                        first = false;
+                        ++g;
+                        c0 = c1;
+                    }
+                }
+            }
+        }
+        if (!dead) {
+            int st;
+            if (claim(st)) {
+                if (lane == 0) {
+                    StageMeta &m = sh.meta[st];
+                    m.base = 0;
+                    m.lo = m.hi = m.count = 0;
+                    m.flags = kStop;
+                    m.q = m.tile = 0;
+                    m.thr = 0.0f;
+                    MbarArrive(&sh.full[st]);
+                }
+                __syncwarp();
+                ++g;
+            } else {
+                dead = true;
+            }
+        }
+        if (lane == 0) {
+            if (bad)
+                atomicOr(a.status, bad);
+            // the last producer to run dry resets the work counter for the next Search
+            const unsigned d = atomicAdd(&a.ctrl->done, 1u);
+            if (d == gridDim.x - 1) {
+                a.ctrl->next = 0u;
+                a.ctrl->done = 0u;
+            }
+        }
+        if (dead && lane == 0) {
+            // drain copies still in flight into this CTA's ring (bounded)
+            for (unsigned long long h = (g > (unsigned long long)a.stages ? g - a.stages : 0); h < g; ++h) {
+                const int st = (int)(h % (unsigned long long)a.stages);
+                const long long t0 = clock64();
+                while (!MbarTryWait(&sh.full[st], (unsigned)((h / a.stages) & 1)) && clock64() - t0 < kWaitBudget) {
+                }
+            }
+        }
+        return;
+    }
+
+    // ================= consumer warps (independent) =================
+    const int region_docs = a.tile_docs / kConsumerWarps;
+    float *region = row + warp * region_docs;
+    unsigned long long g = 0;
+    unsigned bad = 0;
+    int q = 0, tile = 0;
+    float thr = 0.0f;
+    for (;;) {
+        const int st = (int)(g % (unsigned long long)a.stages);
+        const unsigned parity = (unsigned)((g / (unsigned long long)a.stages) & 1);
+        if (!WarpWait(&sh.full[st], parity, abort, lane))
+            break;
+        const StageMeta m = sh.meta[st];
+        if (m.flags & kStop)
+            break;
+        if (m.flags & kFirstOfTask) {
+            q = m.q;
+            tile = m.tile;
+            thr = m.thr;
+        }
+        // this warp's slice of the chunk: postings of documents in its region
+        const long long lo = (long long)tile * a.tile_docs;
+        const long long dlo = lo + (long long)warp * region_docs, dhi = dlo + region_docs;
+        const int *ids = ring_ids + (size_t)st * kChunk;
+        const float *vals = ring_vals + (size_t)st * kChunk;
+        if (m.hi > m.lo && (long long)ids[m.hi - 1] >= dlo && (long long)ids[m.lo] < dhi) {
+            const int s0 = WarpLowerBound(ids, m.lo, m.hi, dlo, lane);
+            const int s1 = WarpLowerBound(ids, s0, m.hi, dhi, lane);
+#pragma unroll 4
+            for (int i = s0 + lane; i < s1; i += 32) {
+                const long long d = (long long)ids[i] - lo;
+                const float sum = row[d] + vals[i];
+                row[d] = sum;
+                if (!(sum <= FLT_MAX))
+                    bad |= kStatusOverflow;
+            }
+        }
+        __syncwarp();
+        if (lane == 0)
+            MbarArrive(&sh.empty[st]);
+        ++g;
+        if (!(m.flags & kLastOfTask))
+            continue;
+
+        // ---- end of task: this warp's candidates, straight to the query's buffer ----
+        float kth;
+        const int n = WarpRegionSelect(sh, region, region_docs, thr, a.k, (int)dlo, lane, warp, &kth);
+        if (n > 0) {
+            unsigned at = 0;
+            if (lane == 0) {
+                at = atomicAdd(a.cand_count + q, (unsigned)n);
+                if (kth > thr)
+                    atomicMax(a.threshold + q, __float_as_uint(kth));
+            }
+            at = __shfl_sync(kFull, at, 0);
+            if (lane < n) {
+                if ((long long)at + lane < a.cand_cap) {
+                    const long long off = (long long)q * a.cand_cap + at + lane;
+                    a.cand_scores[off] = sh.wsel_s[warp][lane];
+                    a.cand_ids[off] = sh.wsel_i[warp][lane];
+                } else {
+                    bad |= kStatusCandOverflow;
+                }
+            }
+        }
+        {
+            float4 *reg4 = reinterpret_cast<float4 *>(region);
+            for (int i = lane; i < region_docs / 4; i += 32)
+                reg4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        __syncwarp();
+    }
+    bad = __reduce_or_sync(kFull, bad);
+    if (lane == 0 && (bad || *abort))
+        atomicOr(a.status, bad | (*abort ? kStatusTimeout : 0u));
+}
+
+// ---- final per-query selection ---------------------------------------------------
+
+// Exact top-k of one query's candidates: bound from per-thread maxima (m warps
+// with j threads each holding a score >= tau, j * m >= k), raised to the
+// query's threshold; survivors ranked exactly (insertion select when ties
+// overflow the buffer); zero-score fill; then the query's state is reset.
+__global__ void __launch_bounds__(kFinalThreads) FinalSelectKernel(const StreamArgs a)
+{
+    constexpr int kWarps = kFinalThreads / 32;
+    __shared__ float surv_s[kSurvCap];
+    __shared__ int surv_i[kSurvCap];
+    __shared__ float sel_s[32];
+    __shared__ int sel_i[32];
+    __shared__ float wl_s[kWarps][32];
+    __shared__ int wl_i[kWarps][32];
+    __shared__ float wv[kWarps];
+    __shared__ unsigned surv_count;
+    __shared__ int sel_count;
+    const int q = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int k = a.k;
+    const unsigned appended = __ldcg(a.cand_count + q);
+    const int n = (int)min((long long)appended, a.cand_cap);
+    if (tid == 0 && (long long)appended > a.cand_cap)
+        atomicOr(a.status, kStatusCandOverflow);
+    const float floor = __uint_as_float(__ldcg(a.threshold + q));
+    const float *cs = a.cand_scores + (long long)q * a.cand_cap;
+    const int *ci = a.cand_ids + (long long)q * a.cand_cap;
+
+    float tmax = 0.0f;
+    for (int i = tid; i < n; i += kFinalThreads)
+        tmax = fmaxf(tmax, __ldcg(cs + i));
+    const int j = (k + kWarps - 1) / kWarps;
+    float v = tmax, jth = 0.0f;
+    for (int r = 0; r < j; ++r) {
+        float mx = v;
+#pragma unroll
+        for (int o = 16; o; o >>= 1)
+            mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, o));
+        jth = mx;
+        const unsigned who = __ballot_sync(kFull, v == mx);
+        if (lane == __ffs(who) - 1)
+            v = -1.0f;
+    }
+    if (lane == 0)
+        wv[warp] = fmaxf(jth, 0.0f);
+    if (tid == 0)
+        surv_count = 0;
+    __syncthreads();
+    const int m = (k + j - 1) / j;
+    float w[kWarps];
+#pragma unroll
+    for (int i = 0; i < kWarps; ++i)
+        w[i] = wv[i];
+    float tau = 0.0f;
+    for (int r = 0; r < m; ++r) {
+        int best = 0;
+#pragma unroll
+        for (int i = 1; i < kWarps; ++i)
+            if (w[i] > w[best])
+                best = i;
+        tau = w[best];
+#pragma unroll
+        for (int i = 0; i < kWarps; ++i)
+            if (i == best)
+                w[i] = -2.0f;
+    }
+    tau = fmaxf(tau, floor);
+    for (int i = tid; i < n; i += kFinalThreads) {
+        const float s = __ldcg(cs + i);
+        if (s > 0.0f && s >= tau) {
+            const unsigned at = atomicAdd(&surv_count, 1u);
+            if (at < (unsigned)kSurvCap) {
+                surv_s[at] = s;
+                surv_i[at] = __ldcg(ci + i);
+            }
+        }
+    }
+    __syncthreads();
+    const unsigned c = surv_count;
+    if (c <= (unsigned)kSurvCap) {
+        for (unsigned i = tid; i < c; i += kFinalThreads) {
+            const float s = surv_s[i];
+            const int id = surv_i[i];
+            int rank = 0;
+            for (unsigned t = 0; t < c; ++t)
+                rank += Better(surv_s[t], surv_i[t], s, id);
+            if (rank < k) {
+                sel_s[rank] = s;
+                sel_i[rank] = id;
+            }
+        }
+        if (tid == 0)
+            sel_count = (int)min(c, (unsigned)k);
+    } else {
+        WarpTopK top;
+        top.Reset();
+        for (int base = warp * 32; base < n; base += kFinalThreads) {
+            const int i = base + lane;
+            float s = 0.0f;
+            int id = kNoId;
+            if (i < n) {
+                s = __ldcg(cs + i);
+                id = __ldcg(ci + i);
+            }
+            top.Offer(s, id, i < n && s > 0.0f && s >= tau, k, lane);
+        }
+        wl_s[warp][lane] = top.ls;
+        wl_i[warp][lane] = top.li;
+        __syncthreads();
+        if (warp == 0) {
+            top.Reset();
+            for (int w2 = 0; w2 < kWarps; ++w2)
+                top.Offer(wl_s[w2][lane], wl_i[w2][lane], wl_i[w2][lane] != kNoId, k, lane);
+            const int cnt = __popc(__ballot_sync(kFull, lane < k && top.li != kNoId));
+            if (lane < cnt) {
+                sel_s[lane] = top.ls;
+                sel_i[lane] = top.li;
+            }
+            if (lane == 0)
+                sel_count = cnt;
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const int cnt = sel_count;
+        float ls = -1.0f;
+        int li = kNoId;
+        if (lane < cnt) {
+            ls = sel_s[lane];
+            li = sel_i[lane];
+        }
+        int r = cnt;
+        for (int d = 0; r < k && d < a.num_docs; ++d) {  // zero-score fill, smallest ids first
+            if (!__any_sync(kFull, li == d)) {
+                if (lane == r) {
+                    ls = 0.0f;
+                    li = d;
+                }
+                ++r;
+            }
+        }
+        if (lane < k) {
+            a.out_scores[(long long)q * k + lane] = ls;
+            a.out_ids[(long long)q * k + lane] = li;
+        }
+        if (lane == 0) {
+            a.cand_count[q] = 0u;
+            a.threshold[q] = 0u;
+        }
+    }
+}
+
+} // namespace bm25k

@@ -64,6 +64,7 @@ struct TileArgs {
     long long dir_stride;
     const long long *qoffsets;  // [Q + 1]
     const int *words;
+    long long word_cap;         // words readable; a query reaching beyond is rejected
     int vocab, num_docs, tile_docs, tiles, k, fan_in, levels;
     Level lv[kMaxLevels];
     float *out_scores;  // [Q][K]
@@ -328,7 +329,7 @@ __global__ void __launch_bounds__(kThreads, 2) TileSearchKernel(const TileArgs a
         sh.bad = 0;
         sh.nonempty = 0;
     }
-    if (nq < 0 || nq > kMaxTerms) {
+    if (nq < 0 || nq > kMaxTerms || qb < 0 || qb + nq > a.word_cap) {
         if (tid == 0)
             sh.bad = kStatusBadQuery;
         nq = 0;

@@ -47,6 +47,8 @@ typedef struct bm25_options {
     int32_t merge_fan_in;    /* lists merged per tree node; 0 = automatic (2..32) */
     int64_t directory_bytes; /* byte budget of the per-tile posting directory; 0 = automatic */
     void *stream;            /* borrowed cudaStream_t, or NULL for an engine-owned stream */
+    int32_t kernel;          /* 0 = persistent streaming kernel (bulk-async posting ring), 1 = one CTA per (query, tile) */
+    int32_t ring_stages;     /* posting-ring depth of the streaming kernel, 2..8; 0 = automatic */
 } bm25_options;
 
 /* Fills defaults: device 0, max_k 10, 8 queries, 24 words (the reference's Bm25Config defaults). */
@@ -122,6 +124,7 @@ typedef struct bm25_info {
     int64_t directory_rows, directory_min_df;
     int64_t index_bytes, device_bytes;
     int64_t graph_replays, searches;
+    int32_t kernel, ring_stages, grid, smem_bytes;
 } bm25_info;
 int bm25_get_info(const bm25_handle *handle, bm25_info *info);
 

@@ -20,7 +20,11 @@ def _oracle(oracle_mod, index, data, offsets, words, k):
     return oracle_mod.search(index.offsets, index.docs, data, index.num_docs, offsets, words, k)
 
 
-def test_config_8192_docs_q8x3_k10(pkg, oracle_mod, cuda_ok):
+KERNELS = pytest.mark.parametrize('kernel', [0, 1], ids=['stream', 'per_tile'])
+
+
+@KERNELS
+def test_config_8192_docs_q8x3_k10(pkg, oracle_mod, cuda_ok, kernel):
     """8192 docs, V 30,000 Zipf(1.1), lognormal mean 60, k1 1.5, b 0.75, 8 x 3 df-sampled terms, K 10."""
     spec = pkg.CONFIG_SHAPES['synthetic_8192']
     index = pkg.synthetic_index(spec)
@@ -28,14 +32,17 @@ def test_config_8192_docs_q8x3_k10(pkg, oracle_mod, cuda_ok):
     for seed in (1, 2, 3):
         offsets, words = pkg.synthetic_queries(index.offsets, 8, 3, 3, seed)
         ref = _oracle(oracle_mod, index, data, offsets, words, 10)
-        with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs) as s:
+        with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, kernel=kernel) as s:
             assert_same_topk(*s.search((offsets, words), 10), *ref, 'eager')
-        with pkg.Bm25Session.from_lazy(index.offsets, index.docs, index.tf, index.norm, index.idf, k1=spec.k1) as s:
+        with pkg.Bm25Session.from_lazy(index.offsets, index.docs, index.tf, index.norm, index.idf, k1=spec.k1,
+                                       kernel=kernel) as s:
             assert_same_topk(*s.search((offsets, words), 10), *ref, 'lazy')
 
 
-@pytest.mark.parametrize('tile_docs,fan_in', [(2048, 2), (2048, 4), (4096, 32), (0, 0), (32768, 8)])
-def test_tiles_and_merge_tree(pkg, oracle_mod, corpus, cuda_ok, tile_docs, fan_in):
+@KERNELS
+@pytest.mark.parametrize('tile_docs,fan_in,stages', [(2048, 2, 2), (2048, 4, 3), (4096, 32, 8), (0, 0, 0),
+                                                     (32768, 8, 4)])
+def test_tiles_and_merge_tree(pkg, oracle_mod, corpus, cuda_ok, tile_docs, fan_in, stages, kernel):
     spec, index, data = corpus
     rng = np.random.default_rng(tile_docs + fan_in)
     rows = mixed_queries(index.vocab, rng, 24, 0, 12)
@@ -44,7 +51,8 @@ def test_tiles_and_merge_tree(pkg, oracle_mod, corpus, cuda_ok, tile_docs, fan_i
     rows[2] = []                 # zero fill only
     offsets, words = pack(rows)
     with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, query_capacity=32,
-                                  word_capacity=512, max_k=32, tile_docs=tile_docs, merge_fan_in=fan_in) as s:
+                                  word_capacity=512, max_k=32, tile_docs=tile_docs, merge_fan_in=fan_in,
+                                  kernel=kernel, ring_stages=stages) as s:
         info = s.info()
         assert info['tiles'] == -(-index.num_docs // info['tile_docs'])
         for k in (1, 7, 10, 32):
@@ -52,31 +60,35 @@ def test_tiles_and_merge_tree(pkg, oracle_mod, corpus, cuda_ok, tile_docs, fan_i
             assert_same_topk(*got, *_oracle(oracle_mod, index, data, offsets, words, k), f'k={k}')
 
 
-def test_directory_and_scan_paths_agree(pkg, oracle_mod, corpus, cuda_ok):
+@KERNELS
+def test_directory_and_scan_paths_agree(pkg, oracle_mod, corpus, cuda_ok, kernel):
     spec, index, data = corpus
     rng = np.random.default_rng(5)
     offsets, words = pack(mixed_queries(index.vocab, rng, 16, 1, 10))
     ref = _oracle(oracle_mod, index, data, offsets, words, 10)
     for budget in (1, 1 << 30):  # 1 byte: every list is counted inside the CTA; 1 GiB: directory for long lists
         with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, query_capacity=16,
-                                      word_capacity=256, tile_docs=2048, directory_bytes=budget) as s:
+                                      word_capacity=256, tile_docs=2048, directory_bytes=budget,
+                                      kernel=kernel) as s:
             assert_same_topk(*s.search((offsets, words), 10), *ref, f'budget={budget}')
 
 
-def test_reference_edge_queries(pkg, oracle_mod, corpus, cuda_ok):
+@KERNELS
+def test_reference_edge_queries(pkg, oracle_mod, corpus, cuda_ok, kernel):
     spec, index, data = corpus
     with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, query_capacity=7,
-                                  word_capacity=128, max_k=32, tile_docs=4096) as s:
+                                  word_capacity=128, max_k=32, tile_docs=4096, kernel=kernel) as s:
         for rows in (EDGE_A, EDGE_B, EDGE_A, [[]] * 3, EDGE_B):
             offsets, words = pack(rows)
             for k in (1, 3, 10, 32):
                 assert_same_topk(*s.search((offsets, words), k), *_oracle(oracle_mod, index, data, offsets, words, k))
 
 
-def test_empty_bootstrap_is_zero_fill(pkg, corpus, cuda_ok):
+@KERNELS
+def test_empty_bootstrap_is_zero_fill(pkg, corpus, cuda_ok, kernel):
     """Search(empty) returns score 0 and ids 0..K-1 (large_search.cpp:184-187)."""
     spec, index, data = corpus
-    with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, max_k=10) as s:
+    with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, max_k=10, kernel=kernel) as s:
         scores, ids = s.search([[]] * 8, 10)
         assert (scores == 0).all() and (ids == np.arange(10)[None, :]).all()
 
@@ -114,13 +126,15 @@ def test_invalid_index_rejected(pkg, cuda_ok):
                                  np.array([1, np.nan, 1], np.float32), 4)
 
 
-def test_device_resident_search_matches_host(pkg, oracle_mod, corpus, cuda_ok):
+@KERNELS
+def test_device_resident_search_matches_host(pkg, oracle_mod, corpus, cuda_ok, kernel):
     import torch
     spec, index, data = corpus
     rng = np.random.default_rng(9)
     offsets, words = pack(mixed_queries(index.vocab, rng, 8, 1, 6, oov=False))
     ref = _oracle(oracle_mod, index, data, offsets, words, 10)
-    with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, word_capacity=64) as s:
+    with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, word_capacity=64,
+                                  kernel=kernel) as s:
         d_off = torch.from_numpy(offsets).cuda()
         d_words = torch.from_numpy(words).cuda()
         d_scores = torch.empty((8, 10), dtype=torch.float32, device='cuda')
@@ -134,14 +148,15 @@ def test_device_resident_search_matches_host(pkg, oracle_mod, corpus, cuda_ok):
         assert_same_topk(*s.search((offsets, words), 10), *ref, 'host after device')
 
 
-def test_alternating_batches_replay(pkg, oracle_mod, corpus, cuda_ok):
+@KERNELS
+def test_alternating_batches_replay(pkg, oracle_mod, corpus, cuda_ok, kernel):
     """A/B alternation through cached graphs, as the reference's benchmark does (benchmark_common.h:51-107)."""
     spec, index, data = corpus
     a = pkg.synthetic_queries(index.offsets, 8, 3, 3, 101)
     b = pkg.synthetic_queries(index.offsets, 8, 3, 3, 102)
     ra = _oracle(oracle_mod, index, data, *a, 10)
     rb = _oracle(oracle_mod, index, data, *b, 10)
-    with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs) as s:
+    with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, kernel=kernel) as s:
         for _ in range(5):
             assert_same_topk(*s.search(a, 10), *ra, 'A')
             assert_same_topk(*s.search(b, 10), *rb, 'B')
