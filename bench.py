@@ -288,8 +288,9 @@ def main():
         for i in range(args.warmup):
             device_step(i)
         stream.synchronize()
-        if session.device_status() != 0:
-            raise RuntimeError('device status set during warm-up')
+        status = session.device_status()
+        if status != 0:
+            raise RuntimeError(f'device status {status:#x} set during warm-up')
         starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
         ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
         clocks = Clocks(local)
@@ -304,8 +305,9 @@ def main():
             ends[i].record(stream)
         torch.cuda.synchronize()
         clock_info = clocks.stop()
-    if session.device_status() != 0:
-        raise RuntimeError('device status set during the timed region')
+    status = session.device_status()
+    if status != 0:
+        raise RuntimeError(f'device status {status:#x} set during the timed region')
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = sum(step_ms)
     if world > 1:
