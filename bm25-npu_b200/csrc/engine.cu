@@ -892,3 +892,164 @@ int bm25_get_info(const bm25_handle *h, bm25_info *info)
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Search with no device allocation (bm25_search_csc_static).
+//
+// For callers that hold their CSC index in device memory they manage
+// themselves and may not allocate: code running where cudaMalloc is not
+// allowed or not wanted (inside a framework that owns every byte of device
+// memory through its own pool, a serving loop that forbids allocation after
+// start-up, or a process whose allocator is locked down).  All per-search
+// scratch lives in the fixed array below; every GPU that loads this library
+// holds it until the process exits.
+#include "static_search.cuh"
+
+namespace {
+constexpr size_t kStaticScratchBytes = size_t(16) << 20;  // 16 MiB, the largest Search this path accepts
+constexpr size_t kStaticHeadBytes = 256;                  // work counter + status word
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+struct StaticDevice {
+    bool ready = false;
+    unsigned char *scratch = nullptr;  // device address of g_static_scratch on this device
+    int sms = 0;
+    int grid[3] = {0, 0, 0};  // streaming-kernel CTAs for tile_docs 2048, 4096, 8192
+};
+std::mutex g_static_mutex;
+StaticDevice g_static_devices[64];
+
+size_t AlignUp(size_t n, size_t a) { return (n + a - 1) / a * a; }
+size_t StaticSmem(int tile_docs)
+{
+    return (size_t)tile_docs * sizeof(float) + 2 * (size_t)4 * bm25k::kChunk * sizeof(int) +
+           sizeof(bm25k::StreamShared);
+}
+
+// The dynamic shared memory cap is one value per kernel, shared with sessions:
+// raise it when this Search needs more, never lower it.
+void StaticRaiseSmem(size_t bytes)
+{
+    cudaFuncAttributes attr{};
+    bm25b200::Cuda(cudaFuncGetAttributes(&attr, bm25k::StreamSearchKernel), "cudaFuncGetAttributes");
+    if ((size_t)attr.maxDynamicSharedSizeBytes < bytes)
+        bm25b200::Cuda(cudaFuncSetAttribute(bm25k::StreamSearchKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)bytes),
+                       "cudaFuncSetAttribute");
+}
+
+// Once per device, with that device current: the device address of the
+// scratch array (its host-side name is only a stand-in), kernel attributes and
+// occupancy.  Must not run inside a stream capture.
+void StaticSetup(int device, StaticDevice &d)
+{
+    if (d.ready)
+        return;
+    void *ptr = nullptr;
+    bm25b200::Cuda(cudaGetSymbolAddress(&ptr, g_static_scratch), "cudaGetSymbolAddress(static scratch)");
+    bm25b200::Cuda(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+    StaticRaiseSmem(StaticSmem(8192));
+    for (int i = 0; i < 3; ++i) {
+        int per_sm = 0;
+        bm25b200::Cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bm25k::StreamSearchKernel,
+                                                                     bm25k::kStreamThreads, StaticSmem(2048 << i)),
+                       "occupancy");
+        d.grid[i] = std::max(1, per_sm) * d.sms;
+    }
+    d.scratch = static_cast<unsigned char *>(ptr);
+    d.ready = true;
+}
+} // namespace
+
+extern "C" int bm25_search_csc_static(const int64_t *indptr, const int32_t *indices, const float *data,
+                                      int64_t vocab, int64_t num_docs, const int64_t *qoffsets,
+                                      const int32_t *words, int64_t q, int64_t num_words, int32_t k,
+                                      float *out_scores, int32_t *out_ids, void *stream, int32_t device_id)
+{
+    return Invoke(
+        [&] {
+            using bm25b200::Check;
+            using bm25b200::Cuda;
+            Check(indptr && indices && data && qoffsets && words && out_scores && out_ids, "Null device buffer");
+            Check(reinterpret_cast<uintptr_t>(indices) % 16 == 0 && reinterpret_cast<uintptr_t>(data) % 16 == 0,
+                  "indices and data must be 16-byte aligned");
+            Check(vocab >= 1 && vocab < INT32_MAX && num_docs >= 1 && num_docs <= INT32_MAX,
+                  "Empty or oversized index");
+            Check(q >= 1 && q <= 65535 && num_words >= 0 && num_words <= 16777216, "Query batch out of range");
+            Check(k >= 1 && k <= bm25k::kMaxSmallK && k <= num_docs, "K outside [1, min(32, N)]");
+            Check(device_id >= 0 && device_id < 64, "device_id out of range");
+            int tile = 2048, ti = 0;
+            const int64_t per_sm = (num_docs + 147) / 148;
+            while (tile < per_sm && tile < 8192) {
+                tile <<= 1;
+                ++ti;
+            }
+            const int64_t tiles = (num_docs + tile - 1) / tile;
+            const long long cand_cap = tiles * bm25k::kConsumerWarps * k;
+            // scratch layout: head | threshold[q] | cand_count[q] | cand_scores[q][cap] | cand_ids[q][cap] | plan
+            const size_t off_thr = kStaticHeadBytes;
+            const size_t off_cnt = AlignUp(off_thr + (size_t)q * 4, 16);
+            const size_t off_cs = AlignUp(off_cnt + (size_t)q * 4, 16);
+            const size_t off_ci = AlignUp(off_cs + (size_t)q * cand_cap * 4, 16);
+            const size_t off_plan = AlignUp(off_ci + (size_t)q * cand_cap * 4, 16);
+            const size_t need = off_plan + (size_t)std::max<int64_t>(1, num_words) * tiles * sizeof(bm25k::PlanEntry);
+            if (need > kStaticScratchBytes)
+                throw bm25b200::InvalidArgument("Search needs " + std::to_string(need) +
+                                                " bytes of scratch; the allocation-free path holds " +
+                                                std::to_string(kStaticScratchBytes));
+            Cuda(cudaSetDevice(device_id), "cudaSetDevice");
+            StaticDevice *dev;
+            {
+                std::lock_guard<std::mutex> guard(g_static_mutex);
+                dev = &g_static_devices[device_id];
+                StaticSetup(device_id, *dev);
+            }
+            StaticRaiseSmem(StaticSmem(tile));
+            unsigned char *base = dev->scratch;
+            cudaStream_t s = static_cast<cudaStream_t>(stream);
+            bm25k::StreamArgs sa{};
+            sa.indptr = reinterpret_cast<const long long *>(indptr);
+            sa.indices = indices;
+            sa.data = data;
+            sa.qoffsets = reinterpret_cast<const long long *>(qoffsets);
+            sa.words = words;
+            sa.vocab = (int)vocab;
+            sa.num_docs = (int)num_docs;
+            sa.tile_docs = tile;
+            sa.tiles = (int)tiles;
+            sa.k = k;
+            sa.q = (int)q;
+            sa.word_cap = std::max<int64_t>(1, num_words);
+            sa.ctrl = reinterpret_cast<bm25k::StreamCtrl *>(base);
+            sa.status = reinterpret_cast<unsigned *>(base + 64);
+            sa.threshold = reinterpret_cast<unsigned *>(base + off_thr);
+            sa.cand_count = reinterpret_cast<unsigned *>(base + off_cnt);
+            sa.cand_scores = reinterpret_cast<float *>(base + off_cs);
+            sa.cand_ids = reinterpret_cast<int *>(base + off_ci);
+            sa.cand_cap = cand_cap;
+            sa.plan = reinterpret_cast<bm25k::PlanEntry *>(base + off_plan);
+            sa.stages = 4;
+            sa.out_scores = out_scores;
+            sa.out_ids = out_ids;
+            // The array keeps the previous call's contents: clear what must start at zero.
+            Cuda(cudaMemsetAsync(base, 0, off_cs, s), "clear static scratch");
+            const int plan_grid = (int)std::max<int64_t>(1, std::min<int64_t>(num_words, (int64_t)dev->sms * 4));
+            bm25k::PlanNoDirectoryKernel<<<plan_grid, bm25k::kPlanThreads, 0, s>>>(sa);
+            Cuda(cudaGetLastError(), "plan kernel launch");
+            const int grid = (int)std::min<long long>(dev->grid[ti], (q * tiles + bm25k::kTaskBatch - 1) /
+                                                                         bm25k::kTaskBatch);
+            bm25k::StreamSearchKernel<<<std::max(grid, 1), bm25k::kStreamThreads, StaticSmem(tile), s>>>(sa);
+            Cuda(cudaGetLastError(), "stream kernel launch");
+            bm25k::FinalSelectKernel<<<(int)q, bm25k::kFinalThreads, 0, s>>>(sa);
+            Cuda(cudaGetLastError(), "final kernel launch");
+            unsigned status = 0;
+            Cuda(cudaMemcpyAsync(&status, sa.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "status D2H");
+            Cuda(cudaStreamSynchronize(s), "complete static Search");
+            if (status && !(status & ~(unsigned)(bm25k::kStatusBadWord | bm25k::kStatusBadQuery)))
+                throw bm25b200::InvalidArgument("Invalid word ID or query offsets in the device query packet, status=" +
+                                                std::to_string(status));
+            if (status)
+                throw bm25b200::DeviceError(0, "Device reported invalid Search state, status=" + std::to_string(status));
+        },
+        g_create_error, g_create_code);
+}

@@ -117,6 +117,33 @@ void bm25_destroy(bm25_handle *handle);
 /* Last error message of the handle (ErrorInfo, common/bm25/error_info.h:8-20); code = CUDA error or 0. */
 int bm25_last_error(const bm25_handle *handle, char *buffer, size_t length, int64_t *code);
 
+/*
+ * Search without any device allocation, for callers that cannot call
+ * cudaMalloc (a framework that owns all device memory through its own pool, a
+ * serving loop that forbids allocation after start-up): the caller holds the
+ * eager CSC index (same rules as bm25_create) and the query packet in device
+ * memory and passes device pointers for the outputs.  No counterpart in the
+ * reference.
+ *   - indices and data must be 16-byte aligned and readable up to the next
+ *     multiple of 4 elements past indptr[vocab];
+ *   - num_words = qoffsets[q] (at most 64 words per query); 1 <= k <= min(32, num_docs);
+ *   - all scratch comes from one fixed 16 MiB device array inside this library
+ *     (held by every GPU that loads it until exit); a Search needing more
+ *     (roughly q * ceil(num_docs / 8192) * (256 * k + 16 * num_words / q) bytes)
+ *     is rejected with BM25_ERR_INVALID_PARAM;
+ *   - work runs on `stream` (a cudaStream_t) on device `device_id`; the call
+ *     waits for it and returns the device status;
+ *   - the first call on a device looks up the array's device address and sets
+ *     kernel attributes: make it before any stream capture;
+ *   - every call shares the array, so calls that overlap on the GPU (other
+ *     streams, other host threads) race: serialise them;
+ *   - error details: bm25_last_error(NULL, ...).
+ */
+int bm25_search_csc_static(const int64_t *indptr, const int32_t *indices, const float *data, int64_t vocab,
+                           int64_t num_docs, const int64_t *qoffsets, const int32_t *words, int64_t q,
+                           int64_t num_words, int32_t k, float *out_scores, int32_t *out_ids, void *stream,
+                           int32_t device_id);
+
 /* Engine facts for reports and tests. */
 typedef struct bm25_info {
     int64_t num_docs, vocab, postings;
