@@ -70,6 +70,8 @@ SIGNATURES = {
     'bm25_destroy': (None, [c_void_p]),
     'bm25_last_error': (c_int, [c_void_p, c_char_p, c_size_t, POINTER(c_int64)]),
     'bm25_get_info': (c_int, [c_void_p, POINTER(Info)]),
+    'bm25_kernel_timing': (c_int, [c_void_p, c_int32]),
+    'bm25_kernel_times': (c_int, [c_void_p, POINTER(c_float), c_int64, POINTER(c_int64)]),
     'bm25_search_csc_static': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_int64,
                                        c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_int32]),
 }

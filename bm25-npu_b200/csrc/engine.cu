@@ -53,6 +53,18 @@ static void Cuda(cudaError_t e, const char *what)
         throw DeviceError((int64_t)e, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// A kernel's dynamic shared memory cap is one value per process and device,
+// shared by every session: raise it to what this session needs, never lower it
+// under a session created earlier with larger tiles.
+static void RaiseSmemCap(const void *kernel, size_t bytes)
+{
+    cudaFuncAttributes attr{};
+    Cuda(cudaFuncGetAttributes(&attr, kernel), "cudaFuncGetAttributes");
+    if ((size_t)attr.maxDynamicSharedSizeBytes < bytes)
+        Cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
+             "cudaFuncSetAttribute");
+}
+
 static size_t Align32(size_t n) { return (n + 31) & ~size_t(31); }
 
 constexpr int kPad = 256; // zero elements after the posting arrays for 128-bit tail loads
@@ -251,12 +263,53 @@ class Engine {
             cudaStream_t s = stream ? stream : stream_;
             Cuda(cudaStreamWaitEvent(s, done_, 0), "cudaStreamWaitEvent");
             ++searches_;
+            marking_ = !timing_.empty();
             Launch((int)q, k, qoffsets, words, out_scores, out_ids, d_dev_status_, s);
+            if (marking_)
+                ++timed_;
+            marking_ = false;
             Cuda(cudaEventRecord(done_, s), "cudaEventRecord");
         } catch (...) {
             failed_ = true;
             throw;
         }
+    }
+
+    // Event timing of the main search kernel (StreamSearchKernel or
+    // TileSearchKernel) for device-resident Searches: a ring of event pairs
+    // recorded on the launching stream around that one launch.
+    void KernelTiming(bool enable)
+    {
+        RequireUsable();
+        Cuda(cudaSetDevice(device_), "cudaSetDevice");
+        if (enable && timing_.empty()) {
+            timing_.resize(2 * kTimingRing);
+            for (auto &e : timing_)
+                Cuda(cudaEventCreate(&e), "cudaEventCreate");
+        } else if (!enable) {
+            Cuda(cudaStreamWaitEvent(stream_, done_, 0), "cudaStreamWaitEvent");
+            Cuda(cudaStreamSynchronize(stream_), "timing drain");
+            DestroyTiming();
+        }
+        timed_ = 0;
+    }
+
+    int64_t KernelTimes(float *ms, int64_t capacity)
+    {
+        RequireUsable();
+        Check(!timing_.empty(), "Kernel timing is not enabled");
+        Check(ms != nullptr || capacity == 0, "Null output");
+        Cuda(cudaSetDevice(device_), "cudaSetDevice");
+        const int64_t n = std::min<int64_t>(timed_, kTimingRing);
+        const int64_t first = timed_ - n;
+        int64_t out = 0;
+        for (int64_t i = first; i < timed_ && out < capacity; ++i) {
+            const size_t slot = (size_t)(i % kTimingRing);
+            Cuda(cudaEventSynchronize(timing_[2 * slot + 1]), "cudaEventSynchronize");
+            Cuda(cudaEventElapsedTime(&ms[out++], timing_[2 * slot], timing_[2 * slot + 1]), "cudaEventElapsedTime");
+        }
+        timed_ = 0;
+        return out;
     }
 
     uint32_t DeviceStatus()
@@ -450,15 +503,11 @@ class Engine {
         }
         if (plan_.kernel == 1) {
             smem_bytes_ = (size_t)plan_.tile_docs * sizeof(float) + sizeof(bm25k::TileShared);
-            Cuda(cudaFuncSetAttribute(bm25k::TileSearchKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem_bytes_),
-                 "cudaFuncSetAttribute");
+            RaiseSmemCap(reinterpret_cast<const void *>(bm25k::TileSearchKernel), smem_bytes_);
         } else {
             smem_bytes_ = (size_t)plan_.tile_docs * sizeof(float) +
                           2 * (size_t)plan_.stages * bm25k::kChunk * sizeof(int) + sizeof(bm25k::StreamShared);
-            Cuda(cudaFuncSetAttribute(bm25k::StreamSearchKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem_bytes_),
-                 "cudaFuncSetAttribute");
+            RaiseSmemCap(reinterpret_cast<const void *>(bm25k::StreamSearchKernel), smem_bytes_);
             int per_sm = 0, sms = 0;
             Cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bm25k::StreamSearchKernel,
                                                                bm25k::kStreamThreads, smem_bytes_),
@@ -511,7 +560,9 @@ class Engine {
         a.status = status;
         if (plan_.kernel == 1) {
             dim3 grid(plan_.tiles, q);
+            MarkKernel(0, s);
             bm25k::TileSearchKernel<<<grid, bm25k::kThreads, smem_bytes_, s>>>(a);
+            MarkKernel(1, s);
         } else {
             bm25k::StreamArgs sa{};
             sa.indptr = a.indptr;
@@ -545,8 +596,10 @@ class Engine {
             Cuda(cudaGetLastError(), "plan kernel launch");
             const int grid = (int)std::min<long long>(plan_.grid, ((long long)q * plan_.tiles + bm25k::kTaskBatch - 1) /
                                                                       bm25k::kTaskBatch);
+            MarkKernel(0, s);
             bm25k::StreamSearchKernel<<<std::max(grid, 1), bm25k::kStreamThreads, smem_bytes_, s>>>(sa);
             Cuda(cudaGetLastError(), "stream kernel launch");
+            MarkKernel(1, s);
             bm25k::FinalSelectKernel<<<q, bm25k::kFinalThreads, 0, s>>>(sa);
         }
         Cuda(cudaGetLastError(), "search kernel launch");
@@ -554,6 +607,20 @@ class Engine {
 
     size_t IdOffset(int q, int k) const { return Align32((size_t)q * k * 4); }
     size_t StatusOffset(int q, int k) const { return Align32(IdOffset(q, k) + (size_t)q * k * 4); }
+
+    void MarkKernel(int which, cudaStream_t s)
+    {
+        if (marking_)
+            Cuda(cudaEventRecord(timing_[2 * (size_t)(timed_ % kTimingRing) + which], s), "cudaEventRecord");
+    }
+
+    void DestroyTiming()
+    {
+        for (auto e : timing_)
+            cudaEventDestroy(e);
+        timing_.clear();
+        timed_ = 0;
+    }
 
     cudaGraphExec_t GraphFor(int q, int k)
     {
@@ -643,6 +710,7 @@ class Engine {
         if (h_out_)
             cudaFreeHost(h_out_);
         h_in_ = h_out_ = nullptr;
+        DestroyTiming();
         if (done_)
             cudaEventDestroy(done_);
         done_ = nullptr;
@@ -681,6 +749,10 @@ class Engine {
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs_;
     bool closed_ = false, failed_ = false;
     int64_t replays_ = 0, searches_ = 0;
+    static constexpr int64_t kTimingRing = 4096;
+    std::vector<cudaEvent_t> timing_;  // [start, end] per ring slot
+    int64_t timed_ = 0;
+    bool marking_ = false;
 };
 
 } // namespace bm25b200
@@ -847,6 +919,35 @@ int bm25_device_status(bm25_handle *h, uint32_t *status)
         h->error, h->code);
 }
 
+int bm25_kernel_timing(bm25_handle *h, int32_t enable)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            h->engine->KernelTiming(enable != 0);
+        },
+        h->error, h->code);
+}
+
+int bm25_kernel_times(bm25_handle *h, float *ms, int64_t capacity, int64_t *count)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            bm25b200::Check(count != nullptr, "Null count output");
+            *count = h->engine->KernelTimes(ms, capacity);
+        },
+        h->error, h->code);
+}
+
 int bm25_close(bm25_handle *h)
 {
     if (!h)
@@ -926,16 +1027,9 @@ size_t StaticSmem(int tile_docs)
            sizeof(bm25k::StreamShared);
 }
 
-// The dynamic shared memory cap is one value per kernel, shared with sessions:
-// raise it when this Search needs more, never lower it.
 void StaticRaiseSmem(size_t bytes)
 {
-    cudaFuncAttributes attr{};
-    bm25b200::Cuda(cudaFuncGetAttributes(&attr, bm25k::StreamSearchKernel), "cudaFuncGetAttributes");
-    if ((size_t)attr.maxDynamicSharedSizeBytes < bytes)
-        bm25b200::Cuda(cudaFuncSetAttribute(bm25k::StreamSearchKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)bytes),
-                       "cudaFuncSetAttribute");
+    bm25b200::RaiseSmemCap(reinterpret_cast<const void *>(bm25k::StreamSearchKernel), bytes);
 }
 
 // Once per device, with that device current: the device address of the

@@ -164,6 +164,18 @@ class Bm25Session:
                                               c_void_p(scores_ptr), c_void_p(ids_ptr), c_void_p(stream_ptr))
         _raise(self._lib, status, self._handle)
 
+    def kernel_timing(self, enable=True):
+        """Record CUDA events around the main search kernel of each ``search_device`` call."""
+        _raise(self._lib, self._lib.bm25_kernel_timing(self._handle, int(bool(enable))), self._handle)
+
+    def kernel_times(self, capacity=4096):
+        """Durations (ms) of the main search kernel for the timed Searches since the last read."""
+        ms = np.zeros(capacity, dtype=np.float32)
+        count = c_int64(0)
+        _raise(self._lib, self._lib.bm25_kernel_times(self._handle, n.ptr(ms, c_float), capacity,
+                                                      ctypes.byref(count)), self._handle)
+        return ms[:count.value].copy()
+
     def device_status(self):
         s = ctypes.c_uint32(0)
         _raise(self._lib, self._lib.bm25_device_status(self._handle, ctypes.byref(s)), self._handle)

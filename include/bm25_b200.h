@@ -144,6 +144,17 @@ int bm25_search_csc_static(const int64_t *indptr, const int32_t *indices, const 
                            int64_t num_words, int32_t k, float *out_scores, int32_t *out_ids, void *stream,
                            int32_t device_id);
 
+/*
+ * Measurement hook, no counterpart in the reference: with timing enabled,
+ * every bm25_search_device records a CUDA event pair on its stream around the
+ * main search kernel (the streaming kernel, or the per-tile kernel).
+ * bm25_kernel_times waits for them and returns the durations in ms of the
+ * Searches issued since the last read (at most the 4096 most recent), then
+ * starts a new count.  Graph-replayed bm25_search calls are not timed.
+ */
+int bm25_kernel_timing(bm25_handle *h, int32_t enable);
+int bm25_kernel_times(bm25_handle *h, float *ms, int64_t capacity, int64_t *count);
+
 /* Engine facts for reports and tests. */
 typedef struct bm25_info {
     int64_t num_docs, vocab, postings;

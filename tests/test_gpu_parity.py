@@ -161,3 +161,44 @@ def test_alternating_batches_replay(pkg, oracle_mod, corpus, cuda_ok, kernel):
             assert_same_topk(*s.search(a, 10), *ra, 'A')
             assert_same_topk(*s.search(b, 10), *rb, 'B')
         assert s.info()['graph_replays'] == 10
+
+
+def test_sessions_with_different_tiles_coexist(pkg, oracle_mod, corpus, cuda_ok):
+    """The kernels' shared-memory cap is process-wide: a later session with small tiles must not break a
+    live session with large tiles."""
+    spec, index, data = corpus
+    offsets, words = pkg.synthetic_queries(index.offsets, 8, 3, 3, 55)
+    ref = _oracle(oracle_mod, index, data, offsets, words, 10)
+    big = pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, tile_docs=32768)
+    small = pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, tile_docs=2048)
+    try:
+        for s in (big, small, big):
+            assert_same_topk(*s.search((offsets, words), 10), *ref)
+    finally:
+        small.close()
+        big.close()
+
+
+@KERNELS
+def test_kernel_timing_hook(pkg, corpus, cuda_ok, kernel):
+    import torch
+    spec, index, data = corpus
+    offsets, words = pkg.synthetic_queries(index.offsets, 8, 3, 3, 77)
+    with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, kernel=kernel) as s:
+        with pytest.raises(pkg.InvalidParam):
+            s.kernel_times()
+        d_off = torch.from_numpy(offsets).cuda()
+        d_words = torch.from_numpy(words).cuda()
+        d_scores = torch.empty((8, 10), dtype=torch.float32, device='cuda')
+        d_ids = torch.empty((8, 10), dtype=torch.int32, device='cuda')
+        stream = torch.cuda.current_stream()
+        s.kernel_timing(True)
+        for _ in range(5):
+            s.search_device(d_off.data_ptr(), d_words.data_ptr(), 8, 10, d_scores.data_ptr(), d_ids.data_ptr(),
+                            stream.cuda_stream)
+        s.search((offsets, words), 10)  # graph replay: not timed
+        ms = s.kernel_times()
+        assert ms.size == 5 and (ms > 0).all() and (ms < 1000).all()
+        assert s.kernel_times().size == 0
+        s.kernel_timing(False)
+        assert s.device_status() == 0
