@@ -2,6 +2,7 @@
 
   libbm25_b200.so   CUDA engine + C ABI (nvcc, sm_100a only)
   libbm25_synth.so  seeded synthetic corpus -> resident-index arrays (gcc + OpenMP)
+  libbm25_facade.so C++ SDK facade (include/AscendIndexBm25.h) over the C ABI (g++)
 
 Run as ``python bm25-npu_b200/build.py`` or through ``__graft_entry__.build()``.
 """
@@ -58,8 +59,20 @@ def build_synth(force=False):
     return target
 
 
+def build_facade(force=False):
+    target = PACKAGE / 'libbm25_facade.so'
+    src = CSRC / 'AscendIndexBm25.cpp'
+    engine = build_engine(force)
+    deps = [src, INCLUDE / 'AscendIndexBm25.h', INCLUDE / 'bm25_b200.h', engine, Path(__file__)]
+    if not force and not _stale(target, deps):
+        return target
+    _run(['g++', '-O2', '-std=c++17', '-fPIC', '-shared', '-Wall', '-I', INCLUDE, '-o', target, src,
+          '-L', PACKAGE, '-lbm25_b200', "-Wl,-rpath,$ORIGIN"])
+    return target
+
+
 def build_all(force=False):
-    return build_engine(force), build_synth(force)
+    return build_engine(force), build_synth(force), build_facade(force)
 
 
 if __name__ == '__main__':

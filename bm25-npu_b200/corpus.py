@@ -127,3 +127,50 @@ def write_index_dir(index, path):
     path.mkdir(parents=True, exist_ok=True)
     for (name, dt), values in zip(INDEX_FILES.items(), (index.offsets, index.docs, index.tf, index.norm, index.idf)):
         np.ascontiguousarray(values, dtype=dt).tofile(path / name)
+
+
+QUERY_FILES = {'query_offsets.bin': np.dtype('<i8'), 'query_term_ids.bin': np.dtype('<i4')}
+
+
+def read_queries_dir(path):
+    """The reference's packed query files (standalone/resident_index.py:19): (offsets int64, words int32)."""
+    path = Path(path)
+    offsets = np.fromfile(path / 'query_offsets.bin', dtype=QUERY_FILES['query_offsets.bin']).astype(np.int64)
+    words = np.fromfile(path / 'query_term_ids.bin', dtype=QUERY_FILES['query_term_ids.bin']).astype(np.int32)
+    if offsets.size < 2 or offsets[0] != 0 or offsets[-1] != words.size or (np.diff(offsets) < 0).any():
+        raise ValueError('query offsets and word ids differ')
+    return offsets, words
+
+
+def write_queries_dir(offsets, words, path):
+    path = Path(path)
+    path.mkdir(parents=True, exist_ok=True)
+    np.ascontiguousarray(offsets, dtype=QUERY_FILES['query_offsets.bin']).tofile(path / 'query_offsets.bin')
+    np.ascontiguousarray(words, dtype=QUERY_FILES['query_term_ids.bin']).tofile(path / 'query_term_ids.bin')
+
+
+BM25S_FILES = ('data.csc.index.npy', 'indices.csc.index.npy', 'indptr.csc.index.npy', 'params.index.json')
+
+
+def read_bm25s_dir(path):
+    """Eager CSC saved by bm25s ``BM25.save`` (reference_only/bm25s_original/bm25s/__init__.py:941-1040):
+    returns (indptr int64, indices int32, data float32, num_docs) for ``Bm25Session.from_csc``."""
+    import json
+    path = Path(path)
+    data = np.load(path / 'data.csc.index.npy', allow_pickle=False)
+    indices = np.load(path / 'indices.csc.index.npy', allow_pickle=False)
+    indptr = np.load(path / 'indptr.csc.index.npy', allow_pickle=False)
+    num_docs = int(json.loads((path / 'params.index.json').read_text())['num_docs'])
+    return indptr.astype(np.int64), indices.astype(np.int32), data.astype(np.float32), num_docs
+
+
+def write_bm25s_dir(indptr, indices, data, num_docs, path, k1=1.5, b=0.75):
+    """Writes the CSC part of the bm25s layout (arrays + params.index.json; no vocabulary)."""
+    import json
+    path = Path(path)
+    path.mkdir(parents=True, exist_ok=True)
+    np.save(path / 'data.csc.index.npy', np.ascontiguousarray(data, dtype=np.float32))
+    np.save(path / 'indices.csc.index.npy', np.ascontiguousarray(indices, dtype=np.int32))
+    np.save(path / 'indptr.csc.index.npy', np.ascontiguousarray(indptr, dtype=np.int64))
+    (path / 'params.index.json').write_text(json.dumps({'k1': k1, 'b': b, 'method': 'lucene', 'num_docs': int(num_docs)},
+                                                       indent=4))
