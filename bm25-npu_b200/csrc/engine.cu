@@ -591,8 +591,7 @@ class Engine {
             sa.out_scores = out_scores;
             sa.out_ids = out_ids;
             sa.status = status;
-            const int plan_grid = (int)std::max<int64_t>(1, std::min<int64_t>(opts_.word_capacity, (int64_t)sms_ * 4));
-            bm25k::PlanKernel<<<plan_grid, bm25k::kPlanThreads, 0, s>>>(sa);
+            bm25k::PlanKernel<<<bm25k::PlanGrid(opts_.word_capacity, plan_.tiles, sms_), bm25k::kPlanThreads, 0, s>>>(sa);
             Cuda(cudaGetLastError(), "plan kernel launch");
             const int grid = (int)std::min<long long>(plan_.grid, ((long long)q * plan_.tiles + bm25k::kTaskBatch - 1) /
                                                                       bm25k::kTaskBatch);
@@ -1004,7 +1003,6 @@ int bm25_get_info(const bm25_handle *h, bm25_info *info)
 // start-up, or a process whose allocator is locked down).  All per-search
 // scratch lives in the fixed array below; every GPU that loads this library
 // holds it until the process exits.
-#include "static_search.cuh"
 
 namespace {
 constexpr size_t kStaticScratchBytes = size_t(16) << 20;  // 16 MiB, the largest Search this path accepts
@@ -1127,8 +1125,8 @@ extern "C" int bm25_search_csc_static(const int64_t *indptr, const int32_t *indi
             sa.out_ids = out_ids;
             // The array keeps the previous call's contents: clear what must start at zero.
             Cuda(cudaMemsetAsync(base, 0, off_cs, s), "clear static scratch");
-            const int plan_grid = (int)std::max<int64_t>(1, std::min<int64_t>(num_words, (int64_t)dev->sms * 4));
-            bm25k::PlanNoDirectoryKernel<<<plan_grid, bm25k::kPlanThreads, 0, s>>>(sa);
+            // no directory: every word takes the one-pass path of PlanKernel
+            bm25k::PlanKernel<<<bm25k::PlanGrid(num_words, (int)tiles, dev->sms), bm25k::kPlanThreads, 0, s>>>(sa);
             Cuda(cudaGetLastError(), "plan kernel launch");
             const int grid = (int)std::min<long long>(dev->grid[ti], (q * tiles + bm25k::kTaskBatch - 1) /
                                                                          bm25k::kTaskBatch);

@@ -6,9 +6,9 @@
 // (exact per-query top-K, score desc / id asc, zero-score fill by id), organised
 // for a B200 as three launches:
 //
-// PlanKernel -- one CTA per query word resolves the word's posting sub-range in
-//   every tile (per-tile directory for long lists; a shared-memory lower_bound
-//   over short lists), written as absolute [b, e) pairs to plan[word][tile].
+// PlanKernel -- resolves every query word's posting sub-range in every tile
+//   (per-tile directory rows for long lists; one pass over the postings for
+//   short lists), written as absolute [b, e) pairs to plan[word][tile].
 //
 // StreamSearchKernel -- persistent: each CTA has one producer warp and eight
 //   consumer warps.  Tasks are (query, tile) pairs in tile-major order, so every
@@ -44,6 +44,8 @@
 #pragma once
 #include "tile_kernels.cuh"
 
+#include <algorithm>
+
 namespace bm25k {
 
 constexpr int kConsumerWarps = 8;
@@ -58,7 +60,6 @@ constexpr int kFinalThreads = 256;
 constexpr int kSurvCap = 512;                          // candidates ranked exactly per query
 constexpr long long kWaitBudget = 4000000000LL;        // cycles (~2 s) before a wait gives up
 constexpr int kPlanThreads = 256;
-constexpr int kPlanSmemIds = 4096;                     // short lists up to this length are searched in smem
 
 enum : uint32_t {
     kStatusTimeout = 16u,       // a bounded wait gave up
@@ -358,19 +359,6 @@ __device__ __forceinline__ int WarpRegionSelect(StreamShared &sh, const float *r
 
 // ---- plan kernel -------------------------------------------------------------
 
-__device__ __forceinline__ long long LowerBoundSmem(const int *ids, long long n, long long target)
-{
-    long long lo = 0, hi = n;
-    while (lo < hi) {
-        const long long mid = (lo + hi) >> 1;
-        if ((long long)ids[mid] < target)
-            lo = mid + 1;
-        else
-            hi = mid;
-    }
-    return lo;
-}
-
 __device__ __forceinline__ long long LowerBoundGlobal(const int *ids, long long lo, long long hi, long long target)
 {
     while (lo < hi) {
@@ -383,51 +371,79 @@ __device__ __forceinline__ long long LowerBoundGlobal(const int *ids, long long 
     return lo;
 }
 
+constexpr int kPlanTileChunk = 2048;  // tiles per plan CTA (grid.y)
+
 // plan[w][tile] = absolute posting range of query word w inside tile (empty for
-// unknown or negative words).  Grid-stride over the batch's words.
+// unknown or negative words).  CTA (x, y) covers tiles [y * kPlanTileChunk,
+// (y + 1) * kPlanTileChunk) of words x, x + gridDim.x, ...  A word with a
+// directory row copies its per-tile offsets; any other word (a short list, or
+// no directory at all: a.dir_row == nullptr) marks every tile empty and then
+// lets each run of postings that falls in one tile write its own bounds:
+// O(tiles + df) coalesced work per word.
 __global__ void __launch_bounds__(kPlanThreads) PlanKernel(const StreamArgs a)
 {
-    __shared__ int ids[kPlanSmemIds];
+    __shared__ long long range[2];
     long long total = a.qoffsets[a.q];
     if (total < 0 || total > a.word_cap) {
-        if (blockIdx.x == 0 && threadIdx.x == 0)
+        if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
             atomicOr(a.status, kStatusBadQuery);
         total = total < 0 ? 0 : a.word_cap;
     }
+    const int t0 = (int)blockIdx.y * kPlanTileChunk;
+    const int t1 = min(a.tiles, t0 + kPlanTileChunk);
+    if (t0 >= t1)
+        return;
+    const int tid = threadIdx.x;
     for (long long w = blockIdx.x; w < total; w += gridDim.x) {
         const int term = a.words[w];
         PlanEntry *out = a.plan + w * a.tiles;
         if (term < 0 || term >= a.vocab) {
-            if (term < 0 && threadIdx.x == 0)
+            if (term < 0 && tid == 0 && blockIdx.y == 0)
                 atomicOr(a.status, kStatusBadWord);
-            for (int t = threadIdx.x; t < a.tiles; t += kPlanThreads)
+            for (int t = t0 + tid; t < t1; t += kPlanThreads)
                 out[t] = PlanEntry{0, 0};
             continue;
         }
         const long long s = a.indptr[term], e = a.indptr[term + 1];
-        const int r = a.dir_row[term];
+        const int r = a.dir_row ? a.dir_row[term] : -1;
         if (r >= 0) {
             const int *d = a.dir + (long long)r * a.dir_stride;
-            for (int t = threadIdx.x; t < a.tiles; t += kPlanThreads)
+            for (int t = t0 + tid; t < t1; t += kPlanThreads)
                 out[t] = PlanEntry{s + d[t], s + d[t + 1]};
-        } else if (e - s <= kPlanSmemIds) {
-            const int n = (int)(e - s);
-            __syncthreads();  // the previous word's readers are done with ids[]
-            for (int p = threadIdx.x; p < n; p += kPlanThreads)
-                ids[p] = __ldg(a.indices + s + p);
-            __syncthreads();
-            for (int t = threadIdx.x; t < a.tiles; t += kPlanThreads) {
-                const long long lo = (long long)t * a.tile_docs;
-                out[t] = PlanEntry{s + LowerBoundSmem(ids, n, lo), s + LowerBoundSmem(ids, n, lo + a.tile_docs)};
-            }
-        } else {
-            for (int t = threadIdx.x; t < a.tiles; t += kPlanThreads) {
-                const long long lo = (long long)t * a.tile_docs;
-                out[t] = PlanEntry{LowerBoundGlobal(a.indices, s, e, lo),
-                                   LowerBoundGlobal(a.indices, s, e, lo + a.tile_docs)};
-            }
+            continue;
         }
+        for (int t = t0 + tid; t < t1; t += kPlanThreads)
+            out[t] = PlanEntry{0, 0};
+        if (tid == 0) {
+            long long b = s, en = e;
+            if (gridDim.y > 1 && e - s > 4 * kPlanThreads) {  // only this CTA's documents
+                b = LowerBoundGlobal(a.indices, s, e, (long long)t0 * a.tile_docs);
+                en = LowerBoundGlobal(a.indices, b, e, (long long)t1 * a.tile_docs);
+            }
+            range[0] = b;
+            range[1] = en;
+        }
+        __syncthreads();  // the empty marks land before the bounds; range is published
+        const long long b = range[0], en = range[1];
+        for (long long i = b + tid; i < en; i += kPlanThreads) {
+            const int t = __ldg(a.indices + i) / a.tile_docs;
+            if (t < t0 || t >= t1)
+                continue;
+            if (i == s || __ldg(a.indices + i - 1) / a.tile_docs != t)
+                out[t].b = i;
+            if (i == e - 1 || __ldg(a.indices + i + 1) / a.tile_docs != t)
+                out[t].e = i + 1;
+        }
+        __syncthreads();  // range[] is rewritten for the next word
     }
+}
+
+// Grid of PlanKernel for a batch capacity of `words` query words.
+inline dim3 PlanGrid(long long words, int tiles, int sms)
+{
+    const int chunks = (tiles + kPlanTileChunk - 1) / kPlanTileChunk;
+    const long long x = std::max<long long>(1, std::min<long long>(words, std::max(1, sms * 8 / chunks)));
+    return dim3((unsigned)x, (unsigned)chunks);
 }
 
 // ---- the streaming kernel -------------------------------------------------------
