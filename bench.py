@@ -232,7 +232,7 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--tile-docs', type=int, default=0)
     ap.add_argument('--fan-in', type=int, default=0)
-    ap.add_argument('--kernel', type=int, default=0, help='0 streaming (default), 1 one CTA per (query, tile)')
+    ap.add_argument('--kernel', type=int, default=4, help='0 streaming, 1 one CTA per (query, tile), 4 tile groups')
     ap.add_argument('--stages', type=int, default=0)
     ap.add_argument('--docs', type=int, default=0, help='reduced corpus for profiling captures (not a bench line)')
     ap.add_argument('--vocab', type=int, default=0, help='reduced vocabulary for profiling captures')
@@ -356,7 +356,7 @@ def main():
     bytes_avg = bytes_total / args.steps
     achieved = bytes_total / (sum(kernel_ms) / 1e3) / 1e9
     search_achieved = bytes_total / (sum(step_ms) / 1e3) / 1e9
-    launches_per_search = 3 if info['kernel'] == 0 else 1
+    launches_per_search = 1 if info['kernel'] == 1 else 3
     peak, peak_kind = hbm_peak()
     traffic = traffic_from_profile()
 
@@ -389,7 +389,8 @@ def main():
                          'kernel_ms_avg': sum(kernel_ms) / len(kernel_ms),
                          'kernel_share_of_step': sum(kernel_ms) / sum(step_ms),
                          'search_achieved_gbs': search_achieved,
-                         'kernel': 'bm25k::StreamSearchKernel' if info['kernel'] == 0 else 'bm25k::TileSearchKernel'},
+                         'kernel': {0: 'bm25k::StreamSearchKernel', 1: 'bm25k::TileSearchKernel',
+                       4: 'bm25k::TileGroupKernel'}[info['kernel']]},
             'gpu_launches': args.steps * launches_per_search,
             'clocks': clock_info,
             'parity': parity,

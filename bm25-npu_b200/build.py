@@ -20,7 +20,7 @@ NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
 ENGINE_SOURCES = ['engine.cu']
-ENGINE_HEADERS = ['tile_kernels.cuh', 'stream_kernel.cuh']
+ENGINE_HEADERS = ['tile_kernels.cuh', 'stream_kernel.cuh', 'tile_group_kernel.cuh']
 
 
 def _stale(target, sources):

@@ -10,6 +10,7 @@
 // D2H.  Search = validate + pack, graph replay, synchronise, validate result.
 #include "bm25_b200.h"
 #include "stream_kernel.cuh"
+#include "tile_group_kernel.cuh"
 #include "tile_kernels.cuh"
 
 #include <cuda_runtime.h>
@@ -379,18 +380,27 @@ class Engine {
 
     void MakePlan()
     {
-        Check(opts_.kernel == 0 || opts_.kernel == 1, "kernel must be 0 (streaming) or 1 (per-tile)");
+        Check(opts_.kernel == BM25_KERNEL_STREAM || opts_.kernel == BM25_KERNEL_PER_TILE ||
+                  opts_.kernel == BM25_KERNEL_TILE_GROUP,
+              "kernel must be 0 (streaming), 1 (per-tile) or 4 (tile groups)");
         plan_.kernel = opts_.kernel;
         int t = opts_.tile_docs;
-        if (t == 0) {
+        if (plan_.kernel == 4) {
+            Check(t == 0 || t == bm25k::kWgTileDocs, "tile_docs of the tile-group kernel must be 1024");
+            Check(postings_ + kPad < INT32_MAX, "Posting count exceeds the INT32 contract");
+            t = bm25k::kWgTileDocs;
+        } else if (t == 0) {
             const int64_t per_sm = (docs_ + 147) / 148;
             t = 2048;
             while (t < per_sm && t < (plan_.kernel == 0 ? 8192 : 16384))
                 t <<= 1;
         }
-        Check(t >= 2048 && t <= 32768 && (t & (t - 1)) == 0, "tile_docs must be a power of two in [2048, 32768]");
+        Check(plan_.kernel == 4 || (t >= 2048 && t <= 32768 && (t & (t - 1)) == 0),
+              "tile_docs must be a power of two in [2048, 32768]");
         plan_.tile_docs = t;
         plan_.tiles = (int)((docs_ + t - 1) / t);
+        Check((int64_t)plan_.tiles * opts_.query_capacity < (int64_t(1) << 31),
+              "query_capacity x tiles exceeds the work counter");
         int f = opts_.merge_fan_in ? opts_.merge_fan_in : 32;
         Check(f >= 2 && f <= 1024, "merge_fan_in must be in [2, 1024]");
         for (;;) {
@@ -407,7 +417,7 @@ class Engine {
         }
         plan_.fan_in = f;
         plan_.levels = (int)plan_.lists.size();
-        if (plan_.kernel == 0) {
+        if (plan_.kernel != 1) {
             const int st = opts_.ring_stages ? opts_.ring_stages : 4;
             Check(st >= 2 && st <= bm25k::kMaxStages, "ring_stages must be in [2, 8]");
             plan_.stages = st;
@@ -505,22 +515,35 @@ class Engine {
             smem_bytes_ = (size_t)plan_.tile_docs * sizeof(float) + sizeof(bm25k::TileShared);
             RaiseSmemCap(reinterpret_cast<const void *>(bm25k::TileSearchKernel), smem_bytes_);
         } else {
-            smem_bytes_ = (size_t)plan_.tile_docs * sizeof(float) +
-                          2 * (size_t)plan_.stages * bm25k::kChunk * sizeof(int) + sizeof(bm25k::StreamShared);
-            RaiseSmemCap(reinterpret_cast<const void *>(bm25k::StreamSearchKernel), smem_bytes_);
+            const void *kernel;
+            int threads;
+            long long per_tile;  // candidates one tile can append per query
+            if (plan_.kernel == 0) {
+                smem_bytes_ = (size_t)plan_.tile_docs * sizeof(float) +
+                              2 * (size_t)plan_.stages * bm25k::kChunk * sizeof(int) + sizeof(bm25k::StreamShared);
+                kernel = reinterpret_cast<const void *>(bm25k::StreamSearchKernel);
+                threads = bm25k::kStreamThreads;
+                per_tile = (long long)bm25k::kConsumerWarps * opts_.max_k;  // every warp region
+            } else {
+                smem_bytes_ = bm25k::TileGroupSmem(plan_.stages);
+                kernel = reinterpret_cast<const void *>(bm25k::TileGroupKernel);
+                threads = bm25k::kWgThreads;
+                per_tile = opts_.max_k;
+            }
+            RaiseSmemCap(kernel, smem_bytes_);
             int per_sm = 0, sms = 0;
-            Cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bm25k::StreamSearchKernel,
-                                                               bm25k::kStreamThreads, smem_bytes_),
-                 "occupancy");
+            Cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem_bytes_), "occupancy");
             Cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "SM count");
             Check(per_sm >= 1, "tile_docs / ring_stages exceed the shared memory of one SM");
             plan_.grid = per_sm * sms;
             sms_ = sms;
             const size_t qc = (size_t)opts_.query_capacity, tiles_z = (size_t)plan_.tiles;
-            // worst case: every warp of every tile appends max_k candidates
-            cand_cap_ = (long long)tiles_z * bm25k::kConsumerWarps * opts_.max_k;
+            // worst case: every selection of every tile appends max_k candidates
+            cand_cap_ = (long long)tiles_z * per_tile;
             ctrl_ = static_cast<bm25k::StreamCtrl *>(Alloc(sizeof(bm25k::StreamCtrl), "cudaMalloc ctrl"));
             threshold_ = static_cast<unsigned *>(Alloc(qc * sizeof(unsigned), "cudaMalloc threshold"));
+            tslots_ = static_cast<unsigned *>(Alloc(qc * 32 * sizeof(unsigned), "cudaMalloc threshold slots"));
+            Cuda(cudaMemset(tslots_, 0, qc * 32 * sizeof(unsigned)), "cudaMemset");
             cand_count_ = static_cast<unsigned *>(Alloc(qc * sizeof(unsigned), "cudaMalloc cand count"));
             cand_scores_ = static_cast<float *>(Alloc(qc * cand_cap_ * sizeof(float), "cudaMalloc candidates"));
             cand_ids_ = static_cast<int *>(Alloc(qc * cand_cap_ * sizeof(int), "cudaMalloc candidates"));
@@ -582,6 +605,7 @@ class Engine {
             sa.word_cap = a.word_cap;
             sa.plan = plan_entries_;
             sa.threshold = threshold_;
+            sa.tslots = tslots_;
             sa.cand_count = cand_count_;
             sa.cand_scores = cand_scores_;
             sa.cand_ids = cand_ids_;
@@ -593,12 +617,22 @@ class Engine {
             sa.status = status;
             bm25k::PlanKernel<<<bm25k::PlanGrid(opts_.word_capacity, plan_.tiles, sms_), bm25k::kPlanThreads, 0, s>>>(sa);
             Cuda(cudaGetLastError(), "plan kernel launch");
-            const int grid = (int)std::min<long long>(plan_.grid, ((long long)q * plan_.tiles + bm25k::kTaskBatch - 1) /
-                                                                      bm25k::kTaskBatch);
-            MarkKernel(0, s);
-            bm25k::StreamSearchKernel<<<std::max(grid, 1), bm25k::kStreamThreads, smem_bytes_, s>>>(sa);
-            Cuda(cudaGetLastError(), "stream kernel launch");
-            MarkKernel(1, s);
+            if (plan_.kernel == 0) {
+                const int grid = (int)std::min<long long>(
+                    plan_.grid, ((long long)q * plan_.tiles + bm25k::kTaskBatch - 1) / bm25k::kTaskBatch);
+                MarkKernel(0, s);
+                bm25k::StreamSearchKernel<<<std::max(grid, 1), bm25k::kStreamThreads, smem_bytes_, s>>>(sa);
+                Cuda(cudaGetLastError(), "stream kernel launch");
+                MarkKernel(1, s);
+            } else {
+                // one claim per CTA at least, at most the resident grid
+                const long long claims = (long long)q * ((plan_.tiles + bm25k::kWgWarps - 1) / bm25k::kWgWarps);
+                const int grid = (int)std::max<long long>(1, std::min<long long>(plan_.grid, claims));
+                MarkKernel(0, s);
+                bm25k::TileGroupKernel<<<grid, bm25k::kWgThreads, smem_bytes_, s>>>(sa);
+                Cuda(cudaGetLastError(), "tile group kernel launch");
+                MarkKernel(1, s);
+            }
             bm25k::FinalSelectKernel<<<q, bm25k::kFinalThreads, 0, s>>>(sa);
         }
         Cuda(cudaGetLastError(), "search kernel launch");
@@ -739,7 +773,7 @@ class Engine {
     unsigned char *d_in_ = nullptr, *d_out_ = nullptr;
     unsigned *d_dev_status_ = nullptr;
     bm25k::StreamCtrl *ctrl_ = nullptr;
-    unsigned *threshold_ = nullptr, *cand_count_ = nullptr;
+    unsigned *threshold_ = nullptr, *cand_count_ = nullptr, *tslots_ = nullptr;
     float *cand_scores_ = nullptr;
     int *cand_ids_ = nullptr;
     long long cand_cap_ = 0;
@@ -829,6 +863,7 @@ void bm25_default_options(bm25_options *o)
     o->max_k = 10;
     o->query_capacity = 8;
     o->word_capacity = 24;
+    o->kernel = BM25_KERNEL_TILE_GROUP;
 }
 
 int bm25_create(const int64_t *indptr, const int32_t *indices, const float *data, int64_t vocab, int64_t num_docs,
@@ -1078,10 +1113,12 @@ extern "C" int bm25_search_csc_static(const int64_t *indptr, const int32_t *indi
             }
             const int64_t tiles = (num_docs + tile - 1) / tile;
             const long long cand_cap = tiles * bm25k::kConsumerWarps * k;
-            // scratch layout: head | threshold[q] | cand_count[q] | cand_scores[q][cap] | cand_ids[q][cap] | plan
+            // scratch layout: head | threshold[q] | cand_count[q] | slots[q][32] | cand_scores[q][cap] |
+            // cand_ids[q][cap] | plan; everything before cand_scores starts at zero
             const size_t off_thr = kStaticHeadBytes;
             const size_t off_cnt = AlignUp(off_thr + (size_t)q * 4, 16);
-            const size_t off_cs = AlignUp(off_cnt + (size_t)q * 4, 16);
+            const size_t off_slots = AlignUp(off_cnt + (size_t)q * 4, 16);
+            const size_t off_cs = AlignUp(off_slots + (size_t)q * 32 * 4, 16);
             const size_t off_ci = AlignUp(off_cs + (size_t)q * cand_cap * 4, 16);
             const size_t off_plan = AlignUp(off_ci + (size_t)q * cand_cap * 4, 16);
             const size_t need = off_plan + (size_t)std::max<int64_t>(1, num_words) * tiles * sizeof(bm25k::PlanEntry);
@@ -1116,6 +1153,7 @@ extern "C" int bm25_search_csc_static(const int64_t *indptr, const int32_t *indi
             sa.status = reinterpret_cast<unsigned *>(base + 64);
             sa.threshold = reinterpret_cast<unsigned *>(base + off_thr);
             sa.cand_count = reinterpret_cast<unsigned *>(base + off_cnt);
+            sa.tslots = reinterpret_cast<unsigned *>(base + off_slots);
             sa.cand_scores = reinterpret_cast<float *>(base + off_cs);
             sa.cand_ids = reinterpret_cast<int *>(base + off_ci);
             sa.cand_cap = cand_cap;

@@ -94,6 +94,7 @@ struct StreamArgs {
     long long word_cap;     // rows of `plan`; query words beyond it are rejected
     PlanEntry *plan;        // [word][tile]
     unsigned *threshold;    // [Q] running K-th score bits (0 = none yet)
+    unsigned *tslots;       // [Q][32] slot g: best tile maximum among tiles with tile % k == g
     unsigned *cand_count;   // [Q] candidates appended
     float *cand_scores;     // [Q][cand_cap]
     int *cand_ids;          // [Q][cand_cap]
@@ -162,6 +163,23 @@ __device__ __forceinline__ bool MbarTryWait(unsigned long long *bar, unsigned pa
     return ok != 0;
 }
 
+// try_wait that may suspend the thread (up to ~20 us) until the phase completes,
+// so a waiting warp does not spin through issue slots.
+__device__ __forceinline__ bool MbarTryWaitSuspend(unsigned long long *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n"
+        ".reg .pred p;\n"
+        "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n"
+        "selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(ok)
+        : "r"(SmemAddr(bar)), "r"(parity), "r"(20000u)
+        : "memory");
+    return ok != 0;
+}
+
 // Bounded wait; false when the budget ran out or another role aborted.
 __device__ __forceinline__ bool MbarWait(unsigned long long *bar, unsigned parity, volatile int *abort)
 {
@@ -169,7 +187,7 @@ __device__ __forceinline__ bool MbarWait(unsigned long long *bar, unsigned parit
         return true;
     const long long t0 = clock64();
     for (;;) {
-        if (MbarTryWait(bar, parity))
+        if (MbarTryWaitSuspend(bar, parity))
             return true;
         if (*abort)
             return false;
@@ -752,7 +770,20 @@ __global__ void __launch_bounds__(kFinalThreads) FinalSelectKernel(const StreamA
     const int n = (int)min((long long)appended, a.cand_cap);
     if (tid == 0 && (long long)appended > a.cand_cap)
         atomicOr(a.status, kStatusCandOverflow);
-    const float floor = __uint_as_float(__ldcg(a.threshold + q));
+    // floor: the query's threshold, or the least of the k group slots when higher (each slot is a
+    // real document's score from its own group of tiles, so k documents reach the least one)
+    float floor = __uint_as_float(__ldcg(a.threshold + q));
+    {
+        __shared__ unsigned slot_min;
+        if (warp == 0) {
+            const unsigned v = lane < k ? __ldcg(a.tslots + (long long)q * 32 + lane) : 0xffffffffu;
+            const unsigned m = __reduce_min_sync(kFull, v);
+            if (lane == 0)
+                slot_min = m;
+        }
+        __syncthreads();
+        floor = fmaxf(floor, __uint_as_float(slot_min));
+    }
     const float *cs = a.cand_scores + (long long)q * a.cand_cap;
     const int *ci = a.cand_ids + (long long)q * a.cand_cap;
 
@@ -877,6 +908,7 @@ __global__ void __launch_bounds__(kFinalThreads) FinalSelectKernel(const StreamA
             a.cand_count[q] = 0u;
             a.threshold[q] = 0u;
         }
+        a.tslots[(long long)q * 32 + lane] = 0u;
     }
 }
 

@@ -47,11 +47,21 @@ typedef struct bm25_options {
     int32_t merge_fan_in;    /* lists merged per tree node; 0 = automatic (2..32) */
     int64_t directory_bytes; /* byte budget of the per-tile posting directory; 0 = automatic */
     void *stream;            /* borrowed cudaStream_t, or NULL for an engine-owned stream */
-    int32_t kernel;          /* 0 = persistent streaming kernel (bulk-async posting ring), 1 = one CTA per (query, tile) */
-    int32_t ring_stages;     /* posting-ring depth of the streaming kernel, 2..8; 0 = automatic */
+    int32_t kernel;          /* BM25_KERNEL_*: search kernel; bm25_default_options picks BM25_KERNEL_TILE_GROUP */
+    int32_t ring_stages;     /* posting-ring depth of the ring kernels (0 and 4), 2..8; 0 = automatic */
 } bm25_options;
 
-/* Fills defaults: device 0, max_k 10, 8 queries, 24 words (the reference's Bm25Config defaults). */
+/* Search kernels (bm25_options.kernel):
+ *   BM25_KERNEL_STREAM     persistent kernel, 2048-8192-document tiles, one posting ring per CTA
+ *   BM25_KERNEL_PER_TILE   one CTA per (query, tile) and an in-launch merge tree
+ *   BM25_KERNEL_TILE_GROUP persistent kernel, 1024-document tiles, one warp per tile of an
+ *                          8-tile group fed by one bulk copy per query word (the default) */
+#define BM25_KERNEL_STREAM 0
+#define BM25_KERNEL_PER_TILE 1
+#define BM25_KERNEL_TILE_GROUP 4
+
+/* Fills defaults: device 0, max_k 10, 8 queries, 24 words (the reference's Bm25Config defaults),
+ * the tile-group kernel. */
 void bm25_default_options(bm25_options *options);
 
 /*

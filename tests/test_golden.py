@@ -71,7 +71,7 @@ def test_query_files_round_trip(pkg, large, tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize('kernel', [0, 1], ids=['stream', 'per_tile'])
+@pytest.mark.parametrize('kernel', [0, 1, 4], ids=['stream', 'per_tile', 'tile_group'])
 def test_engine_matches_reference_builder(pkg, large, cuda_ok, kernel):
     index, g = large
     with pkg.Bm25Session.from_lazy(index.offsets, index.docs, index.tf, index.norm, index.idf, k1=1.2,
@@ -82,7 +82,7 @@ def test_engine_matches_reference_builder(pkg, large, cuda_ok, kernel):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize('kernel', [0, 1], ids=['stream', 'per_tile'])
+@pytest.mark.parametrize('kernel', [0, 1, 4], ids=['stream', 'per_tile', 'tile_group'])
 def test_engine_matches_bm25s(pkg, tiny, cuda_ok, kernel):
     n = int(tiny['num_docs'][0])
     with pkg.Bm25Session.from_csc(tiny['indptr'], tiny['indices'], tiny['data'], n, query_capacity=16,

@@ -20,7 +20,12 @@ def _oracle(oracle_mod, index, data, offsets, words, k):
     return oracle_mod.search(index.offsets, index.docs, data, index.num_docs, offsets, words, k)
 
 
-KERNELS = pytest.mark.parametrize('kernel', [0, 1], ids=['stream', 'per_tile'])
+KERNELS = pytest.mark.parametrize('kernel', [0, 1, 4], ids=['stream', 'per_tile', 'tile_group'])
+
+
+def _tile(kernel, tile_docs):
+    """The tile-group kernel has one tile size (1024 docs): it takes 0 = automatic."""
+    return 0 if kernel == 4 else tile_docs
 
 
 @KERNELS
@@ -44,6 +49,11 @@ def test_config_8192_docs_q8x3_k10(pkg, oracle_mod, cuda_ok, kernel):
                                                      (32768, 8, 4)])
 def test_tiles_and_merge_tree(pkg, oracle_mod, corpus, cuda_ok, tile_docs, fan_in, stages, kernel):
     spec, index, data = corpus
+    if kernel == 4 and tile_docs:
+        with pytest.raises(pkg.InvalidParam):
+            pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, tile_docs=tile_docs,
+                                     kernel=kernel)
+        tile_docs = 0
     rng = np.random.default_rng(tile_docs + fan_in)
     rows = mixed_queries(index.vocab, rng, 24, 0, 12)
     rows[0] = [0, 1, 2]          # densest terms: candidate list overflow, full-row selection
@@ -68,7 +78,7 @@ def test_directory_and_scan_paths_agree(pkg, oracle_mod, corpus, cuda_ok, kernel
     ref = _oracle(oracle_mod, index, data, offsets, words, 10)
     for budget in (1, 1 << 30):  # 1 byte: every list is counted inside the CTA; 1 GiB: directory for long lists
         with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, query_capacity=16,
-                                      word_capacity=256, tile_docs=2048, directory_bytes=budget,
+                                      word_capacity=256, tile_docs=_tile(kernel, 2048), directory_bytes=budget,
                                       kernel=kernel) as s:
             assert_same_topk(*s.search((offsets, words), 10), *ref, f'budget={budget}')
 
@@ -77,7 +87,7 @@ def test_directory_and_scan_paths_agree(pkg, oracle_mod, corpus, cuda_ok, kernel
 def test_reference_edge_queries(pkg, oracle_mod, corpus, cuda_ok, kernel):
     spec, index, data = corpus
     with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, query_capacity=7,
-                                  word_capacity=128, max_k=32, tile_docs=4096, kernel=kernel) as s:
+                                  word_capacity=128, max_k=32, tile_docs=_tile(kernel, 4096), kernel=kernel) as s:
         for rows in (EDGE_A, EDGE_B, EDGE_A, [[]] * 3, EDGE_B):
             offsets, words = pack(rows)
             for k in (1, 3, 10, 32):
@@ -169,8 +179,8 @@ def test_sessions_with_different_tiles_coexist(pkg, oracle_mod, corpus, cuda_ok)
     spec, index, data = corpus
     offsets, words = pkg.synthetic_queries(index.offsets, 8, 3, 3, 55)
     ref = _oracle(oracle_mod, index, data, offsets, words, 10)
-    big = pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, tile_docs=32768)
-    small = pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, tile_docs=2048)
+    big = pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, tile_docs=32768, kernel=0)
+    small = pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, tile_docs=2048, kernel=0)
     try:
         for s in (big, small, big):
             assert_same_topk(*s.search((offsets, words), 10), *ref)
