@@ -234,6 +234,7 @@ def main():
     ap.add_argument('--fan-in', type=int, default=0)
     ap.add_argument('--kernel', type=int, default=4, help='0 streaming, 1 one CTA per (query, tile), 4 tile groups')
     ap.add_argument('--stages', type=int, default=0)
+    ap.add_argument('--chunk', type=int, default=0, help='postings per ring stage of the tile-group kernel')
     ap.add_argument('--docs', type=int, default=0, help='reduced corpus for profiling captures (not a bench line)')
     ap.add_argument('--vocab', type=int, default=0, help='reduced vocabulary for profiling captures')
     args = ap.parse_args()
@@ -258,7 +259,7 @@ def main():
     session = pkg.Bm25Session.from_lazy(index.offsets, index.docs, index.tf, index.norm, index.idf, k1=spec.k1,
                                         query_capacity=Q, word_capacity=Q * TERMS, max_k=K, device_id=local,
                                         tile_docs=args.tile_docs, merge_fan_in=args.fan_in, kernel=args.kernel,
-                                        ring_stages=args.stages)
+                                        ring_stages=args.stages, ring_chunk=args.chunk)
     info = session.info()
     log(f'engine ready in {time.perf_counter() - t:.1f}s: {info}')
 
@@ -377,7 +378,7 @@ def main():
                        'batches': 'A/B alternating, terms drawn by df', 'l2': 'flushed between steps (256 MiB write)',
                        'tile_docs': info['tile_docs'], 'tiles': info['tiles'], 'merge_fan_in': info['merge_fan_in'],
                        'merge_levels': info['merge_levels'], 'kernel': info['kernel'],
-                       'ring_stages': info['ring_stages'], 'grid': info['grid'],
+                       'ring_stages': info['ring_stages'], 'ring_chunk': info['ring_chunk'], 'grid': info['grid'],
                        'parallelism': f'replicas x{world} (queries sharded)'},
             'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
                     'p50_ms': percentile(host_ms, 50), 'p95_ms': percentile(host_ms, 95),

@@ -30,6 +30,7 @@ class Options(ctypes.Structure):
         ('stream', c_void_p),
         ('kernel', c_int32),
         ('ring_stages', c_int32),
+        ('ring_chunk', c_int32),
     ]
 
 
@@ -52,6 +53,7 @@ class Info(ctypes.Structure):
         ('ring_stages', c_int32),
         ('grid', c_int32),
         ('smem_bytes', c_int32),
+        ('ring_chunk', c_int32),
     ]
 
 

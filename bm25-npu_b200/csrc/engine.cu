@@ -147,7 +147,7 @@ class Engine {
         int tile_docs = 0, tiles = 0, fan_in = 32, levels = 0;
         std::vector<int> lists;  // lists per query at each level
         int64_t dir_rows = 0, dir_min_df = 0;
-        int kernel = 0, stages = 0, grid = 0;
+        int kernel = 0, stages = 0, grid = 0, chunk = 0;
     };
 
     Engine(const bm25_options &o, int64_t vocab, int64_t docs, int64_t postings)
@@ -358,6 +358,7 @@ class Engine {
         info->searches = searches_;
         info->kernel = plan_.kernel;
         info->ring_stages = plan_.stages;
+        info->ring_chunk = plan_.chunk;
         info->grid = plan_.grid;
         info->smem_bytes = (int32_t)smem_bytes_;
     }
@@ -418,9 +419,16 @@ class Engine {
         plan_.fan_in = f;
         plan_.levels = (int)plan_.lists.size();
         if (plan_.kernel != 1) {
-            const int st = opts_.ring_stages ? opts_.ring_stages : 4;
+            // tile-group kernel: 3 stages of 1536 postings keep 3 CTAs on an SM (measured best at 10M docs)
+            const int st = opts_.ring_stages ? opts_.ring_stages : (plan_.kernel == BM25_KERNEL_TILE_GROUP ? 3 : 4);
             Check(st >= 2 && st <= bm25k::kMaxStages, "ring_stages must be in [2, 8]");
             plan_.stages = st;
+            if (plan_.kernel == BM25_KERNEL_TILE_GROUP) {
+                const int c = opts_.ring_chunk ? opts_.ring_chunk : 1536;
+                Check(c >= bm25k::kWgChunkMin && c <= bm25k::kWgChunkMax && c % 4 == 0,
+                      "ring_chunk must be a multiple of 4 in [512, 4096]");
+                plan_.chunk = c;
+            }
         }
     }
 
@@ -525,7 +533,7 @@ class Engine {
                 threads = bm25k::kStreamThreads;
                 per_tile = (long long)bm25k::kConsumerWarps * opts_.max_k;  // every warp region
             } else {
-                smem_bytes_ = bm25k::TileGroupSmem(plan_.stages);
+                smem_bytes_ = bm25k::TileGroupSmem(plan_.stages, plan_.chunk);
                 kernel = reinterpret_cast<const void *>(bm25k::TileGroupKernel);
                 threads = bm25k::kWgThreads;
                 per_tile = opts_.max_k;
@@ -612,6 +620,7 @@ class Engine {
             sa.cand_cap = cand_cap_;
             sa.ctrl = ctrl_;
             sa.stages = plan_.stages;
+            sa.chunk = plan_.chunk;
             sa.out_scores = out_scores;
             sa.out_ids = out_ids;
             sa.status = status;

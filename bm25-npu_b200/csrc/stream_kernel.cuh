@@ -101,6 +101,7 @@ struct StreamArgs {
     long long cand_cap;
     StreamCtrl *ctrl;
     int stages;
+    int chunk;              // postings per ring stage (tile-group kernel)
     float *out_scores;
     int *out_ids;
     unsigned *status;
@@ -208,6 +209,25 @@ __device__ __forceinline__ bool WarpWait(unsigned long long *bar, unsigned parit
     if (ok)
         (void)MbarTryWait(bar, parity);  // complete already: returns at once, acquiring for this lane
     return ok != 0;
+}
+
+// Whole-warp bounded wait with every lane on the barrier (no divergent branch);
+// the outcome is agreed by vote, so all lanes return the same.
+__device__ __forceinline__ bool WarpWaitAll(unsigned long long *bar, unsigned parity, volatile int *abort)
+{
+    bool ok = MbarTryWait(bar, parity);
+    if (!__all_sync(kFull, ok)) {
+        const long long t0 = clock64();
+        while (!ok) {
+            ok = MbarTryWaitSuspend(bar, parity);
+            if (!ok && (*abort || clock64() - t0 > kWaitBudget)) {
+                *abort = 1;
+                break;
+            }
+        }
+        ok = __all_sync(kFull, ok);
+    }
+    return ok;
 }
 
 // 1-D bulk copy global -> shared, completion counted on `bar` (no multicast).
@@ -390,6 +410,27 @@ __device__ __forceinline__ long long LowerBoundGlobal(const int *ids, long long 
 }
 
 constexpr int kPlanTileChunk = 2048;  // tiles per plan CTA (grid.y)
+constexpr int kPlanScanAll = 16384;   // lists up to this length are scanned whole
+
+// First position in ids[lo, hi) (ascending) whose value is >= target; all 32 lanes
+// of a warp, each step probing 32 evenly spaced positions.
+__device__ __forceinline__ long long WarpLowerBoundGlobal(const int *ids, long long lo, long long hi,
+                                                          long long target, int lane)
+{
+    while (hi - lo > 32) {
+        const long long step = (hi - lo + 31) >> 5;
+        const long long p = lo + lane * step;
+        const bool less = p < hi && (long long)__ldg(ids + p) < target;
+        const int c = __popc(__ballot_sync(kFull, less));
+        if (c == 0)
+            return lo;
+        const long long nlo = lo + (long long)(c - 1) * step + 1;
+        hi = min(hi, lo + (long long)c * step);
+        lo = nlo;
+    }
+    const bool less = lo + lane < hi && (long long)__ldg(ids + lo + lane) < target;
+    return lo + __popc(__ballot_sync(kFull, less));
+}
 
 // plan[w][tile] = absolute posting range of query word w inside tile (empty for
 // unknown or negative words).  CTA (x, y) covers tiles [y * kPlanTileChunk,
@@ -432,14 +473,19 @@ __global__ void __launch_bounds__(kPlanThreads) PlanKernel(const StreamArgs a)
         }
         for (int t = t0 + tid; t < t1; t += kPlanThreads)
             out[t] = PlanEntry{0, 0};
-        if (tid == 0) {
+        if (tid < 32) {
+            // lists up to kPlanScanAll postings are scanned whole by every CTA of the word; a
+            // longer one (a list left out of the directory by its byte budget) is first cut to
+            // this CTA's documents with a 32-way search: a few dependent loads, not ~log2(df)
             long long b = s, en = e;
-            if (gridDim.y > 1 && e - s > 4 * kPlanThreads) {  // only this CTA's documents
-                b = LowerBoundGlobal(a.indices, s, e, (long long)t0 * a.tile_docs);
-                en = LowerBoundGlobal(a.indices, b, e, (long long)t1 * a.tile_docs);
+            if (gridDim.y > 1 && e - s > kPlanScanAll) {
+                b = WarpLowerBoundGlobal(a.indices, s, e, (long long)t0 * a.tile_docs, tid);
+                en = WarpLowerBoundGlobal(a.indices, b, e, (long long)t1 * a.tile_docs, tid);
             }
-            range[0] = b;
-            range[1] = en;
+            if (tid == 0) {
+                range[0] = b;
+                range[1] = en;
+            }
         }
         __syncthreads();  // the empty marks land before the bounds; range is published
         const long long b = range[0], en = range[1];

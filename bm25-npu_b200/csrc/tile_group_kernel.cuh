@@ -11,7 +11,7 @@
 //     claims are in flight while the current claim's copies are issued), and
 //     streams each non-empty word run of the claim into a ring of `stages`
 //     shared-memory stages with 1-D bulk async copies (cp.async.bulk ...
-//     mbarrier::complete_tx, no multicast), kWgChunk postings per stage at
+//     mbarrier::complete_tx, no multicast), a.chunk postings per stage at
 //     most, with the 8 tiles' bounds in the stage's meta;
 //   * consumer warp j waits on each stage itself (bounded), adds the postings
 //     of its tile in that stage into its row -- stages arrive in word order and
@@ -36,7 +36,7 @@ namespace bm25k {
 constexpr int kWgTileDocs = 1024;
 constexpr int kWgWarps = 8;                      // consumer warps = tiles per claim
 constexpr int kWgThreads = (kWgWarps + 1) * 32;  // + the producer warp
-constexpr int kWgChunk = 1024;                   // postings per ring stage
+constexpr int kWgChunkMin = 512, kWgChunkMax = 4096;  // postings per ring stage (a.chunk)
 constexpr int kWgPlanWords = 8;                  // words per claim prefetched (2 per lane)
 
 enum : int {
@@ -69,9 +69,9 @@ struct WgShared {
     int abort;
 };
 
-inline size_t TileGroupSmem(int stages)
+inline size_t TileGroupSmem(int stages, int chunk)
 {
-    return (size_t)kWgWarps * kWgTileDocs * sizeof(float) + 2 * (size_t)stages * kWgChunk * sizeof(int) +
+    return (size_t)kWgWarps * kWgTileDocs * sizeof(float) + 2 * (size_t)stages * chunk * sizeof(int) +
            sizeof(WgShared);
 }
 
@@ -199,9 +199,10 @@ __global__ void __launch_bounds__(kWgThreads, 3) TileGroupKernel(const StreamArg
 {
     extern __shared__ __align__(128) unsigned char wg_smem[];
     float *rows = reinterpret_cast<float *>(wg_smem);
+    const int chunk = a.chunk;
     int *ring_ids = reinterpret_cast<int *>(rows + (size_t)kWgWarps * kWgTileDocs);
-    float *ring_vals = reinterpret_cast<float *>(ring_ids + (size_t)a.stages * kWgChunk);
-    WgShared &sh = *reinterpret_cast<WgShared *>(ring_vals + (size_t)a.stages * kWgChunk);
+    float *ring_vals = reinterpret_cast<float *>(ring_ids + (size_t)a.stages * chunk);
+    WgShared &sh = *reinterpret_cast<WgShared *>(ring_vals + (size_t)a.stages * chunk);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
     if (tid == 0) {
@@ -360,7 +361,7 @@ __global__ void __launch_bounds__(kWgThreads, 3) TileGroupKernel(const StreamArg
                     continue;  // the word has no postings in this group
                 const long long a0 = (long long)lo & ~3LL, a1 = ((long long)hi + 3) & ~3LL;
                 for (long long c0 = a0; c0 < a1;) {
-                    const long long c1 = min(c0 + (long long)kWgChunk, a1);
+                    const long long c1 = min(c0 + (long long)chunk, a1);
                     if (!claim_stage()) {
                         dead = true;
                         break;
@@ -391,8 +392,8 @@ __global__ void __launch_bounds__(kWgThreads, 3) TileGroupKernel(const StreamArg
                     if (lane == 0) {
                         const unsigned bytes = (unsigned)(c1 - c0) * 4u;
                         MbarArriveExpectTx(&sh.full[st], 2u * bytes);
-                        BulkLoad(ring_ids + (size_t)st * kWgChunk, a.indices + c0, bytes, &sh.full[st]);
-                        BulkLoad(ring_vals + (size_t)st * kWgChunk, a.data + c0, bytes, &sh.full[st]);
+                        BulkLoad(ring_ids + (size_t)st * chunk, a.indices + c0, bytes, &sh.full[st]);
+                        BulkLoad(ring_vals + (size_t)st * chunk, a.data + c0, bytes, &sh.full[st]);
                     }
                     __syncwarp();
                     first = false;
@@ -444,7 +445,7 @@ __global__ void __launch_bounds__(kWgThreads, 3) TileGroupKernel(const StreamArg
     unsigned bad = 0;
     bool touched = false;
     for (;;) {
-        if (!WarpWait(&sh.full[st], parity, abort, lane))
+        if (!WarpWaitAll(&sh.full[st], parity, abort))
             break;
         const WgMeta &m = sh.meta[st];
         const int flags = m.flags;
@@ -455,8 +456,8 @@ __global__ void __launch_bounds__(kWgThreads, 3) TileGroupKernel(const StreamArg
         const int q = m.q, tile = m.tile0 + warp;
         const float thr = m.thr;
         const int base_doc = tile * kWgTileDocs;
-        const int *ids = ring_ids + (size_t)st * kWgChunk;
-        const float *vals = ring_vals + (size_t)st * kWgChunk;
+        const int *ids = ring_ids + (size_t)st * chunk;
+        const float *vals = ring_vals + (size_t)st * chunk;
         if (lo < hi)
             touched = true;
         for (int x0 = lo + lane; x0 < hi; x0 += 128) {

@@ -70,7 +70,7 @@ def pack_queries(queries):
 
 
 def _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes, stream,
-             kernel=4, ring_stages=0):
+             kernel=4, ring_stages=0, ring_chunk=0):
     o = n.Options()
     n.engine_library().bm25_default_options(ctypes.byref(o))
     o.device_id = device_id
@@ -83,6 +83,7 @@ def _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_f
     o.stream = stream
     o.kernel = kernel
     o.ring_stages = ring_stages
+    o.ring_chunk = ring_chunk
     return o
 
 
@@ -97,7 +98,8 @@ class Bm25Session:
 
     @classmethod
     def from_csc(cls, indptr, indices, data, num_docs, *, query_capacity=8, word_capacity=24, max_k=10,
-                 device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0, stream=None, kernel=4, ring_stages=0):
+                 device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0, stream=None, kernel=4, ring_stages=0,
+                 ring_chunk=0):
         """Eager CSC index (bm25s layout): indptr int64 [V+1], indices int32 [M], data float32 [M]."""
         lib = n.engine_library()
         indptr = np.ascontiguousarray(indptr, dtype=np.int64)
@@ -107,7 +109,7 @@ class Bm25Session:
         if vocab < 1 or indices.size != indptr[-1] or data.size != indices.size:
             raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'Index dimensions/endpoints differ')
         o = _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes,
-                     stream, kernel, ring_stages)
+                     stream, kernel, ring_stages, ring_chunk)
         h = c_void_p()
         status = lib.bm25_create(n.ptr(indptr, c_int64), n.ptr(indices, c_int32), n.ptr(data, c_float), vocab,
                                  int(num_docs), ctypes.byref(o), ctypes.byref(h))
@@ -117,7 +119,7 @@ class Bm25Session:
     @classmethod
     def from_lazy(cls, term_offsets, posting_doc_ids, posting_tf, doc_norm, idf, *, k1=1.2, query_capacity=8,
                   word_capacity=24, max_k=10, device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0,
-                  stream=None, kernel=4, ring_stages=0):
+                  stream=None, kernel=4, ring_stages=0, ring_chunk=0):
         """The reference's resident index (common/bm25/index_data.h:9-42); posting scores built on the GPU."""
         lib = n.engine_library()
         offsets = np.ascontiguousarray(term_offsets, dtype=np.int64)
@@ -129,7 +131,7 @@ class Bm25Session:
         if offsets.size != vocab + 1 or docs.size != tf.size or offsets[-1] != docs.size:
             raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'Index dimensions/endpoints differ')
         o = _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes,
-                     stream, kernel, ring_stages)
+                     stream, kernel, ring_stages, ring_chunk)
         h = c_void_p()
         status = lib.bm25_create_lazy(n.ptr(offsets, c_int64), n.ptr(docs, c_int32), n.ptr(tf, c_float),
                                       n.ptr(norm, c_float), n.ptr(idf, c_float), vocab, norm.size, float(k1),

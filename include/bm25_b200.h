@@ -49,6 +49,8 @@ typedef struct bm25_options {
     void *stream;            /* borrowed cudaStream_t, or NULL for an engine-owned stream */
     int32_t kernel;          /* BM25_KERNEL_*: search kernel; bm25_default_options picks BM25_KERNEL_TILE_GROUP */
     int32_t ring_stages;     /* posting-ring depth of the ring kernels (0 and 4), 2..8; 0 = automatic */
+    int32_t ring_chunk;      /* postings per ring stage of the tile-group kernel, 512..4096, a multiple of 4;
+                                0 = automatic */
 } bm25_options;
 
 /* Search kernels (bm25_options.kernel):
@@ -172,7 +174,7 @@ typedef struct bm25_info {
     int64_t directory_rows, directory_min_df;
     int64_t index_bytes, device_bytes;
     int64_t graph_replays, searches;
-    int32_t kernel, ring_stages, grid, smem_bytes;
+    int32_t kernel, ring_stages, grid, smem_bytes, ring_chunk;
 } bm25_info;
 int bm25_get_info(const bm25_handle *handle, bm25_info *info);
 
