@@ -387,9 +387,9 @@ class Engine {
         plan_.kernel = opts_.kernel;
         int t = opts_.tile_docs;
         if (plan_.kernel == 4) {
-            Check(t == 0 || t == bm25k::kWgTileDocs, "tile_docs of the tile-group kernel must be 1024");
+            Check(t == 0 || t == 1024 || t == 2048, "tile_docs of the tile-group kernel must be 1024 or 2048");
             Check(postings_ + kPad < INT32_MAX, "Posting count exceeds the INT32 contract");
-            t = bm25k::kWgTileDocs;
+            t = t ? t : bm25k::kWgTileDocs;
         } else if (t == 0) {
             const int64_t per_sm = (docs_ + 147) / 148;
             t = 2048;
@@ -533,8 +533,8 @@ class Engine {
                 threads = bm25k::kStreamThreads;
                 per_tile = (long long)bm25k::kConsumerWarps * opts_.max_k;  // every warp region
             } else {
-                smem_bytes_ = bm25k::TileGroupSmem(plan_.stages, plan_.chunk);
-                kernel = reinterpret_cast<const void *>(bm25k::TileGroupKernel);
+                smem_bytes_ = bm25k::TileGroupSmem(plan_.stages, plan_.chunk, plan_.tile_docs);
+                kernel = bm25k::TileGroupKernelFor(plan_.tile_docs);
                 threads = bm25k::kWgThreads;
                 per_tile = opts_.max_k;
             }
@@ -638,7 +638,10 @@ class Engine {
                 const long long claims = (long long)q * ((plan_.tiles + bm25k::kWgWarps - 1) / bm25k::kWgWarps);
                 const int grid = (int)std::max<long long>(1, std::min<long long>(plan_.grid, claims));
                 MarkKernel(0, s);
-                bm25k::TileGroupKernel<<<grid, bm25k::kWgThreads, smem_bytes_, s>>>(sa);
+                if (plan_.tile_docs == 2048)
+                    bm25k::TileGroupKernel<2048><<<grid, bm25k::kWgThreads, smem_bytes_, s>>>(sa);
+                else
+                    bm25k::TileGroupKernel<1024><<<grid, bm25k::kWgThreads, smem_bytes_, s>>>(sa);
                 Cuda(cudaGetLastError(), "tile group kernel launch");
                 MarkKernel(1, s);
             }

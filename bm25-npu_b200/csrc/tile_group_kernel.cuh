@@ -33,7 +33,7 @@
 
 namespace bm25k {
 
-constexpr int kWgTileDocs = 1024;
+constexpr int kWgTileDocs = 1024;                // default documents per tile (kTile: 1024 or 2048)
 constexpr int kWgWarps = 8;                      // consumer warps = tiles per claim
 constexpr int kWgThreads = (kWgWarps + 1) * 32;  // + the producer warp
 constexpr int kWgChunkMin = 512, kWgChunkMax = 4096;  // postings per ring stage (a.chunk)
@@ -69,9 +69,9 @@ struct WgShared {
     int abort;
 };
 
-inline size_t TileGroupSmem(int stages, int chunk)
+inline size_t TileGroupSmem(int stages, int chunk, int tile_docs)
 {
-    return (size_t)kWgWarps * kWgTileDocs * sizeof(float) + 2 * (size_t)stages * chunk * sizeof(int) +
+    return (size_t)kWgWarps * tile_docs * sizeof(float) + 2 * (size_t)stages * chunk * sizeof(int) +
            sizeof(WgShared);
 }
 
@@ -195,12 +195,14 @@ __device__ __forceinline__ int2 WgFarRange(const StreamArgs &a, const WgClaim &c
     return make_int2((int)pe.b, (int)pe.e);
 }
 
-__global__ void __launch_bounds__(kWgThreads, 3) TileGroupKernel(const StreamArgs a)
+// kTile: documents per tile (a.tile_docs), 1024 or 2048.
+template <int kTile>
+__global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKernel(const StreamArgs a)
 {
     extern __shared__ __align__(128) unsigned char wg_smem[];
     float *rows = reinterpret_cast<float *>(wg_smem);
     const int chunk = a.chunk;
-    int *ring_ids = reinterpret_cast<int *>(rows + (size_t)kWgWarps * kWgTileDocs);
+    int *ring_ids = reinterpret_cast<int *>(rows + (size_t)kWgWarps * kTile);
     float *ring_vals = reinterpret_cast<float *>(ring_ids + (size_t)a.stages * chunk);
     WgShared &sh = *reinterpret_cast<WgShared *>(ring_vals + (size_t)a.stages * chunk);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -213,7 +215,7 @@ __global__ void __launch_bounds__(kWgThreads, 3) TileGroupKernel(const StreamArg
         sh.abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int i = tid; i < kWgWarps * kWgTileDocs / 4; i += kWgThreads)
+    for (int i = tid; i < kWgWarps * kTile / 4; i += kWgThreads)
         reinterpret_cast<float4 *>(rows)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     __syncthreads();
     volatile int *abort = &sh.abort;
@@ -437,7 +439,7 @@ __global__ void __launch_bounds__(kWgThreads, 3) TileGroupKernel(const StreamArg
     }
 
     // ================= consumer warp `warp` owns tile tile0 + warp of each claim =================
-    float *row = rows + (size_t)warp * kWgTileDocs;
+    float *row = rows + (size_t)warp * kTile;
     float4 *row4 = reinterpret_cast<float4 *>(row);
     WarpSel &ws = sh.wsel[warp];
     int st = 0;
@@ -455,7 +457,7 @@ __global__ void __launch_bounds__(kWgThreads, 3) TileGroupKernel(const StreamArg
         const int lo = max(m.b[warp], c0) - c0, hi = min(m.e[warp], c0 + m.count) - c0;
         const int q = m.q, tile = m.tile0 + warp;
         const float thr = m.thr;
-        const int base_doc = tile * kWgTileDocs;
+        const int base_doc = tile * kTile;
         const int *ids = ring_ids + (size_t)st * chunk;
         const float *vals = ring_vals + (size_t)st * chunk;
         if (lo < hi)
@@ -469,7 +471,7 @@ __global__ void __launch_bounds__(kWgThreads, 3) TileGroupKernel(const StreamArg
                 d[u] = -1;
                 if (x < hi) {
                     const int rel = ids[x] - base_doc;
-                    if ((unsigned)rel < (unsigned)kWgTileDocs) {
+                    if ((unsigned)rel < (unsigned)kTile) {
                         d[u] = rel;
                         v[u] = vals[x];
                     } else {
@@ -499,7 +501,7 @@ __global__ void __launch_bounds__(kWgThreads, 3) TileGroupKernel(const StreamArg
 
         // ---- end of the claim: select this warp's tile ----
         float kth;
-        const int sel = WarpRowSelect<kWgTileDocs / 128>(ws, row4, thr, a.k, base_doc, lane, &kth);
+        const int sel = WarpRowSelect<kTile / 128>(ws, row4, thr, a.k, base_doc, lane, &kth);
         if (sel > 0) {
             if (!(ws.sel_s[0] <= FLT_MAX))
                 bad |= kStatusOverflow;  // an overflowed sum would be the tile's best score
@@ -526,6 +528,12 @@ __global__ void __launch_bounds__(kWgThreads, 3) TileGroupKernel(const StreamArg
     bad = __reduce_or_sync(kFull, bad);
     if (lane == 0 && (bad || *abort))
         atomicOr(a.status, bad | (*abort ? kStatusTimeout : 0u));
+}
+
+inline const void *TileGroupKernelFor(int tile_docs)
+{
+    return tile_docs == 2048 ? reinterpret_cast<const void *>(&TileGroupKernel<2048>)
+                             : reinterpret_cast<const void *>(&TileGroupKernel<1024>);
 }
 
 } // namespace bm25k

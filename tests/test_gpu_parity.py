@@ -24,7 +24,7 @@ KERNELS = pytest.mark.parametrize('kernel', [0, 1, 4], ids=['stream', 'per_tile'
 
 
 def _tile(kernel, tile_docs):
-    """The tile-group kernel has one tile size (1024 docs): it takes 0 = automatic."""
+    """The tile-group kernel takes 1024- or 2048-document tiles (0 = automatic)."""
     return 0 if kernel == 4 else tile_docs
 
 
@@ -49,7 +49,7 @@ def test_config_8192_docs_q8x3_k10(pkg, oracle_mod, cuda_ok, kernel):
                                                      (32768, 8, 4)])
 def test_tiles_and_merge_tree(pkg, oracle_mod, corpus, cuda_ok, tile_docs, fan_in, stages, kernel):
     spec, index, data = corpus
-    if kernel == 4 and tile_docs:
+    if kernel == 4 and tile_docs not in (0, 1024, 2048):
         with pytest.raises(pkg.InvalidParam):
             pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, tile_docs=tile_docs,
                                      kernel=kernel)
