@@ -54,10 +54,10 @@ struct WarpSel {
 };
 
 struct __align__(16) WgMeta {
-    int b[kWgWarps], e[kWgWarps];  // tile j's postings [b[j], e[j]) of the stage's word (absolute)
-    int c0, count;                 // ring element 0 is posting c0; count elements copied
-    int q, tile0, flags;
-    float thr;                     // the query's running bound when the claim was taken
+    int2 be[kWgWarps];  // tile j's postings [be[j].x, be[j].y) of the stage's word (absolute)
+    int4 span;          // x: ring element 0 is posting x; y: elements copied; z: query; w: first tile
+    int flags;
+    float thr;          // the query's running bound when the claim was taken
     int pad[2];
 };
 
@@ -372,21 +372,13 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
                     WgMeta &m = sh.meta[st];
                     // tile bounds of word s: lane 8 * (s % 4) + j holds tile j
                     if (s < kWgPlanWords) {
-                        if ((lane >> 3) == (s & 3)) {
-                            const int2 r = s < 4 ? cur.p0 : cur.p1;
-                            m.b[lane & 7] = r.x;
-                            m.e[lane & 7] = r.y;
-                        }
+                        if ((lane >> 3) == (s & 3))
+                            m.be[lane & 7] = s < 4 ? cur.p0 : cur.p1;
                     } else if (lane < kWgWarps) {
-                        const int2 r = WgFarRange(a, cur, s, lane);
-                        m.b[lane] = r.x;
-                        m.e[lane] = r.y;
+                        m.be[lane] = WgFarRange(a, cur, s, lane);
                     }
                     if (lane == 0) {
-                        m.c0 = (int)c0;
-                        m.count = (int)(c1 - c0);
-                        m.q = cur.q;
-                        m.tile0 = cur.tile0;
+                        m.span = make_int4((int)c0, (int)(c1 - c0), cur.q, cur.tile0);
                         m.flags = (first ? kWgFirstOfClaim : 0) | (s == last_word && c1 == a1 ? kWgLastOfClaim : 0);
                         m.thr = thr;
                     }
@@ -453,40 +445,48 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
         const int flags = m.flags;
         if (flags & kWgStop)
             break;
-        const int c0 = m.c0;
-        const int lo = max(m.b[warp], c0) - c0, hi = min(m.e[warp], c0 + m.count) - c0;
-        const int q = m.q, tile = m.tile0 + warp;
+        const int4 span = m.span;
+        const int2 be = m.be[warp];
+        const int c0 = span.x;
+        const int lo = max(be.x, c0) - c0, hi = min(be.y, c0 + span.y) - c0;
+        const int q = span.z, tile = span.w + warp;
         const float thr = m.thr;
         const int base_doc = tile * kTile;
         const int *ids = ring_ids + (size_t)st * chunk;
         const float *vals = ring_vals + (size_t)st * chunk;
         if (lo < hi)
             touched = true;
-        for (int x0 = lo + lane; x0 < hi; x0 += 128) {
+        // windows of 128 ring elements from the 16-byte boundary at or below lo; lane l takes
+        // elements 4l..4l+3 of a window with one 128-bit load of ids and one of scores
+        for (int w0 = lo & ~3; w0 < hi; w0 += 128) {
+            const int x = w0 + 4 * lane;
+            int4 id4 = make_int4(0, 0, 0, 0);
+            float4 v4 = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (x < hi) {
+                id4 = *reinterpret_cast<const int4 *>(ids + x);
+                v4 = *reinterpret_cast<const float4 *>(vals + x);
+            }
+            const int idv[4] = {id4.x, id4.y, id4.z, id4.w};
+            const float vv[4] = {v4.x, v4.y, v4.z, v4.w};
             int d[4];
-            float v[4], r[4];
+            bool ok[4];
+            float r[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                const int x = x0 + 32 * u;
-                d[u] = -1;
-                if (x < hi) {
-                    const int rel = ids[x] - base_doc;
-                    if ((unsigned)rel < (unsigned)kTile) {
-                        d[u] = rel;
-                        v[u] = vals[x];
-                    } else {
-                        bad |= kStatusBadPosting;
-                    }
-                }
+                const bool in = x + u >= lo && x + u < hi;
+                d[u] = idv[u] - base_doc;
+                ok[u] = in && (unsigned)d[u] < (unsigned)kTile;
+                if (in && !ok[u])
+                    bad |= kStatusBadPosting;
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                if (d[u] >= 0)
+                if (ok[u])
                     r[u] = row[d[u]];
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                if (d[u] >= 0)
-                    row[d[u]] = r[u] + v[u];
+                if (ok[u])
+                    row[d[u]] = r[u] + vv[u];
         }
         __syncwarp();
         if (lane == 0)
