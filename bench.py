@@ -75,7 +75,7 @@ def algorithmic_bytes(df, vocab, offsets, words, k, distinct=False):
     return total + (offsets.size - 1) * k * 8
 
 
-def traffic_from_profile(name='stream_search_kernel_synthetic_10m.txt'):
+def traffic_from_profile(name='tile_group_kernel_synthetic_10m.txt'):
     """DRAM bytes per launch from the committed ncu summary, if present."""
     path = ROOT / 'profiles' / name
     if not path.exists():
@@ -359,7 +359,10 @@ def main():
     search_achieved = bytes_total / (sum(step_ms) / 1e3) / 1e9
     launches_per_search = 1 if info['kernel'] == 1 else 3
     peak, peak_kind = hbm_peak()
-    traffic = traffic_from_profile()
+    traffic = traffic_from_profile({0: 'stream_search_kernel_synthetic_10m.txt',
+                                    4: 'tile_group_kernel_synthetic_10m.txt'}.get(info['kernel'], '-'))
+    if args.docs or args.vocab:
+        traffic = None  # the profiles cover the full-size workload
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
