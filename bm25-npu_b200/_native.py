@@ -31,6 +31,7 @@ class Options(ctypes.Structure):
         ('kernel', c_int32),
         ('ring_stages', c_int32),
         ('ring_chunk', c_int32),
+        ('prune', c_int32),
     ]
 
 
@@ -74,6 +75,24 @@ SIGNATURES = {
     'bm25_get_info': (c_int, [c_void_p, POINTER(Info)]),
     'bm25_kernel_timing': (c_int, [c_void_p, c_int32]),
     'bm25_kernel_times': (c_int, [c_void_p, POINTER(c_float), c_int64, POINTER(c_int64)]),
+    'bm25_search_pruned_device': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p,
+                                          c_void_p, c_void_p, c_void_p]),
+    'bm25_search_pruned': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p,
+                                   c_void_p]),
+    'bm25_set_threshold_model': (c_int, [c_void_p, c_void_p, c_float]),
+    'bm25_query_features_device': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p,
+                                           c_void_p]),
+    'bm25_search_learned': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p]),
+    'bm25_search_learned_device': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p,
+                                           c_void_p, c_void_p]),
+    'bm25_search_stats': (c_int, [c_void_p, c_void_p, c_int32]),
+    'bm25_mlp_param_count': (c_int64, []),
+    'bm25_mlp_scratch_floats': (c_int64, [c_int64]),
+    'bm25_mlp_forward': (c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
+    'bm25_mlp_gradient': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_float, c_void_p, c_void_p, c_void_p,
+                                  c_void_p]),
+    'bm25_mlp_adam': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_float, c_int32, c_void_p]),
+    'bm25_mlp_last_error': (c_int, [ctypes.c_char_p, c_size_t]),
     'bm25_search_csc_static': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_int64,
                                        c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_int32]),
 }

@@ -19,8 +19,8 @@ INCLUDE = ROOT / 'include'
 NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
-ENGINE_SOURCES = ['engine.cu']
-ENGINE_HEADERS = ['tile_kernels.cuh', 'stream_kernel.cuh', 'tile_group_kernel.cuh']
+ENGINE_SOURCES = ['engine.cu', 'mlp.cu']
+ENGINE_HEADERS = ['tile_kernels.cuh', 'stream_kernel.cuh', 'tile_group_kernel.cuh', 'learned_kernels.cuh', 'mlp.cuh']
 
 
 def _stale(target, sources):

@@ -9,6 +9,7 @@
 // and one CUDA graph per (Q, K) holding H2D -> fused scoring/selection/merge ->
 // D2H.  Search = validate + pack, graph replay, synchronise, validate result.
 #include "bm25_b200.h"
+#include "learned_kernels.cuh"
 #include "stream_kernel.cuh"
 #include "tile_group_kernel.cuh"
 #include "tile_kernels.cuh"
@@ -25,6 +26,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -157,6 +159,7 @@ class Engine {
         Check(o.max_k <= docs, "max_k exceeds the document count");
         Check(o.query_capacity >= 1 && o.query_capacity <= 65535, "query_capacity must be in [1, 65535]");
         Check(o.word_capacity >= 0 && o.word_capacity <= 16777216, "word_capacity must be in [0, 2^24]");
+        Check(!o.prune || o.kernel == BM25_KERNEL_TILE_GROUP, "prune needs the tile-group kernel");
         Cuda(cudaSetDevice(o.device_id), "cudaSetDevice");
         device_ = o.device_id;
         size_t total = 0;
@@ -276,6 +279,150 @@ class Engine {
         }
     }
 
+    // Pruned Search on device buffers: tau [q] starting bounds (nullptr: learned bounds),
+    // out_exact [q] flags; queries whose bound proved too high are answered by the retry pass.
+    void SearchPrunedDevice(const int64_t *qoffsets, const int32_t *words, const float *tau, int64_t q, int32_t k,
+                            float *out_scores, int32_t *out_ids, int32_t *out_exact, cudaStream_t stream)
+    {
+        RequireUsable();
+        RequirePrune();
+        Check(q >= 1 && q <= opts_.query_capacity, "Query batch exceeds declared capacity or is empty");
+        Check(k >= 1 && k <= opts_.max_k && k <= docs_, "K outside [1, min(max_k, N)]");
+        Check(qoffsets && words && out_scores && out_ids && out_exact, "Null device buffer");
+        try {
+            Cuda(cudaSetDevice(device_), "cudaSetDevice");
+            cudaStream_t s = stream ? stream : stream_;
+            Cuda(cudaStreamWaitEvent(s, done_, 0), "cudaStreamWaitEvent");
+            ++searches_;
+            marking_ = !timing_.empty();
+            Launch((int)q, k, qoffsets, words, out_scores, out_ids, d_dev_status_, s, tau ? tau : d_tau_, out_exact,
+                   tau == nullptr);
+            if (marking_)
+                ++timed_;
+            marking_ = false;
+            Cuda(cudaEventRecord(done_, s), "cudaEventRecord");
+        } catch (...) {
+            failed_ = true;
+            throw;
+        }
+    }
+
+    // Pruned Search on host buffers: one graph replay (H2D, pruned Search, retry pass, D2H).
+    // out_exact[i] = 1 where the pruned result stood, 0 where the retry pass answered.
+    // tau == nullptr: the starting bounds come from the learned-bound kernel (the session's
+    // threshold model, or the safe bounds alone without one).
+    void SearchPruned(const int64_t *qoffsets, const int32_t *words, const float *tau, int64_t q, int32_t k,
+                      float *out_scores, int32_t *out_ids, int32_t *out_exact)
+    {
+        RequireUsable();
+        RequirePrune();
+        Check(out_scores && out_ids && out_exact, "Null buffer");
+        Pack(qoffsets, words, q, k);
+        if (tau)
+            std::memcpy(static_cast<unsigned char *>(h_in_) + tau_offset_, tau, q * sizeof(float));
+        try {
+            Cuda(cudaSetDevice(device_), "cudaSetDevice");
+            cudaGraphExec_t exec = GraphFor((int)q, k, tau ? kModePruned : kModeLearned);
+            Cuda(cudaStreamWaitEvent(stream_, done_, 0), "cudaStreamWaitEvent");
+            ++searches_;
+            Cuda(cudaGraphLaunch(exec, stream_), "cudaGraphLaunch");
+            ++replays_;
+            Cuda(cudaEventRecord(done_, stream_), "cudaEventRecord");
+            Cuda(cudaStreamSynchronize(stream_), "complete pruned Search through result D2H");
+            Receive(q, k, out_scores, out_ids);
+        } catch (...) {
+            failed_ = true;
+            throw;
+        }
+        const int32_t *exact =
+            reinterpret_cast<const int32_t *>(static_cast<const unsigned char *>(h_out_) + ExactOffset((int)q, k));
+        for (int64_t i = 0; i < q; ++i)
+            out_exact[i] = exact[i] ? 1 : 0;
+    }
+
+    // Threshold model of the learned bounds (host params, bm25mlp::kParams floats), or none.
+    void SetThresholdModel(const float *params, float margin)
+    {
+        RequireUsable();
+        RequirePrune();
+        Check(!params || std::isfinite(margin), "margin must be finite");
+        if (params)
+            for (int i = 0; i < bm25mlp::kParams; ++i)
+                Check(std::isfinite(params[i]), "Threshold model holds a non-finite parameter");
+        Cuda(cudaSetDevice(device_), "cudaSetDevice");
+        Cuda(cudaStreamWaitEvent(stream_, done_, 0), "cudaStreamWaitEvent");
+        Cuda(cudaStreamSynchronize(stream_), "model update");
+        if (params)
+            Cuda(cudaMemcpy(d_model_, params, bm25mlp::kParams * sizeof(float), cudaMemcpyHostToDevice),
+                 "model upload");
+        has_model_ = params != nullptr;
+        margin_ = params ? margin : 0.0f;
+        // graphs hold the model pointer and margin by value: rebuild the learned ones
+        for (auto it = graphs_.begin(); it != graphs_.end();) {
+            if (std::get<2>(it->first) == kModeLearned) {
+                cudaGraphExecDestroy(it->second);
+                it = graphs_.erase(it);
+            } else {
+                ++it;
+            }
+        }
+    }
+
+    // Query features [q][32] and safe bounds [q] on device buffers (training data of the model).
+    void QueryFeaturesDevice(const int64_t *qoffsets, const int32_t *words, int64_t q, int32_t k, float *features,
+                             float *safe, cudaStream_t stream)
+    {
+        RequireUsable();
+        RequirePrune();
+        Check(q >= 1 && q <= opts_.query_capacity, "Query batch exceeds declared capacity or is empty");
+        Check(k >= 1 && k <= opts_.max_k && k <= docs_, "K outside [1, min(max_k, N)]");
+        Check(qoffsets && words && features, "Null device buffer");
+        Cuda(cudaSetDevice(device_), "cudaSetDevice");
+        cudaStream_t s = stream ? stream : stream_;
+        Cuda(cudaStreamWaitEvent(s, done_, 0), "cudaStreamWaitEvent");
+        bm25k::LearnedArgs la = LearnedArgsFor((int)q, k, qoffsets, words);
+        la.features = features;
+        la.safe = safe;
+        bm25k::QueryFeaturesKernel<<<(int)((q + 127) / 128), 128, 0, s>>>(la);
+        Cuda(cudaGetLastError(), "feature kernel launch");
+        Cuda(cudaEventRecord(done_, s), "cudaEventRecord");
+    }
+
+    // Tile-group counters since the last reset: claims, claims dropped, tiles scanned, postings copied.
+    void SearchStats(uint64_t *out, bool reset)
+    {
+        RequireUsable();
+        Check(out != nullptr, "Null output");
+        Cuda(cudaSetDevice(device_), "cudaSetDevice");
+        Cuda(cudaStreamWaitEvent(stream_, done_, 0), "cudaStreamWaitEvent");
+        Cuda(cudaStreamSynchronize(stream_), "stats");
+        if (!d_stats_) {
+            std::memset(out, 0, 4 * sizeof(uint64_t));
+            return;
+        }
+        Cuda(cudaMemcpy(out, d_stats_, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost), "stats D2H");
+        if (reset)
+            Cuda(cudaMemset(d_stats_, 0, 4 * sizeof(uint64_t)), "stats reset");
+    }
+
+    bm25k::LearnedArgs LearnedArgsFor(int q, int k, const int64_t *qoffsets, const int32_t *words) const
+    {
+        bm25k::LearnedArgs la{};
+        la.indptr = (const long long *)d_indptr_;
+        la.top = d_term_top_;
+        la.mean = d_term_mean_;
+        la.vocab = (int)vocab_;
+        la.qoffsets = (const long long *)qoffsets;
+        la.words = words;
+        la.q = q;
+        la.k = k;
+        la.word_cap = std::max<int64_t>(1, opts_.word_capacity);
+        la.params = has_model_ ? d_model_ : nullptr;
+        la.margin = margin_;
+        la.tau = d_tau_;
+        return la;
+    }
+
     // Event timing of the main search kernel (StreamSearchKernel or
     // TileSearchKernel) for device-resident Searches: a ring of event pairs
     // recorded on the launching stream around that one launch.
@@ -364,6 +511,12 @@ class Engine {
     }
 
   private:
+    void RequirePrune() const
+    {
+        if (!opts_.prune || plan_.kernel != BM25_KERNEL_TILE_GROUP)
+            throw InvalidState("Pruned Search needs a session created with prune = 1 and the tile-group kernel");
+    }
+
     void RequireUsable() const
     {
         if (closed_ || failed_)
@@ -488,13 +641,38 @@ class Engine {
             bm25k::BuildDirectoryKernel<<<grid, 256, 0, stream_>>>((const long long *)d_indptr_, d_indices_, d_terms,
                                                                    rows, plan_.tile_docs, tiles, d_dir_, tiles + 1);
             Cuda(cudaGetLastError(), "directory kernel launch");
+            if (opts_.prune) {
+                d_dir_max_ = static_cast<float *>(Alloc(rows * (size_t)tiles * sizeof(float), "cudaMalloc dir max"));
+                const long long cells = rows * (long long)tiles;
+                bm25k::BuildDirMaxKernel<<<(int)std::min<long long>((cells + 255) / 256, 148 * 64), 256, 0, stream_>>>(
+                    (const long long *)d_indptr_, d_data_, d_terms, d_dir_, rows, tiles, tiles + 1, d_dir_max_);
+                Cuda(cudaGetLastError(), "directory bound kernel launch");
+            }
             Cuda(cudaStreamSynchronize(stream_), "directory kernel");
+        }
+        if (opts_.prune) {
+            wbound_ = static_cast<float *>(Alloc(std::max<size_t>(1, opts_.word_capacity) * (size_t)tiles *
+                                                     sizeof(float),
+                                                 "cudaMalloc word bounds"));
+            d_term_top_ = static_cast<float *>(Alloc(vocab_ * bm25k::kTermTop * sizeof(float), "cudaMalloc term top"));
+            d_term_mean_ = static_cast<float *>(Alloc(vocab_ * sizeof(float), "cudaMalloc term mean"));
+            d_model_ = static_cast<float *>(Alloc(bm25mlp::kParams * sizeof(float), "cudaMalloc model"));
+            d_tau_ = static_cast<float *>(Alloc(opts_.query_capacity * sizeof(float), "cudaMalloc tau"));
+            d_fail_list_ = static_cast<int *>(Alloc(opts_.query_capacity * sizeof(int), "cudaMalloc fail list"));
+            d_fail_count_ = static_cast<unsigned *>(Alloc(sizeof(unsigned), "cudaMalloc fail count"));
+            Cuda(cudaMemset(d_fail_count_, 0, sizeof(unsigned)), "cudaMemset");
+            const int grid = (int)std::min<long long>((vocab_ + 7) / 8, 148 * 16);
+            bm25k::TermStatsKernel<<<grid, 256, 0, stream_>>>((const long long *)d_indptr_, d_data_, vocab_,
+                                                               d_term_top_, d_term_mean_);
+            Cuda(cudaGetLastError(), "term statistics kernel launch");
+            Cuda(cudaStreamSynchronize(stream_), "term statistics kernel");
         }
         // Query packet / result arenas (fixed_query_packet.h:15-25 layout).
         word_offset_ = Align32((opts_.query_capacity + 1) * sizeof(int64_t));
-        in_bytes_ = Align32(word_offset_ + std::max<int64_t>(1, opts_.word_capacity) * sizeof(int32_t));
+        tau_offset_ = Align32(word_offset_ + std::max<int64_t>(1, opts_.word_capacity) * sizeof(int32_t));
+        in_bytes_ = tau_offset_ + (opts_.prune ? Align32(opts_.query_capacity * sizeof(float)) : 0);
         const size_t qk = (size_t)opts_.query_capacity * opts_.max_k;
-        out_bytes_ = Align32(qk * 4) * 2 + 32;
+        out_bytes_ = Align32(qk * 4) * 2 + 32 + Align32(opts_.query_capacity * sizeof(int32_t));
         Cuda(cudaHostAlloc(&h_in_, in_bytes_, cudaHostAllocDefault), "cudaHostAlloc");
         Cuda(cudaHostAlloc(&h_out_, out_bytes_, cudaHostAllocDefault), "cudaHostAlloc");
         std::memset(h_in_, 0, in_bytes_);
@@ -558,14 +736,18 @@ class Engine {
             plan_entries_ = static_cast<bm25k::PlanEntry *>(
                 Alloc(std::max<size_t>(1, opts_.word_capacity) * tiles_z * sizeof(bm25k::PlanEntry), "cudaMalloc plan"));
             Cuda(cudaMemset(ctrl_, 0, sizeof(bm25k::StreamCtrl)), "cudaMemset");
+            d_stats_ = static_cast<unsigned long long *>(Alloc(4 * sizeof(unsigned long long), "cudaMalloc stats"));
+            Cuda(cudaMemset(d_stats_, 0, 4 * sizeof(unsigned long long)), "cudaMemset");
             Cuda(cudaMemset(threshold_, 0, qc * sizeof(unsigned)), "cudaMemset");
             Cuda(cudaMemset(cand_count_, 0, qc * sizeof(unsigned)), "cudaMemset");
         }
         Cuda(cudaDeviceSynchronize(), "index preparation");
     }
 
+    // tau / exact: the pruned Search's starting bounds and exactness flags (nullptr: plain Search).
     void Launch(int q, int k, const int64_t *qoffsets, const int32_t *words, float *out_scores, int32_t *out_ids,
-                unsigned *status, cudaStream_t s)
+                unsigned *status, cudaStream_t s, const float *tau = nullptr, int32_t *exact = nullptr,
+                bool learned = false)
     {
         bm25k::TileArgs a{};
         a.indptr = (const long long *)d_indptr_;
@@ -624,8 +806,27 @@ class Engine {
             sa.out_scores = out_scores;
             sa.out_ids = out_ids;
             sa.status = status;
+            sa.stats = plan_.kernel == BM25_KERNEL_TILE_GROUP ? d_stats_ : nullptr;
+            if (learned) {  // tau is this session's bound array, written here
+                const bm25k::LearnedArgs la = LearnedArgsFor(q, k, qoffsets, words);
+                bm25k::LearnedBoundKernel<<<(q + bm25k::kLearnedThreads - 1) / bm25k::kLearnedThreads,
+                                            bm25k::kLearnedThreads, 0, s>>>(la);
+                Cuda(cudaGetLastError(), "learned bound kernel launch");
+            }
+            if (tau) {
+                sa.dir_max = d_dir_max_;
+                sa.wbound = wbound_;
+                sa.tau = tau;
+                sa.exact = exact;
+                sa.fail_list = d_fail_list_;
+                sa.fail_count = d_fail_count_;
+            }
             bm25k::PlanKernel<<<bm25k::PlanGrid(opts_.word_capacity, plan_.tiles, sms_), bm25k::kPlanThreads, 0, s>>>(sa);
             Cuda(cudaGetLastError(), "plan kernel launch");
+            if (tau) {
+                bm25k::SeedBoundKernel<<<(q + 255) / 256, 256, 0, s>>>(sa);
+                Cuda(cudaGetLastError(), "seed kernel launch");
+            }
             if (plan_.kernel == 0) {
                 const int grid = (int)std::min<long long>(
                     plan_.grid, ((long long)q * plan_.tiles + bm25k::kTaskBatch - 1) / bm25k::kTaskBatch);
@@ -646,12 +847,32 @@ class Engine {
                 MarkKernel(1, s);
             }
             bm25k::FinalSelectKernel<<<q, bm25k::kFinalThreads, 0, s>>>(sa);
+            if (tau) {
+                // retry pass: the queries whose bound proved too high, on the plain path (an
+                // empty fail list ends both kernels at once)
+                Cuda(cudaGetLastError(), "final select launch");
+                bm25k::StreamArgs ra = sa;
+                ra.wbound = nullptr;
+                ra.dir_max = nullptr;
+                ra.tau = nullptr;
+                ra.exact = nullptr;
+                ra.retry = 1;
+                const long long claims = (long long)q * ((plan_.tiles + bm25k::kWgWarps - 1) / bm25k::kWgWarps);
+                const int grid = (int)std::max<long long>(1, std::min<long long>(plan_.grid, claims));
+                if (plan_.tile_docs == 2048)
+                    bm25k::TileGroupKernel<2048><<<grid, bm25k::kWgThreads, smem_bytes_, s>>>(ra);
+                else
+                    bm25k::TileGroupKernel<1024><<<grid, bm25k::kWgThreads, smem_bytes_, s>>>(ra);
+                Cuda(cudaGetLastError(), "retry kernel launch");
+                bm25k::FinalSelectKernel<<<q, bm25k::kFinalThreads, 0, s>>>(ra);
+            }
         }
         Cuda(cudaGetLastError(), "search kernel launch");
     }
 
     size_t IdOffset(int q, int k) const { return Align32((size_t)q * k * 4); }
     size_t StatusOffset(int q, int k) const { return Align32(IdOffset(q, k) + (size_t)q * k * 4); }
+    size_t ExactOffset(int q, int k) const { return StatusOffset(q, k) + 32; }
 
     void MarkKernel(int which, cudaStream_t s)
     {
@@ -667,9 +888,12 @@ class Engine {
         timed_ = 0;
     }
 
-    cudaGraphExec_t GraphFor(int q, int k)
+    static constexpr int kModePlain = 0, kModePruned = 1, kModeLearned = 2;
+
+    cudaGraphExec_t GraphFor(int q, int k, int mode = kModePlain)
     {
-        const auto key = std::make_pair(q, k);
+        const auto key = std::make_tuple(q, k, mode);
+        const bool pruned = mode != kModePlain;
         auto it = graphs_.find(key);
         if (it != graphs_.end())
             return it->second;
@@ -677,13 +901,21 @@ class Engine {
         cudaGraphExec_t exec = nullptr;
         Cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin graph capture");
         try {
-            Cuda(cudaMemcpyAsync(d_in_, h_in_, in_bytes_, cudaMemcpyHostToDevice, stream_), "query H2D");
+            // the plain Search sends the query packet; the pruned one adds the bounds after it
+            Cuda(cudaMemcpyAsync(d_in_, h_in_, mode == kModePruned ? tau_offset_ + (size_t)q * sizeof(float) : tau_offset_,
+                                 cudaMemcpyHostToDevice, stream_),
+                 "query H2D");
             unsigned *status = reinterpret_cast<unsigned *>(d_out_ + StatusOffset(q, k));
             Cuda(cudaMemsetAsync(status, 0, sizeof(unsigned), stream_), "status reset");
             Launch(q, k, reinterpret_cast<const int64_t *>(d_in_), reinterpret_cast<const int32_t *>(d_in_ + word_offset_),
                    reinterpret_cast<float *>(d_out_), reinterpret_cast<int32_t *>(d_out_ + IdOffset(q, k)), status,
-                   stream_);
-            Cuda(cudaMemcpyAsync(h_out_, d_out_, StatusOffset(q, k) + 32, cudaMemcpyDeviceToHost, stream_),
+                   stream_,
+                   mode == kModePruned ? reinterpret_cast<const float *>(d_in_ + tau_offset_)
+                                       : (mode == kModeLearned ? d_tau_ : nullptr),
+                   pruned ? reinterpret_cast<int32_t *>(d_out_ + ExactOffset(q, k)) : nullptr,
+                   mode == kModeLearned);
+            Cuda(cudaMemcpyAsync(h_out_, d_out_, pruned ? ExactOffset(q, k) + (size_t)q * 4 : StatusOffset(q, k) + 32,
+                                 cudaMemcpyDeviceToHost, stream_),
                  "top-K D2H");
         } catch (...) {
             cudaStreamEndCapture(stream_, &graph);
@@ -780,7 +1012,8 @@ class Engine {
     float *d_data_ = nullptr;
     int32_t *d_dir_row_ = nullptr, *d_dir_ = nullptr;
     std::vector<bm25k::Level> levels_;
-    size_t word_offset_ = 0, in_bytes_ = 0, out_bytes_ = 0, smem_bytes_ = 0;
+    size_t word_offset_ = 0, tau_offset_ = 0, in_bytes_ = 0, out_bytes_ = 0, smem_bytes_ = 0;
+    float *d_dir_max_ = nullptr, *wbound_ = nullptr;
     void *h_in_ = nullptr, *h_out_ = nullptr;
     unsigned char *d_in_ = nullptr, *d_out_ = nullptr;
     unsigned *d_dev_status_ = nullptr;
@@ -791,7 +1024,13 @@ class Engine {
     long long cand_cap_ = 0;
     bm25k::PlanEntry *plan_entries_ = nullptr;
     int sms_ = 148;
-    std::map<std::pair<int, int>, cudaGraphExec_t> graphs_;
+    std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs_;
+    float *d_term_top_ = nullptr, *d_term_mean_ = nullptr, *d_model_ = nullptr, *d_tau_ = nullptr;
+    unsigned long long *d_stats_ = nullptr;
+    int *d_fail_list_ = nullptr;
+    unsigned *d_fail_count_ = nullptr;
+    bool has_model_ = false;
+    float margin_ = 0.0f;
     bool closed_ = false, failed_ = false;
     int64_t replays_ = 0, searches_ = 0;
     static constexpr int64_t kTimingRing = 4096;
@@ -946,6 +1185,114 @@ int bm25_search_device(bm25_handle *h, const int64_t *qoffsets, const int32_t *w
             if (!h->engine)
                 throw bm25b200::InvalidState("BM25 is not initialized");
             h->engine->SearchDevice(qoffsets, words, q, k, out_scores, out_ids, static_cast<cudaStream_t>(stream));
+        },
+        h->error, h->code);
+}
+
+int bm25_search_pruned_device(bm25_handle *h, const int64_t *qoffsets, const int32_t *words, const float *tau,
+                              int64_t q, int32_t k, float *out_scores, int32_t *out_ids, int32_t *out_exact,
+                              void *stream)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            bm25b200::Check(tau != nullptr, "Null tau buffer");
+            h->engine->SearchPrunedDevice(qoffsets, words, tau, q, k, out_scores, out_ids, out_exact,
+                                          static_cast<cudaStream_t>(stream));
+        },
+        h->error, h->code);
+}
+
+int bm25_search_pruned(bm25_handle *h, const int64_t *qoffsets, const int32_t *words, const float *tau, int64_t q,
+                       int32_t k, float *out_scores, int32_t *out_ids, int32_t *out_exact)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            bm25b200::Check(tau != nullptr, "Null tau buffer");
+            h->engine->SearchPruned(qoffsets, words, tau, q, k, out_scores, out_ids, out_exact);
+        },
+        h->error, h->code);
+}
+
+int bm25_search_learned(bm25_handle *h, const int64_t *qoffsets, const int32_t *words, int64_t q, int32_t k,
+                        float *out_scores, int32_t *out_ids, int32_t *out_exact)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            h->engine->SearchPruned(qoffsets, words, nullptr, q, k, out_scores, out_ids, out_exact);
+        },
+        h->error, h->code);
+}
+
+int bm25_search_learned_device(bm25_handle *h, const int64_t *qoffsets, const int32_t *words, int64_t q, int32_t k,
+                               float *out_scores, int32_t *out_ids, int32_t *out_exact, void *stream)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            h->engine->SearchPrunedDevice(qoffsets, words, nullptr, q, k, out_scores, out_ids, out_exact,
+                                          static_cast<cudaStream_t>(stream));
+        },
+        h->error, h->code);
+}
+
+int bm25_set_threshold_model(bm25_handle *h, const float *params, float margin)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            h->engine->SetThresholdModel(params, margin);
+        },
+        h->error, h->code);
+}
+
+int bm25_query_features_device(bm25_handle *h, const int64_t *qoffsets, const int32_t *words, int64_t q, int32_t k,
+                               float *features, float *safe, void *stream)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            h->engine->QueryFeaturesDevice(qoffsets, words, q, k, features, safe, static_cast<cudaStream_t>(stream));
+        },
+        h->error, h->code);
+}
+
+int bm25_search_stats(bm25_handle *h, uint64_t *out, int32_t reset)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            h->engine->SearchStats(out, reset != 0);
         },
         h->error, h->code);
 }

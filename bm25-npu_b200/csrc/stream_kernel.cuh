@@ -105,6 +105,17 @@ struct StreamArgs {
     float *out_scores;
     int *out_ids;
     unsigned *status;
+    // pruned Search (tile-group kernel): nullptr on the plain path
+    const float *dir_max;  // [dir row][tile] largest posting score of the row's term in the tile
+    float *wbound;         // [word][tile] upper bound of the word's score in the tile (PlanKernel output)
+    const float *tau;      // [Q] starting bound guesses
+    int *exact;            // [Q] 1 where K candidates reached tau
+    int *fail_list;        // queries whose pruned pass fell short, in the order found
+    unsigned *fail_count;  // their count (reset by SeedBoundKernel)
+    int retry;             // nonzero: this pass searches the fail_list queries on the plain path
+    // tile-group kernel counters, accumulated (nullptr: not kept): claims taken, claims dropped
+    // whole by their bounds, tiles scanned, postings copied into the rings
+    unsigned long long *stats;
 };
 
 struct __align__(16) StageMeta {
@@ -456,23 +467,33 @@ __global__ void __launch_bounds__(kPlanThreads) PlanKernel(const StreamArgs a)
     for (long long w = blockIdx.x; w < total; w += gridDim.x) {
         const int term = a.words[w];
         PlanEntry *out = a.plan + w * a.tiles;
+        float *wb = a.wbound ? a.wbound + w * a.tiles : nullptr;
         if (term < 0 || term >= a.vocab) {
             if (term < 0 && tid == 0 && blockIdx.y == 0)
                 atomicOr(a.status, kStatusBadWord);
-            for (int t = t0 + tid; t < t1; t += kPlanThreads)
+            for (int t = t0 + tid; t < t1; t += kPlanThreads) {
                 out[t] = PlanEntry{0, 0};
+                if (wb)
+                    wb[t] = 0.0f;
+            }
             continue;
         }
         const long long s = a.indptr[term], e = a.indptr[term + 1];
         const int r = a.dir_row ? a.dir_row[term] : -1;
         if (r >= 0) {
             const int *d = a.dir + (long long)r * a.dir_stride;
-            for (int t = t0 + tid; t < t1; t += kPlanThreads)
+            for (int t = t0 + tid; t < t1; t += kPlanThreads) {
                 out[t] = PlanEntry{s + d[t], s + d[t + 1]};
+                if (wb)
+                    wb[t] = a.dir_max[(long long)r * a.tiles + t];
+            }
             continue;
         }
-        for (int t = t0 + tid; t < t1; t += kPlanThreads)
+        for (int t = t0 + tid; t < t1; t += kPlanThreads) {
             out[t] = PlanEntry{0, 0};
+            if (wb)
+                wb[t] = 0.0f;
+        }
         if (tid < 32) {
             // lists up to kPlanScanAll postings are scanned whole by every CTA of the word; a
             // longer one (a list left out of the directory by its byte budget) is first cut to
@@ -497,6 +518,8 @@ __global__ void __launch_bounds__(kPlanThreads) PlanKernel(const StreamArgs a)
                 out[t].b = i;
             if (i == e - 1 || __ldg(a.indices + i + 1) / a.tile_docs != t)
                 out[t].e = i + 1;
+            if (wb)  // bits of scores >= 0 order like the values (a negative one is bounded by 0)
+                atomicMax(reinterpret_cast<unsigned *>(wb + t), __float_as_uint(fmaxf(__ldg(a.data + i), 0.0f)));
         }
         __syncthreads();  // range[] is rewritten for the next word
     }
@@ -810,7 +833,13 @@ __global__ void __launch_bounds__(kFinalThreads) FinalSelectKernel(const StreamA
     __shared__ float wv[kWarps];
     __shared__ unsigned surv_count;
     __shared__ int sel_count;
-    const int q = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    int q = blockIdx.x;
+    if (a.retry) {  // block b answers the b-th query of the fail list
+        if ((unsigned)q >= __ldcg(a.fail_count))
+            return;
+        q = __ldcg(a.fail_list + q);
+    }
     const int k = a.k;
     const unsigned appended = __ldcg(a.cand_count + q);
     const int n = (int)min((long long)appended, a.cand_cap);
@@ -950,11 +979,46 @@ __global__ void __launch_bounds__(kFinalThreads) FinalSelectKernel(const StreamA
             a.out_scores[(long long)q * k + lane] = ls;
             a.out_ids[(long long)q * k + lane] = li;
         }
+        if (a.exact && !a.retry && lane == 0) {  // K results at or above the starting bound, or no bound
+            const int ok = cnt == k || !(a.tau[q] > 0.0f) ? 1 : 0;
+            a.exact[q] = ok;
+            if (!ok)
+                a.fail_list[atomicAdd(a.fail_count, 1u)] = q;
+        }
         if (lane == 0) {
             a.cand_count[q] = 0u;
             a.threshold[q] = 0u;
         }
         a.tslots[(long long)q * 32 + lane] = 0u;
+    }
+}
+
+// Pruned Search: each query's running bound starts at its guess tau[q] (>= 0).
+__global__ void SeedBoundKernel(const StreamArgs a)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        *a.fail_count = 0u;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < a.q; q += gridDim.x * blockDim.x) {
+        const float t = a.tau[q];
+        a.threshold[q] = t > 0.0f ? __float_as_uint(t) : 0u;  // NaN or negative: no bound
+    }
+}
+
+// dir_max[r][t] = largest posting score of directory row r's term inside tile t.
+__global__ void BuildDirMaxKernel(const long long *indptr, const float *data, const int *dir_terms, const int *dir,
+                                  long long rows, int tiles, long long stride, float *dir_max)
+{
+    const long long total = rows * (long long)tiles;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / tiles;
+        const int t = (int)(i % tiles);
+        const long long s = indptr[dir_terms[r]];
+        const int *d = dir + r * stride;
+        float m = 0.0f;
+        for (long long p = s + d[t]; p < s + d[t + 1]; ++p)
+            m = fmaxf(m, data[p]);
+        dir_max[i] = m;
     }
 }
 

@@ -28,6 +28,15 @@
 // most tiles append nothing.  Consecutive claims walk the queries of one tile
 // group, so every query gets tiles early and words that queries share are read
 // from DRAM once and from L2 after.  FinalSelectKernel finishes every query.
+//
+// Pruned Search (a.wbound set): the running bound starts at the query's guess
+// tau, and the producer adds, per tile of a claim, the query words' per-tile
+// score maxima in query-word order -- an FP32 upper bound of every document's
+// sum in that tile, since rounded addition is monotone in both operands -- and
+// drops the tiles whose bound is below the claim's running bound (a whole
+// claim when all eight are).  A dropped tile holds no document scoring at or
+// above the bound, so it holds none of the top K whenever K documents reach
+// tau; FinalSelectKernel reports whether they did.
 #pragma once
 #include "stream_kernel.cuh"
 
@@ -184,12 +193,14 @@ struct WgClaim {
     unsigned thr_bits;   // the query's threshold
     unsigned slot_bits;  // lane g < k: group slot g (others: all ones)
     int2 p0, p1;         // lane l: word l / 8 (p0) and 4 + l / 8 (p1) in tile tile0 + l % 8; .x = b, .y = e
+    float b0, b1;        // pruned Search: the same words' score bounds in the same tiles
 };
 
-// Range of word s (>= kWgPlanWords, warp-uniform) in tile j of the claim, from the plan.
-__device__ __forceinline__ int2 WgFarRange(const StreamArgs &a, const WgClaim &c, int s, int j)
+// Range of word s (>= kWgPlanWords, warp-uniform) in tile j of the claim, from the plan;
+// empty for a tile outside the kept set `keep` (bit j).
+__device__ __forceinline__ int2 WgFarRange(const StreamArgs &a, const WgClaim &c, int s, int j, unsigned keep)
 {
-    if (c.tile0 + j >= a.tiles)
+    if (c.tile0 + j >= a.tiles || !((keep >> j) & 1u))
         return make_int2(0, 0);
     const PlanEntry pe = a.plan[(c.qb + s) * a.tiles + c.tile0 + j];
     return make_int2((int)pe.b, (int)pe.e);
@@ -220,7 +231,9 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
     __syncthreads();
     volatile int *abort = &sh.abort;
     const unsigned groups = (unsigned)((a.tiles + kWgWarps - 1) / kWgWarps);
-    const unsigned claims = (unsigned)a.q * groups;
+    // a retry pass covers only the queries on the fail list (possibly none)
+    const unsigned nq = a.retry ? __ldcg(a.fail_count) : (unsigned)a.q;
+    const unsigned claims = nq * groups;
 
     if (warp == kWgWarps) {
         // ================= producer warp =================
@@ -229,6 +242,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
         unsigned wraps = 0;        // times the ring has wrapped
         unsigned bad = 0;
         bool dead = false;
+        unsigned long long n_claims = 0, n_dropped = 0, n_tiles = 0, n_copied = 0;  // lane 0's counts
         // Waits until stage pst is free (its previous use released).
         auto claim_stage = [&]() -> bool {
             int ok = 1;
@@ -250,12 +264,15 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
         // claim index -> query and group: consecutive claims walk the queries of one group
         auto decode = [&](unsigned c, WgClaim &w) {
             w.valid = c < claims;
-            w.q = (int)(c % (unsigned)a.q);
-            w.tile0 = (int)(c / (unsigned)a.q) * kWgWarps;
+            w.q = w.valid ? (int)(c % nq) : 0;
+            if (a.retry && w.valid)
+                w.q = __ldcg(a.fail_list + w.q);
+            w.tile0 = w.valid ? (int)(c / nq) * kWgWarps : 0;
             w.n = 0;
             w.qb = w.qe = 0;
             w.p0 = make_int2(0, 0);
             w.p1 = make_int2(0, 0);
+            w.b0 = w.b1 = 0.0f;
             w.thr_bits = 0u;
             w.slot_bits = 0xffffffffu;
         };
@@ -279,10 +296,14 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
             if (tile_ok && s0 < w.n) {
                 const PlanEntry pe = a.plan[(w.qb + s0) * a.tiles + w.tile0 + j];
                 w.p0 = make_int2((int)pe.b, (int)pe.e);
+                if (a.wbound)
+                    w.b0 = a.wbound[(w.qb + s0) * a.tiles + w.tile0 + j];
             }
             if (tile_ok && s0 + 4 < w.n) {
                 const PlanEntry pe = a.plan[(w.qb + s0 + 4) * a.tiles + w.tile0 + j];
                 w.p1 = make_int2((int)pe.b, (int)pe.e);
+                if (a.wbound)
+                    w.b1 = a.wbound[(w.qb + s0 + 4) * a.tiles + w.tile0 + j];
             }
             w.thr_bits = __ldcg(a.threshold + w.q);
             if (lane < a.k)
@@ -312,6 +333,33 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
 
             const float thr =
                 fmaxf(__uint_as_float(cur.thr_bits), __uint_as_float(__reduce_min_sync(kFull, cur.slot_bits)));
+            unsigned keep = 0xffu;
+            ++n_claims;
+            if (a.wbound) {
+                // lane l bounds tile l % 8: the words' tile maxima added in query-word order
+                const int j = lane & 7;
+                float bound = 0.0f;
+                for (int s = 0; s < cur.n; ++s) {
+                    float b;
+                    if (s < 4)
+                        b = __shfl_sync(kFull, cur.b0, s * 8 + j);
+                    else if (s < kWgPlanWords)
+                        b = __shfl_sync(kFull, cur.b1, (s - 4) * 8 + j);
+                    else
+                        b = cur.tile0 + j < a.tiles ? a.wbound[(cur.qb + s) * a.tiles + cur.tile0 + j] : 0.0f;
+                    bound = __fadd_rn(bound, b);
+                }
+                keep = __ballot_sync(kFull, !(bound < thr)) & 0xffu;
+                if (!((keep >> j) & 1u)) {
+                    cur.p0 = make_int2(0, 0);
+                    cur.p1 = make_int2(0, 0);
+                }
+                if (!keep) {
+                    ++n_dropped;
+                    continue;  // no tile of the claim can reach the bound
+                }
+            }
+            n_tiles += __popc(keep & (a.tiles - cur.tile0 >= kWgWarps ? 0xffu : (1u << (a.tiles - cur.tile0)) - 1u));
             // each word's run over the group, reduced within its 8 lanes
             const bool ne0 = cur.p0.x < cur.p0.y, ne1 = cur.p1.x < cur.p1.y;
             int lo0 = ne0 ? cur.p0.x : 0x7fffffff, hi0 = ne0 ? cur.p0.y : -1;
@@ -328,7 +376,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
             int last_word = -1;
             for (int s = cur.n - 1; s >= kWgPlanWords && last_word < 0; --s)
                 for (int j = 0; j < kWgWarps; ++j) {
-                    const int2 r = WgFarRange(a, cur, s, j);
+                    const int2 r = WgFarRange(a, cur, s, j, keep);
                     if (r.x < r.y) {
                         last_word = s;
                         break;
@@ -352,7 +400,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
                     lo = 0x7fffffff;
                     hi = -1;
                     for (int j = 0; j < kWgWarps; ++j) {
-                        const int2 r = WgFarRange(a, cur, s, j);
+                        const int2 r = WgFarRange(a, cur, s, j, keep);
                         if (r.x < r.y) {
                             lo = min(lo, r.x);
                             hi = max(hi, r.y);
@@ -375,7 +423,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
                         if ((lane >> 3) == (s & 3))
                             m.be[lane & 7] = s < 4 ? cur.p0 : cur.p1;
                     } else if (lane < kWgWarps) {
-                        m.be[lane] = WgFarRange(a, cur, s, lane);
+                        m.be[lane] = WgFarRange(a, cur, s, lane, keep);
                     }
                     if (lane == 0) {
                         m.span = make_int4((int)c0, (int)(c1 - c0), cur.q, cur.tile0);
@@ -385,6 +433,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
                     __syncwarp();  // the meta is complete before lane 0 starts the stage
                     if (lane == 0) {
                         const unsigned bytes = (unsigned)(c1 - c0) * 4u;
+                        n_copied += (unsigned long long)(c1 - c0);
                         MbarArriveExpectTx(&sh.full[st], 2u * bytes);
                         BulkLoad(ring_ids + (size_t)st * chunk, a.indices + c0, bytes, &sh.full[st]);
                         BulkLoad(ring_vals + (size_t)st * chunk, a.data + c0, bytes, &sh.full[st]);
@@ -411,6 +460,12 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
         if (lane == 0) {
             if (bad)
                 atomicOr(a.status, bad);
+            if (a.stats) {
+                atomicAdd(a.stats, n_claims);
+                atomicAdd(a.stats + 1, n_dropped);
+                atomicAdd(a.stats + 2, n_tiles);
+                atomicAdd(a.stats + 3, n_copied);
+            }
             // the last producer to run dry resets the work counter for the next Search
             const unsigned d = atomicAdd(&a.ctrl->done, 1u);
             if (d == gridDim.x - 1) {

@@ -70,7 +70,7 @@ def pack_queries(queries):
 
 
 def _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes, stream,
-             kernel=4, ring_stages=0, ring_chunk=0):
+             kernel=4, ring_stages=0, ring_chunk=0, prune=False):
     o = n.Options()
     n.engine_library().bm25_default_options(ctypes.byref(o))
     o.device_id = device_id
@@ -84,6 +84,7 @@ def _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_f
     o.kernel = kernel
     o.ring_stages = ring_stages
     o.ring_chunk = ring_chunk
+    o.prune = int(bool(prune))
     return o
 
 
@@ -99,7 +100,7 @@ class Bm25Session:
     @classmethod
     def from_csc(cls, indptr, indices, data, num_docs, *, query_capacity=8, word_capacity=24, max_k=10,
                  device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0, stream=None, kernel=4, ring_stages=0,
-                 ring_chunk=0):
+                 ring_chunk=0, prune=False):
         """Eager CSC index (bm25s layout): indptr int64 [V+1], indices int32 [M], data float32 [M]."""
         lib = n.engine_library()
         indptr = np.ascontiguousarray(indptr, dtype=np.int64)
@@ -109,7 +110,7 @@ class Bm25Session:
         if vocab < 1 or indices.size != indptr[-1] or data.size != indices.size:
             raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'Index dimensions/endpoints differ')
         o = _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes,
-                     stream, kernel, ring_stages, ring_chunk)
+                     stream, kernel, ring_stages, ring_chunk, prune)
         h = c_void_p()
         status = lib.bm25_create(n.ptr(indptr, c_int64), n.ptr(indices, c_int32), n.ptr(data, c_float), vocab,
                                  int(num_docs), ctypes.byref(o), ctypes.byref(h))
@@ -119,7 +120,7 @@ class Bm25Session:
     @classmethod
     def from_lazy(cls, term_offsets, posting_doc_ids, posting_tf, doc_norm, idf, *, k1=1.2, query_capacity=8,
                   word_capacity=24, max_k=10, device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0,
-                  stream=None, kernel=4, ring_stages=0, ring_chunk=0):
+                  stream=None, kernel=4, ring_stages=0, ring_chunk=0, prune=False):
         """The reference's resident index (common/bm25/index_data.h:9-42); posting scores built on the GPU."""
         lib = n.engine_library()
         offsets = np.ascontiguousarray(term_offsets, dtype=np.int64)
@@ -131,7 +132,7 @@ class Bm25Session:
         if offsets.size != vocab + 1 or docs.size != tf.size or offsets[-1] != docs.size:
             raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'Index dimensions/endpoints differ')
         o = _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes,
-                     stream, kernel, ring_stages, ring_chunk)
+                     stream, kernel, ring_stages, ring_chunk, prune)
         h = c_void_p()
         status = lib.bm25_create_lazy(n.ptr(offsets, c_int64), n.ptr(docs, c_int32), n.ptr(tf, c_float),
                                       n.ptr(norm, c_float), n.ptr(idf, c_float), vocab, norm.size, float(k1),
@@ -159,6 +160,86 @@ class Bm25Session:
                                        n.ptr(scores, c_float), n.ptr(ids, c_int32))
         _raise(self._lib, status, self._handle)
         return scores, ids
+
+    def search_pruned(self, queries, k, tau):
+        """Exact top-k with tile pruning from starting bounds tau [Q] (a guess of each query's k-th score).
+
+        Returns (scores, ids, exact): exact[i] is 1 where the pruned pass stood and 0 where the
+        guess was too high and the call's retry pass searched the query on the plain path."""
+        if isinstance(queries, tuple):
+            offsets = np.ascontiguousarray(queries[0], dtype=np.int64)
+            words = np.ascontiguousarray(queries[1], dtype=np.int32)
+        else:
+            offsets, words = pack_queries(queries)
+        q = offsets.size - 1
+        tau = np.ascontiguousarray(tau, dtype=np.float32)
+        if tau.shape != (q,):
+            raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'tau must hold one bound per query')
+        scores = np.empty((q, k), dtype=np.float32)
+        ids = np.empty((q, k), dtype=np.int32)
+        exact = np.empty(q, dtype=np.int32)
+        if words.size == 0:
+            words = np.zeros(1, dtype=np.int32)
+        status = self._lib.bm25_search_pruned(self._handle, n.ptr(offsets, c_int64), n.ptr(words, c_int32),
+                                              n.ptr(tau, c_float), q, k, n.ptr(scores, c_float),
+                                              n.ptr(ids, c_int32), n.ptr(exact, c_int32))
+        _raise(self._lib, status, self._handle)
+        return scores, ids, exact
+
+    def search_pruned_device(self, qoffsets_ptr, words_ptr, tau_ptr, q, k, scores_ptr, ids_ptr, exact_ptr,
+                             stream_ptr=None):
+        """Device-resident pruned Search; every row exact, exact[i] = 0 where the retry pass answered."""
+        status = self._lib.bm25_search_pruned_device(self._handle, c_void_p(qoffsets_ptr), c_void_p(words_ptr),
+                                                     c_void_p(tau_ptr), q, k, c_void_p(scores_ptr),
+                                                     c_void_p(ids_ptr), c_void_p(exact_ptr), c_void_p(stream_ptr))
+        _raise(self._lib, status, self._handle)
+
+    def set_threshold_model(self, model):
+        """Threshold model of the learned bounds (a ThresholdModel, or None for the safe bounds alone)."""
+        if model is None:
+            status = self._lib.bm25_set_threshold_model(self._handle, None, c_float(0.0))
+        else:
+            params = np.ascontiguousarray(model.params, dtype=np.float32)
+            status = self._lib.bm25_set_threshold_model(self._handle, n.ptr(params, c_float), c_float(model.margin))
+        _raise(self._lib, status, self._handle)
+
+    def search_learned(self, queries, k):
+        """Exact top-k with learned starting bounds; returns (scores, ids, exact) as search_pruned."""
+        if isinstance(queries, tuple):
+            offsets = np.ascontiguousarray(queries[0], dtype=np.int64)
+            words = np.ascontiguousarray(queries[1], dtype=np.int32)
+        else:
+            offsets, words = pack_queries(queries)
+        q = offsets.size - 1
+        scores = np.empty((q, k), dtype=np.float32)
+        ids = np.empty((q, k), dtype=np.int32)
+        exact = np.empty(q, dtype=np.int32)
+        if words.size == 0:
+            words = np.zeros(1, dtype=np.int32)
+        status = self._lib.bm25_search_learned(self._handle, n.ptr(offsets, c_int64), n.ptr(words, c_int32), q, k,
+                                               n.ptr(scores, c_float), n.ptr(ids, c_int32), n.ptr(exact, c_int32))
+        _raise(self._lib, status, self._handle)
+        return scores, ids, exact
+
+    def search_learned_device(self, qoffsets_ptr, words_ptr, q, k, scores_ptr, ids_ptr, exact_ptr, stream_ptr=None):
+        """Device-resident learned pruned Search (rows as search_pruned_device)."""
+        status = self._lib.bm25_search_learned_device(self._handle, c_void_p(qoffsets_ptr), c_void_p(words_ptr), q,
+                                                      k, c_void_p(scores_ptr), c_void_p(ids_ptr),
+                                                      c_void_p(exact_ptr), c_void_p(stream_ptr))
+        _raise(self._lib, status, self._handle)
+
+    def query_features_device(self, qoffsets_ptr, words_ptr, q, k, features_ptr, safe_ptr=None, stream_ptr=None):
+        """Features [q][32] and safe bounds [q] of a device query batch (asynchronous)."""
+        status = self._lib.bm25_query_features_device(self._handle, c_void_p(qoffsets_ptr), c_void_p(words_ptr), q,
+                                                      k, c_void_p(features_ptr), c_void_p(safe_ptr),
+                                                      c_void_p(stream_ptr))
+        _raise(self._lib, status, self._handle)
+
+    def search_stats(self, reset=True):
+        """Tile-group counters since the last reset: claims, claims dropped, tiles scanned, postings copied."""
+        out = (ctypes.c_uint64 * 4)()
+        _raise(self._lib, self._lib.bm25_search_stats(self._handle, out, int(bool(reset))), self._handle)
+        return {'claims': out[0], 'claims_dropped': out[1], 'tiles_scanned': out[2], 'postings_copied': out[3]}
 
     def search_device(self, qoffsets_ptr, words_ptr, q, k, scores_ptr, ids_ptr, stream_ptr=None):
         """Device-resident Search on raw device pointers (e.g. torch ``data_ptr()``); asynchronous."""

@@ -51,6 +51,8 @@ typedef struct bm25_options {
     int32_t ring_stages;     /* posting-ring depth of the ring kernels (0 and 4), 2..8; 0 = automatic */
     int32_t ring_chunk;      /* postings per ring stage of the tile-group kernel, 512..4096, a multiple of 4;
                                 0 = automatic */
+    int32_t prune;           /* nonzero: prepare per-(word, tile) score bounds for bm25_search_pruned_device
+                                (tile-group kernel only; costs one float per directory row and tile) */
 } bm25_options;
 
 /* Search kernels (bm25_options.kernel):
@@ -116,6 +118,57 @@ int bm25_search(bm25_handle *handle, const int64_t *qoffsets, const int32_t *wor
 int bm25_search_device(bm25_handle *handle, const int64_t *qoffsets, const int32_t *words, int64_t q, int32_t k,
                        float *out_scores, int32_t *out_ids, void *stream);
 
+/*
+ * Pruned device-resident Search (no counterpart in the reference; the learned
+ * part of the engine).  As bm25_search_device, plus tau float [q]: a starting
+ * lower bound guess for each query's K-th score (e.g. the threshold MLP's
+ * prediction).  Tiles whose FP32 upper bound (the query words' per-tile maxima
+ * added in query-word order) is below a query's running bound -- which starts
+ * at tau -- are skipped.  out_exact int32 [q]: 1 where K documents reached tau,
+ * which proves the pruned top-K exact; 0 where the guess was too high, and a
+ * retry pass in the same call searched the query again on the plain path.
+ * Every output row is the exact top-K.  Needs a session created with
+ * options.prune = 1 and the tile-group kernel.
+ */
+int bm25_search_pruned_device(bm25_handle *handle, const int64_t *qoffsets, const int32_t *words, const float *tau,
+                              int64_t q, int32_t k, float *out_scores, int32_t *out_ids, int32_t *out_exact,
+                              void *stream);
+
+/* Pruned Search on host buffers (as bm25_search, plus tau [q] and out_exact [q]; one graph replay). */
+int bm25_search_pruned(bm25_handle *handle, const int64_t *qoffsets, const int32_t *words, const float *tau,
+                       int64_t q, int32_t k, float *out_scores, int32_t *out_ids, int32_t *out_exact);
+
+/*
+ * Learned starting bounds.  A prune session keeps, per term, its 32 largest
+ * posting scores and its mean posting score (computed on the device at
+ * creation).  From them each query gets 32 features and a safe bound (the
+ * largest K-th posting score among its words, which K documents always reach);
+ * the threshold model (an MLP 32 -> 64 -> 64 -> 1 predicting the log of the
+ * K-th score; see bm25_mlp_*) turns the features into tau = max(exp(prediction
+ * - margin), safe bound).  Without a model (params = NULL) tau is the safe bound.
+ */
+int bm25_set_threshold_model(bm25_handle *handle, const float *params, float margin);
+
+/* features float [q][32] and safe float [q] (may be NULL) on device buffers; asynchronous on stream. */
+int bm25_query_features_device(bm25_handle *handle, const int64_t *qoffsets, const int32_t *words, int64_t q,
+                               int32_t k, float *features, float *safe, void *stream);
+
+/* bm25_search_pruned with the learned bounds (host buffers). */
+int bm25_search_learned(bm25_handle *handle, const int64_t *qoffsets, const int32_t *words, int64_t q, int32_t k,
+                        float *out_scores, int32_t *out_ids, int32_t *out_exact);
+
+/* bm25_search_pruned_device with the learned bounds. */
+int bm25_search_learned_device(bm25_handle *handle, const int64_t *qoffsets, const int32_t *words, int64_t q,
+                               int32_t k, float *out_scores, int32_t *out_ids, int32_t *out_exact, void *stream);
+
+/*
+ * Tile-group kernel counters summed over Searches since the last reset (waits for
+ * the handle's work): out[0] claims (query x 8-tile groups) taken, out[1] claims
+ * dropped whole by their bounds, out[2] tiles scanned, out[3] postings copied
+ * from HBM into the staging rings.
+ */
+int bm25_search_stats(bm25_handle *handle, uint64_t *out, int32_t reset);
+
 /* Waits for the handle's device-resident Searches and returns their accumulated device status word
  * (0 = clean), then clears it.  Device-resident Searches only OR into this word. */
 int bm25_device_status(bm25_handle *handle, uint32_t *status);
@@ -166,6 +219,28 @@ int bm25_search_csc_static(const int64_t *indptr, const int32_t *indices, const 
  */
 int bm25_kernel_timing(bm25_handle *h, int32_t enable);
 int bm25_kernel_times(bm25_handle *h, float *ms, int64_t capacity, int64_t *count);
+
+/*
+ * Threshold MLP of the learned-pruning path (no counterpart in the reference).
+ * A 32 -> 64 -> 64 -> 1 ReLU network in FP32 whose parameters are one flat array
+ * of bm25_mlp_param_count() floats: W1[64][32] | b1[64] | W2[64][64] | b2[64] |
+ * w3[64] | b3.  It predicts a query's log K-th score from 32 features; all
+ * pointers are device pointers, work is enqueued on `stream` (a cudaStream_t).
+ *   bm25_mlp_forward:  out[i] = f(features[i][0..31]) for i < batch.
+ *   bm25_mlp_gradient: grad = d/dparams of mean_i w_i * (f(x_i) - t_i)^2, w_i =
+ *     over_weight when f(x_i) > t_i else 1 (an over-estimate costs a plain re-run),
+ *     and *loss = that mean; deterministic (fixed summation order).  `scratch`
+ *     holds bm25_mlp_scratch_floats(batch) floats.  `loss` may be NULL.
+ *   bm25_mlp_adam: one Adam step (beta1 0.9, beta2 0.999, eps 1e-8), step >= 1.
+ * Error details: bm25_mlp_last_error.
+ */
+int64_t bm25_mlp_param_count(void);
+int64_t bm25_mlp_scratch_floats(int64_t batch);
+int bm25_mlp_forward(const float *params, const float *features, int64_t batch, float *out, void *stream);
+int bm25_mlp_gradient(const float *params, const float *features, const float *targets, int64_t batch,
+                      float over_weight, float *scratch, float *grad, float *loss, void *stream);
+int bm25_mlp_adam(float *params, float *m, float *v, const float *grad, float lr, int32_t step, void *stream);
+int bm25_mlp_last_error(char *buffer, size_t length);
 
 /* Engine facts for reports and tests. */
 typedef struct bm25_info {
