@@ -15,6 +15,13 @@ frequency, K = 10; two batches A/B alternate as in the reference's benchmark.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
+  learned_pruned   the same Searches with learned starting bounds: a threshold MLP
+          (32 -> 64 -> 64 -> 1) trained on the GPU by the engine's own kernels on
+          200k generated queries of the same shape (targets: the plain engine's
+          K-th scores), then timed as above (device-resident and through
+          bm25_search_learned), beside the safe bounds alone; every result checked
+          bit for bit against the oracle.
+
 --impl reference times the reference's own CPU search (oracle/_ref, compiled from
 the reference's sources; the oracle's C restatement where that was not built) on
 the same corpus and batches with every host thread.
@@ -201,6 +208,229 @@ def cpu_search_leg(index, sets, k, budget_s, max_steps, warmup=1):
             'p50_ms': percentile(times, 50) * 1e3, 'p95_ms': percentile(times, 95) * 1e3}
 
 
+def timed_device(session, step, steps, warmup, flush, stream, world, with_clocks=None):
+    """Device-resident steps timed with CUDA events on the launching stream, L2 flushed between
+    steps; returns (step ms, main-kernel ms, clocks)."""
+    import torch
+    import torch.distributed as dist
+    with torch.cuda.stream(stream):
+        for i in range(warmup):
+            step(i)
+        stream.synchronize()
+        status = session.device_status()
+        if status != 0:
+            raise RuntimeError(f'device status {status:#x} set during warm-up')
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        session.kernel_timing(True)
+        session.search_stats(reset=True)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        if with_clocks:
+            with_clocks.start()
+        for i in range(steps):
+            flush.zero_()
+            starts[i].record(stream)
+            step(i)
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+        clock_info = with_clocks.stop() if with_clocks else None
+    status = session.device_status()
+    if status != 0:
+        raise RuntimeError(f'device status {status:#x} set during the timed region')
+    step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    kernel_ms = [float(x) for x in session.kernel_times()]
+    session.kernel_timing(False)
+    if len(kernel_ms) != steps:
+        raise RuntimeError(f'{len(kernel_ms)} kernel timings for {steps} steps')
+    return step_ms, kernel_ms, clock_info
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device='cuda', dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def learned_leg(pkg, args, spec, index, session, sets, want, flush, stream, dev_sets, local, world):
+    """Learned-pruned Search on the same session, batches and timing rules as the plain line.
+
+    A threshold MLP is trained on the GPU (the engine's own kernels) from queries of the same
+    shape whose targets the plain engine computes, then the learned Search is timed device-resident
+    and end to end; the safe bounds alone (the method without the network) are timed beside it."""
+    import torch
+    t = time.perf_counter()
+    cap = 2048
+    trainer = pkg.Bm25Session.from_lazy(index.offsets, index.docs, index.tf, index.norm, index.idf, k1=spec.k1,
+                                        query_capacity=cap, word_capacity=cap * TERMS, max_k=K, device_id=local,
+                                        prune=True)
+    model = pkg.learned.fit(trainer, index.offsets, queries=args.train_queries, ks=(K,), lo=TERMS, hi=TERMS,
+                            seed=args.train_seed, steps=args.train_steps, batch=4096, gen_batch=cap,
+                            target_fallback=args.target_fallback, device=f'cuda:{local}')
+    trainer.close()
+    train_s = time.perf_counter() - t
+    log(f'threshold model trained in {train_s:.1f}s: {model.report}')
+    d_scores = torch.empty((Q, K), dtype=torch.float32, device='cuda')
+    d_ids = torch.empty((Q, K), dtype=torch.int32, device='cuda')
+    d_exact = torch.empty(Q, dtype=torch.int32, device='cuda')
+
+    def step(i):
+        o, w = dev_sets[i % 2]
+        session.search_learned_device(o.data_ptr(), w.data_ptr(), Q, K, d_scores.data_ptr(), d_ids.data_ptr(),
+                                      d_exact.data_ptr(), stream.cuda_stream)
+
+    out = {}
+    for label, m in (('safe_bounds_only', None), ('learned', model)):
+        session.set_threshold_model(m)
+        parity = True
+        if want is not None:
+            for qs, (rs, ri) in zip(sets, want):
+                gs, gi, _ = session.search_learned(qs, K)
+                parity &= bool(np.array_equal(gi, ri) and np.array_equal(gs.view(np.uint32), rs.view(np.uint32)))
+        step_ms, kernel_ms, _ = timed_device(session, step, args.steps, args.warmup, flush, stream, world)
+        stats = session.search_stats(reset=True)
+        total = max_over_ranks(sum(step_ms), world)
+        host_ms, fallbacks = [], 0
+        for i in range(args.warmup):
+            session.search_learned(sets[i % 2], K)
+        for i in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            _, _, exact = session.search_learned(sets[i % 2], K)
+            host_ms.append((time.perf_counter() - t0) * 1e3)
+            fallbacks += int(np.sum(exact == 0))
+        e2e_total = max_over_ranks(sum(host_ms), world)
+        out[label] = {
+            'value': world * Q * args.steps / (total / 1e3), 'unit': UNIT,
+            'p50_ms': percentile(step_ms, 50), 'p95_ms': percentile(step_ms, 95),
+            'pruned_kernel_ms_avg': sum(kernel_ms) / len(kernel_ms),
+            'e2e': {'value': world * Q * args.steps / (e2e_total / 1e3), 'unit': UNIT,
+                    'p50_ms': percentile(host_ms, 50), 'p95_ms': percentile(host_ms, 95),
+                    'path': 'bm25_search_learned (C ABI, host buffers): one graph replay'},
+            'fallback_share': fallbacks / (Q * args.steps),
+            'gpu_launches': args.steps * 7,  # bound, plan, seed, pruned pass, select, retry pass, retry select
+            'per_search': {key: v / args.steps for key, v in stats.items()},
+            'bit_exact_vs_oracle': parity if want is not None else None,
+        }
+    out['learned']['model'] = {'train_queries': model.report['train_queries'], 'train_s': train_s,
+                               'margin': model.margin, 'val_fallback': model.report['val_fallback'],
+                               'first_loss': model.report['first_loss'], 'last_loss': model.report['last_loss'],
+                               'trained_with': 'bm25_mlp_gradient + bm25_mlp_adam (engine kernels)'}
+    return out
+
+
+MIX_WORKLOAD = 'passages_8p8m'
+MIX_Q, MIX_TERMS, MIX_KS = 256, (2, 12), (10, 100, 1000)
+
+
+def mix_leg(pkg, args, local, world, flush, stream, rank):
+    """The batched mix: 8.8M passages (V 2.5M, Zipf 1.05, mean 56), 256 queries per Search with
+    2-12 terms drawn by df and K drawn from {10, 100, 1000} per query, all in one Search
+    (bm25_search_batch: one graph replay).  Plain and learned-pruned, device-resident and e2e."""
+    import torch
+    spec = pkg.CONFIG_SHAPES[MIX_WORKLOAD]
+    t = time.perf_counter()
+    index = pkg.synthetic_index(spec)
+    log(f'mix corpus: N={index.num_docs} V={index.vocab} M={index.postings} in {time.perf_counter() - t:.1f}s')
+    lo, hi = MIX_TERMS
+    batches = []
+    for b in range(2):
+        qo, w = pkg.synthetic_queries(index.offsets, MIX_Q, lo, hi, 880000 + 1000 * rank + b)
+        ks = np.random.default_rng(770 + 1000 * rank + b).choice(MIX_KS, MIX_Q).astype(np.int32)
+        batches.append((qo, w, ks))
+    kmax = max(MIX_KS)
+    session = pkg.Bm25Session.from_lazy(index.offsets, index.docs, index.tf, index.norm, index.idf, k1=spec.k1,
+                                        query_capacity=MIX_Q, word_capacity=MIX_Q * hi, max_k=kmax,
+                                        device_id=local, prune=True)
+    parity = None
+    if rank == 0:
+        from oracle import oracle
+        data = oracle.contributions(index, spec.k1)
+        ok = True
+        qo, w, ks = batches[0]
+        gs, gi, koff = session.search_batch((qo, w), ks)
+        for k in MIX_KS:
+            sel = np.nonzero(ks == k)[0]
+            rows = [w[qo[i]:qo[i + 1]] for i in sel]
+            o = np.zeros(len(rows) + 1, np.int64)
+            o[1:] = np.cumsum([len(r) for r in rows])
+            rs, ri = oracle.search(index.offsets, index.docs, data, index.num_docs, o,
+                                   np.concatenate(rows).astype(np.int32), int(k), threads=os.cpu_count() or 1)
+            for j, i in enumerate(sel):
+                ok &= bool(np.array_equal(gi[koff[i]:koff[i + 1]], ri[j]) and
+                           np.array_equal(gs[koff[i]:koff[i + 1]].view(np.uint32), rs[j].view(np.uint32)))
+        del data
+        parity = {'batch': 0, 'bit_exact': ok, 'against': 'oracle (C restatement), per K group'}
+        log(f'mix parity vs oracle: {parity}')
+    t = time.perf_counter()
+    cap = 1024
+    trainer = pkg.Bm25Session.from_lazy(index.offsets, index.docs, index.tf, index.norm, index.idf, k1=spec.k1,
+                                        query_capacity=cap, word_capacity=cap * hi, max_k=kmax, device_id=local,
+                                        prune=True)
+    model = pkg.learned.fit(trainer, index.offsets, queries=args.mix_train_queries, ks=MIX_KS, lo=lo, hi=hi,
+                            seed=args.train_seed, steps=args.train_steps, batch=4096, gen_batch=cap,
+                            target_fallback=args.target_fallback, device=f'cuda:{local}')
+    trainer.close()
+    train_s = time.perf_counter() - t
+    log(f'mix threshold model trained in {train_s:.1f}s: {model.report}')
+    dev = []
+    for qo, w, ks in batches:
+        koff = np.zeros(MIX_Q + 1, np.int64)
+        np.cumsum(ks, out=koff[1:])
+        dev.append(tuple(torch.from_numpy(x).cuda() for x in (qo, w, ks, koff[:-1].copy())))
+    d_s = torch.empty(MIX_Q * kmax, dtype=torch.float32, device='cuda')
+    d_i = torch.empty(MIX_Q * kmax, dtype=torch.int32, device='cuda')
+    d_x = torch.empty(MIX_Q, dtype=torch.int32, device='cuda')
+    out = {'workload': MIX_WORKLOAD, 'docs': spec.docs, 'vocab': spec.vocab, 'zipf_s': spec.zipf_s,
+           'len_mean': spec.len_mean, 'postings': index.postings, 'queries_per_search': MIX_Q,
+           'terms': f'U{{{lo}..{hi}}} drawn by df', 'k': 'per query from {10, 100, 1000}', 'parity': parity,
+           'model': {'train_queries': model.report['train_queries'], 'train_s': train_s, 'margin': model.margin,
+                     'val_fallback': model.report['val_fallback']}}
+    steps = max(3, args.steps // 4)
+    for label, learned in (('plain', False), ('learned', True)):
+        session.set_threshold_model(model if learned else None)
+
+        def step(i):
+            o, w, k, ko = dev[i % 2]
+            session.search_batch_device(o.data_ptr(), w.data_ptr(), k.data_ptr(), ko.data_ptr(), MIX_Q, kmax,
+                                        d_s.data_ptr(), d_i.data_ptr(), d_x.data_ptr(), learned,
+                                        stream.cuda_stream)
+
+        step_ms, kernel_ms, _ = timed_device(session, step, steps, args.warmup, flush, stream, world)
+        stats = session.search_stats(reset=True)
+        total = max_over_ranks(sum(step_ms), world)
+        host_ms, fallbacks = [], 0
+        for i in range(args.warmup):
+            session.search_batch(batches[i % 2][:2], batches[i % 2][2], learned=learned)
+        for i in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = session.search_batch(batches[i % 2][:2], batches[i % 2][2], learned=learned)
+            host_ms.append((time.perf_counter() - t0) * 1e3)
+            if learned:
+                fallbacks += int(np.sum(r[3] == 0))
+        e2e_total = max_over_ranks(sum(host_ms), world)
+        out[label] = {'value': world * MIX_Q * steps / (total / 1e3), 'unit': UNIT,
+                      'p50_ms': percentile(step_ms, 50), 'p95_ms': percentile(step_ms, 95),
+                      'main_kernel_ms_avg': sum(kernel_ms) / len(kernel_ms),
+                      'e2e': {'value': world * MIX_Q * steps / (e2e_total / 1e3), 'unit': UNIT,
+                              'p50_ms': percentile(host_ms, 50), 'p95_ms': percentile(host_ms, 95)},
+                      'per_search': {key: v / steps for key, v in stats.items()}, 'steps': steps}
+        if learned:
+            out[label]['fallback_share'] = fallbacks / (MIX_Q * steps)
+    out['speedup_learned_vs_plain'] = out['learned']['value'] / out['plain']['value']
+    out['e2e_speedup_learned_vs_plain'] = out['learned']['e2e']['value'] / out['plain']['e2e']['value']
+    session.close()
+    return out
+
+
 def run_reference(args):
     rank, world, _ = setup_dist(args.gpus)
     if rank != 0:
@@ -237,6 +467,13 @@ def main():
     ap.add_argument('--chunk', type=int, default=0, help='postings per ring stage of the tile-group kernel')
     ap.add_argument('--docs', type=int, default=0, help='reduced corpus for profiling captures (not a bench line)')
     ap.add_argument('--vocab', type=int, default=0, help='reduced vocabulary for profiling captures')
+    ap.add_argument('--no-learned', action='store_true', help='skip the learned-pruned leg')
+    ap.add_argument('--train-queries', type=int, default=200_000)
+    ap.add_argument('--train-steps', type=int, default=3000)
+    ap.add_argument('--train-seed', type=int, default=7)
+    ap.add_argument('--target-fallback', type=float, default=0.02)
+    ap.add_argument('--no-mix', action='store_true', help='skip the batched 256-query mix')
+    ap.add_argument('--mix-train-queries', type=int, default=120_000)
     args = ap.parse_args()
     if args.impl == 'reference':
         return run_reference(args)
@@ -259,18 +496,22 @@ def main():
     session = pkg.Bm25Session.from_lazy(index.offsets, index.docs, index.tf, index.norm, index.idf, k1=spec.k1,
                                         query_capacity=Q, word_capacity=Q * TERMS, max_k=K, device_id=local,
                                         tile_docs=args.tile_docs, merge_fan_in=args.fan_in, kernel=args.kernel,
-                                        ring_stages=args.stages, ring_chunk=args.chunk)
+                                        ring_stages=args.stages, ring_chunk=args.chunk,
+                                        prune=args.kernel == 4 and not args.no_learned)
     info = session.info()
     log(f'engine ready in {time.perf_counter() - t:.1f}s: {info}')
 
     # Parity of both batches against the CPU oracle (outside every timer).
     parity = None
+    want = None
     if rank == 0:
         from oracle import oracle
         data = oracle.contributions(index, spec.k1)
         ok = True
+        want = []
         for qs in sets:
             rs, ri = oracle.search(index.offsets, index.docs, data, index.num_docs, *qs, K)
+            want.append((rs, ri))
             gs, gi = session.search(qs, K)
             ok &= bool(np.array_equal(gi, ri) and np.array_equal(gs.view(np.uint32), rs.view(np.uint32)))
         parity = {'batches': len(sets), 'bit_exact': ok, 'against': 'oracle (C restatement, eager FP32)'}
@@ -290,41 +531,10 @@ def main():
         session.search_device(o.data_ptr(), w.data_ptr(), Q, K, d_scores.data_ptr(), d_ids.data_ptr(),
                               stream.cuda_stream)
 
-    with torch.cuda.stream(stream):
-        for i in range(args.warmup):
-            device_step(i)
-        stream.synchronize()
-        status = session.device_status()
-        if status != 0:
-            raise RuntimeError(f'device status {status:#x} set during warm-up')
-        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        clocks = Clocks(local)
-        session.kernel_timing(True)
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-        clocks.start()
-        for i in range(args.steps):
-            flush.zero_()
-            starts[i].record(stream)
-            device_step(i)
-            ends[i].record(stream)
-        torch.cuda.synchronize()
-        clock_info = clocks.stop()
-    status = session.device_status()
-    if status != 0:
-        raise RuntimeError(f'device status {status:#x} set during the timed region')
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    kernel_ms = [float(x) for x in session.kernel_times()]
-    session.kernel_timing(False)
-    if len(kernel_ms) != args.steps:
-        raise RuntimeError(f'{len(kernel_ms)} kernel timings for {args.steps} steps')
-    total_ms = sum(step_ms)
-    if world > 1:
-        tt = torch.tensor([total_ms], device='cuda', dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    step_ms, kernel_ms, clock_info = timed_device(session, device_step, args.steps, args.warmup, flush, stream,
+                                                  world, Clocks(local))
+    plain_stats = session.search_stats(reset=True)
+    total_ms = max_over_ranks(sum(step_ms), world)
     value = world * Q * args.steps / (total_ms / 1e3)
 
     # End to end through the C ABI with host buffers (pinned arenas, H2D/D2H inside the call).
@@ -364,6 +574,18 @@ def main():
     if args.docs or args.vocab:
         traffic = None  # the profiles cover the full-size workload
 
+    learned = None
+    if info['kernel'] == 4 and not args.no_learned:
+        learned = learned_leg(pkg, args, spec, index, session, sets, want, flush, stream, dev_sets, local, world)
+        learned['speedup_vs_plain'] = learned['learned']['value'] / value
+        learned['e2e_speedup_vs_plain'] = learned['learned']['e2e']['value'] / e2e_value
+        learned['plain_per_search'] = {key: v / args.steps for key, v in plain_stats.items()}
+
+    mix = None
+    if info['kernel'] == 4 and not args.no_mix and not (args.docs or args.vocab):
+        session.close()  # frees the 10M index before the mix corpus is resident
+        mix = mix_leg(pkg, args, local, world, flush, stream, rank)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         res = cpu_search_leg(index, sets, K, budget_s=20.0, max_steps=40)
@@ -399,10 +621,15 @@ def main():
             'clocks': clock_info,
             'parity': parity,
         }
+        if learned is not None:
+            line['learned_pruned'] = learned
+        if mix is not None:
+            line['batched_mix'] = mix
         if cpu is not None:
             line['cpu_baseline'] = cpu
         print(json.dumps(line), flush=True)
-    session.close()
+    if mix is None:
+        session.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -32,6 +32,7 @@ class Options(ctypes.Structure):
         ('ring_stages', c_int32),
         ('ring_chunk', c_int32),
         ('prune', c_int32),
+        ('candidate_capacity', c_int64),
     ]
 
 
@@ -79,6 +80,11 @@ SIGNATURES = {
                                           c_void_p, c_void_p, c_void_p]),
     'bm25_search_pruned': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p,
                                    c_void_p]),
+    'bm25_search_batch': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
+    'bm25_search_batch_learned': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p,
+                                          c_void_p]),
+    'bm25_search_batch_device': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_int32,
+                                         c_void_p, c_void_p, c_void_p, c_void_p]),
     'bm25_set_threshold_model': (c_int, [c_void_p, c_void_p, c_float]),
     'bm25_query_features_device': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p,
                                            c_void_p]),

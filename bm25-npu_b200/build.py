@@ -20,7 +20,8 @@ NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
 ENGINE_SOURCES = ['engine.cu', 'mlp.cu']
-ENGINE_HEADERS = ['tile_kernels.cuh', 'stream_kernel.cuh', 'tile_group_kernel.cuh', 'learned_kernels.cuh', 'mlp.cuh']
+ENGINE_HEADERS = ['tile_kernels.cuh', 'stream_kernel.cuh', 'tile_group_kernel.cuh', 'block_kernels.cuh',
+                  'learned_kernels.cuh', 'mlp.cuh']
 
 
 def _stale(target, sources):

@@ -9,6 +9,7 @@
 // and one CUDA graph per (Q, K) holding H2D -> fused scoring/selection/merge ->
 // D2H.  Search = validate + pack, graph replay, synchronise, validate result.
 #include "bm25_b200.h"
+#include "block_kernels.cuh"
 #include "learned_kernels.cuh"
 #include "stream_kernel.cuh"
 #include "tile_group_kernel.cuh"
@@ -155,7 +156,9 @@ class Engine {
     Engine(const bm25_options &o, int64_t vocab, int64_t docs, int64_t postings)
         : opts_(o), vocab_(vocab), docs_(docs), postings_(postings)
     {
-        Check(o.max_k >= 1 && o.max_k <= bm25k::kMaxSmallK, "max_k must be in [1, 32]");
+        Check(o.max_k >= 1 && o.max_k <= bm25k::kLargeMaxK, "max_k must be in [1, 1024]");
+        Check(o.max_k <= bm25k::kMaxSmallK || o.kernel == BM25_KERNEL_TILE_GROUP,
+              "max_k above 32 needs the tile-group kernel");
         Check(o.max_k <= docs, "max_k exceeds the document count");
         Check(o.query_capacity >= 1 && o.query_capacity <= 65535, "query_capacity must be in [1, 65535]");
         Check(o.word_capacity >= 0 && o.word_capacity <= 16777216, "word_capacity must be in [0, 2^24]");
@@ -340,6 +343,106 @@ class Engine {
             out_exact[i] = exact[i] ? 1 : 0;
     }
 
+    // A batch with a K per query (host buffers): results packed by query, query i's ks[i] rows from
+    // the sum of the K before it.  learned: starting bounds from the learned-bound kernel, out_exact
+    // as in SearchPruned.
+    void SearchBatch(const int64_t *qoffsets, const int32_t *words, const int32_t *ks, int64_t q, bool learned,
+                     float *out_scores, int32_t *out_ids, int32_t *out_exact)
+    {
+        RequireUsable();
+        if (learned)
+            RequirePrune();
+        Check(plan_.kernel == BM25_KERNEL_TILE_GROUP, "A K per query needs the tile-group kernel");
+        Check(ks && out_scores && out_ids && (!learned || out_exact), "Null buffer");
+        Check(q >= 1 && q <= opts_.query_capacity, "Query batch exceeds declared capacity or is empty");
+        int kmax = 1;
+        std::vector<int64_t> kout(q);
+        int64_t total = 0;
+        for (int64_t i = 0; i < q; ++i) {
+            Check(ks[i] >= 1 && ks[i] <= opts_.max_k && ks[i] <= docs_, "K outside [1, min(max_k, N)]");
+            kout[i] = total;
+            total += ks[i];
+            kmax = std::max(kmax, ks[i]);
+        }
+        Pack(qoffsets, words, q, kmax);
+        unsigned char *in = static_cast<unsigned char *>(h_in_);
+        std::memcpy(in + ks_offset_, ks, q * sizeof(int32_t));
+        std::memcpy(in + kout_offset_, kout.data(), q * sizeof(int64_t));
+        try {
+            Cuda(cudaSetDevice(device_), "cudaSetDevice");
+            cudaGraphExec_t exec = GraphFor((int)q, kmax, (learned ? kModeLearned : kModePlain) | kModeMixed);
+            Cuda(cudaStreamWaitEvent(stream_, done_, 0), "cudaStreamWaitEvent");
+            ++searches_;
+            Cuda(cudaGraphLaunch(exec, stream_), "cudaGraphLaunch");
+            ++replays_;
+            unsigned char *ho = static_cast<unsigned char *>(h_out_);
+            Cuda(cudaMemcpyAsync(ho, d_out_, total * sizeof(float), cudaMemcpyDeviceToHost, stream_), "D2H");
+            const size_t ids = IdOffset((int)q, kmax);
+            Cuda(cudaMemcpyAsync(ho + ids, d_out_ + ids, total * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_),
+                 "D2H");
+            const size_t st = StatusOffset((int)q, kmax);
+            Cuda(cudaMemcpyAsync(ho + st, d_out_ + st, 32 + (learned ? (size_t)q * 4 : 0), cudaMemcpyDeviceToHost,
+                                 stream_),
+                 "D2H");
+            Cuda(cudaEventRecord(done_, stream_), "cudaEventRecord");
+            Cuda(cudaStreamSynchronize(stream_), "complete batch Search through result D2H");
+            unsigned status = 0;
+            std::memcpy(&status, ho + st, sizeof(unsigned));
+            if (status)
+                throw DeviceError(0, "Device reported invalid Search state, status=" + std::to_string(status));
+            const float *scores = reinterpret_cast<const float *>(ho);
+            const int32_t *idv = reinterpret_cast<const int32_t *>(ho + ids);
+            for (int64_t i = 0; i < q; ++i)
+                for (int64_t r = kout[i]; r < kout[i] + ks[i]; ++r) {
+                    if (!(idv[r] >= 0 && idv[r] < docs_ && std::isfinite(scores[r]) && scores[r] >= 0))
+                        throw DeviceError(0, "Invalid real-document result");
+                    if (r > kout[i] && !(scores[r - 1] > scores[r] || (scores[r - 1] == scores[r] && idv[r - 1] < idv[r])))
+                        throw DeviceError(0, "Strict global ranking failure");
+                }
+            std::memcpy(out_scores, scores, total * sizeof(float));
+            std::memcpy(out_ids, idv, total * sizeof(int32_t));
+            if (learned) {
+                const int32_t *ex = reinterpret_cast<const int32_t *>(ho + ExactOffset((int)q, kmax));
+                for (int64_t i = 0; i < q; ++i)
+                    out_exact[i] = ex[i] ? 1 : 0;
+            }
+        } catch (...) {
+            failed_ = true;
+            throw;
+        }
+    }
+
+    // Device-resident batch with a K per query: ks [q], kout [q] (first output slot of each query,
+    // rows packed), kmax >= every ks[i]; learned: learned bounds and out_exact [q].
+    void SearchBatchDevice(const int64_t *qoffsets, const int32_t *words, const int32_t *ks, const int64_t *kout,
+                           int64_t q, int32_t kmax, bool learned, float *out_scores, int32_t *out_ids,
+                           int32_t *out_exact, cudaStream_t stream)
+    {
+        RequireUsable();
+        if (learned)
+            RequirePrune();
+        Check(plan_.kernel == BM25_KERNEL_TILE_GROUP, "A K per query needs the tile-group kernel");
+        Check(q >= 1 && q <= opts_.query_capacity, "Query batch exceeds declared capacity or is empty");
+        Check(kmax >= 1 && kmax <= opts_.max_k && kmax <= docs_, "K outside [1, min(max_k, N)]");
+        Check(qoffsets && words && ks && kout && out_scores && out_ids && (!learned || out_exact), "Null device buffer");
+        try {
+            Cuda(cudaSetDevice(device_), "cudaSetDevice");
+            cudaStream_t s = stream ? stream : stream_;
+            Cuda(cudaStreamWaitEvent(s, done_, 0), "cudaStreamWaitEvent");
+            ++searches_;
+            marking_ = !timing_.empty();
+            Launch((int)q, kmax, qoffsets, words, out_scores, out_ids, d_dev_status_, s, learned ? d_tau_ : nullptr,
+                   learned ? out_exact : nullptr, learned, ks, kout);
+            if (marking_)
+                ++timed_;
+            marking_ = false;
+            Cuda(cudaEventRecord(done_, s), "cudaEventRecord");
+        } catch (...) {
+            failed_ = true;
+            throw;
+        }
+    }
+
     // Threshold model of the learned bounds (host params, bm25mlp::kParams floats), or none.
     void SetThresholdModel(const float *params, float margin)
     {
@@ -359,7 +462,7 @@ class Engine {
         margin_ = params ? margin : 0.0f;
         // graphs hold the model pointer and margin by value: rebuild the learned ones
         for (auto it = graphs_.begin(); it != graphs_.end();) {
-            if (std::get<2>(it->first) == kModeLearned) {
+            if (std::get<2>(it->first) & kModeLearned) {
                 cudaGraphExecDestroy(it->second);
                 it = graphs_.erase(it);
             } else {
@@ -383,12 +486,12 @@ class Engine {
         bm25k::LearnedArgs la = LearnedArgsFor((int)q, k, qoffsets, words);
         la.features = features;
         la.safe = safe;
-        bm25k::QueryFeaturesKernel<<<(int)((q + 127) / 128), 128, 0, s>>>(la);
+        bm25k::QueryFeaturesKernel<<<(int)((q + 7) / 8), 256, 0, s>>>(la);
         Cuda(cudaGetLastError(), "feature kernel launch");
         Cuda(cudaEventRecord(done_, s), "cudaEventRecord");
     }
 
-    // Tile-group counters since the last reset: claims, claims dropped, tiles scanned, postings copied.
+    // Search counters since the last reset (bm25_search_stats).
     void SearchStats(uint64_t *out, bool reset)
     {
         RequireUsable();
@@ -397,12 +500,12 @@ class Engine {
         Cuda(cudaStreamWaitEvent(stream_, done_, 0), "cudaStreamWaitEvent");
         Cuda(cudaStreamSynchronize(stream_), "stats");
         if (!d_stats_) {
-            std::memset(out, 0, 4 * sizeof(uint64_t));
+            std::memset(out, 0, bm25k::kStats * sizeof(uint64_t));
             return;
         }
-        Cuda(cudaMemcpy(out, d_stats_, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost), "stats D2H");
+        Cuda(cudaMemcpy(out, d_stats_, bm25k::kStats * sizeof(uint64_t), cudaMemcpyDeviceToHost), "stats D2H");
         if (reset)
-            Cuda(cudaMemset(d_stats_, 0, 4 * sizeof(uint64_t)), "stats reset");
+            Cuda(cudaMemset(d_stats_, 0, bm25k::kStats * sizeof(uint64_t)), "stats reset");
     }
 
     bm25k::LearnedArgs LearnedArgsFor(int q, int k, const int64_t *qoffsets, const int32_t *words) const
@@ -642,25 +745,29 @@ class Engine {
                                                                    rows, plan_.tile_docs, tiles, d_dir_, tiles + 1);
             Cuda(cudaGetLastError(), "directory kernel launch");
             if (opts_.prune) {
-                d_dir_max_ = static_cast<float *>(Alloc(rows * (size_t)tiles * sizeof(float), "cudaMalloc dir max"));
-                const long long cells = rows * (long long)tiles;
-                bm25k::BuildDirMaxKernel<<<(int)std::min<long long>((cells + 255) / 256, 148 * 64), 256, 0, stream_>>>(
-                    (const long long *)d_indptr_, d_data_, d_terms, d_dir_, rows, tiles, tiles + 1, d_dir_max_);
-                Cuda(cudaGetLastError(), "directory bound kernel launch");
+                // 128-document block index of the directory rows: offsets (uint16) and maxima
+                const size_t cells = (size_t)rows * tiles * (plan_.tile_docs / bm25k::kBlockDocs);
+                d_boff_ = static_cast<unsigned short *>(Alloc(cells * sizeof(unsigned short), "cudaMalloc block offsets"));
+                d_bmax_ = static_cast<float *>(Alloc(cells * sizeof(float), "cudaMalloc block maxima"));
+                const long long pairs = rows * (long long)tiles;
+                bm25k::BuildBlockIndexKernel<<<(int)std::min<long long>((pairs + 255) / 256, 148 * 64), 256, 0,
+                                               stream_>>>((const long long *)d_indptr_, d_indices_, d_data_, d_terms,
+                                                          d_dir_, rows, tiles, tiles + 1, plan_.tile_docs, d_boff_,
+                                                          d_bmax_);
+                Cuda(cudaGetLastError(), "block index kernel launch");
             }
             Cuda(cudaStreamSynchronize(stream_), "directory kernel");
         }
         if (opts_.prune) {
-            wbound_ = static_cast<float *>(Alloc(std::max<size_t>(1, opts_.word_capacity) * (size_t)tiles *
-                                                     sizeof(float),
-                                                 "cudaMalloc word bounds"));
+            item_cap_ = (long long)opts_.query_capacity * tiles;
+            d_items_ = static_cast<uint4 *>(Alloc(item_cap_ * sizeof(uint4), "cudaMalloc block work list"));
+            d_wrow_ = static_cast<int *>(Alloc(std::max<size_t>(1, opts_.word_capacity) * sizeof(int),
+                                               "cudaMalloc word rows"));
+            d_item_count_ = static_cast<unsigned *>(Alloc(2 * sizeof(unsigned), "cudaMalloc block work count"));
             d_term_top_ = static_cast<float *>(Alloc(vocab_ * bm25k::kTermTop * sizeof(float), "cudaMalloc term top"));
             d_term_mean_ = static_cast<float *>(Alloc(vocab_ * sizeof(float), "cudaMalloc term mean"));
             d_model_ = static_cast<float *>(Alloc(bm25mlp::kParams * sizeof(float), "cudaMalloc model"));
             d_tau_ = static_cast<float *>(Alloc(opts_.query_capacity * sizeof(float), "cudaMalloc tau"));
-            d_fail_list_ = static_cast<int *>(Alloc(opts_.query_capacity * sizeof(int), "cudaMalloc fail list"));
-            d_fail_count_ = static_cast<unsigned *>(Alloc(sizeof(unsigned), "cudaMalloc fail count"));
-            Cuda(cudaMemset(d_fail_count_, 0, sizeof(unsigned)), "cudaMemset");
             const int grid = (int)std::min<long long>((vocab_ + 7) / 8, 148 * 16);
             bm25k::TermStatsKernel<<<grid, 256, 0, stream_>>>((const long long *)d_indptr_, d_data_, vocab_,
                                                                d_term_top_, d_term_mean_);
@@ -670,7 +777,9 @@ class Engine {
         // Query packet / result arenas (fixed_query_packet.h:15-25 layout).
         word_offset_ = Align32((opts_.query_capacity + 1) * sizeof(int64_t));
         tau_offset_ = Align32(word_offset_ + std::max<int64_t>(1, opts_.word_capacity) * sizeof(int32_t));
-        in_bytes_ = tau_offset_ + (opts_.prune ? Align32(opts_.query_capacity * sizeof(float)) : 0);
+        ks_offset_ = tau_offset_ + (opts_.prune ? Align32(opts_.query_capacity * sizeof(float)) : 0);
+        kout_offset_ = ks_offset_ + Align32(opts_.query_capacity * sizeof(int32_t));
+        in_bytes_ = kout_offset_ + Align32(opts_.query_capacity * sizeof(int64_t));
         const size_t qk = (size_t)opts_.query_capacity * opts_.max_k;
         out_bytes_ = Align32(qk * 4) * 2 + 32 + Align32(opts_.query_capacity * sizeof(int32_t));
         Cuda(cudaHostAlloc(&h_in_, in_bytes_, cudaHostAllocDefault), "cudaHostAlloc");
@@ -724,8 +833,33 @@ class Engine {
             plan_.grid = per_sm * sms;
             sms_ = sms;
             const size_t qc = (size_t)opts_.query_capacity, tiles_z = (size_t)plan_.tiles;
-            // worst case: every selection of every tile appends max_k candidates
+            // worst case for K <= 32: every selection of every tile appends max_k candidates.  For
+            // K > 32 a tile appends every document at or above the running bound; the buffer holds
+            // 256 K (at least 2^18) and a query that overflows it is searched again from its final
+            // bound by the retry pass.
             cand_cap_ = (long long)tiles_z * per_tile;
+            if (opts_.max_k > bm25k::kMaxSmallK) {
+                Check(opts_.candidate_capacity == 0 || opts_.candidate_capacity >= opts_.max_k,
+                      "candidate_capacity must be 0 or at least max_k");
+                cand_cap_ = std::min<long long>(cand_cap_, opts_.candidate_capacity
+                                                               ? opts_.candidate_capacity
+                                                               : std::max<long long>(1 << 18, 256LL * opts_.max_k));
+            }
+            if (opts_.prune || opts_.max_k > bm25k::kMaxSmallK) {
+                d_fail_list_ = static_cast<int *>(Alloc(2 * qc * sizeof(int), "cudaMalloc fail lists"));
+                d_fail_count_ = static_cast<unsigned *>(Alloc(2 * sizeof(unsigned), "cudaMalloc fail counts"));
+                Cuda(cudaMemset(d_fail_count_, 0, 2 * sizeof(unsigned)), "cudaMemset");
+            }
+            if (opts_.prune) {
+                bs_smem_ = bm25k::BlockScoreSmem(plan_.tile_docs);
+                const void *bs = bm25k::BlockScoreKernelFor(plan_.tile_docs);
+                RaiseSmemCap(bs, bs_smem_);
+                int bs_per_sm = 0;
+                Cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bs_per_sm, bs, bm25k::kBsThreads, bs_smem_),
+                     "occupancy");
+                Check(bs_per_sm >= 1, "block score kernel does not fit an SM");
+                bs_grid_ = bs_per_sm * sms;
+            }
             ctrl_ = static_cast<bm25k::StreamCtrl *>(Alloc(sizeof(bm25k::StreamCtrl), "cudaMalloc ctrl"));
             threshold_ = static_cast<unsigned *>(Alloc(qc * sizeof(unsigned), "cudaMalloc threshold"));
             tslots_ = static_cast<unsigned *>(Alloc(qc * 32 * sizeof(unsigned), "cudaMalloc threshold slots"));
@@ -736,8 +870,8 @@ class Engine {
             plan_entries_ = static_cast<bm25k::PlanEntry *>(
                 Alloc(std::max<size_t>(1, opts_.word_capacity) * tiles_z * sizeof(bm25k::PlanEntry), "cudaMalloc plan"));
             Cuda(cudaMemset(ctrl_, 0, sizeof(bm25k::StreamCtrl)), "cudaMemset");
-            d_stats_ = static_cast<unsigned long long *>(Alloc(4 * sizeof(unsigned long long), "cudaMalloc stats"));
-            Cuda(cudaMemset(d_stats_, 0, 4 * sizeof(unsigned long long)), "cudaMemset");
+            d_stats_ = static_cast<unsigned long long *>(Alloc(bm25k::kStats * sizeof(unsigned long long), "cudaMalloc stats"));
+            Cuda(cudaMemset(d_stats_, 0, bm25k::kStats * sizeof(unsigned long long)), "cudaMemset");
             Cuda(cudaMemset(threshold_, 0, qc * sizeof(unsigned)), "cudaMemset");
             Cuda(cudaMemset(cand_count_, 0, qc * sizeof(unsigned)), "cudaMemset");
         }
@@ -747,7 +881,7 @@ class Engine {
     // tau / exact: the pruned Search's starting bounds and exactness flags (nullptr: plain Search).
     void Launch(int q, int k, const int64_t *qoffsets, const int32_t *words, float *out_scores, int32_t *out_ids,
                 unsigned *status, cudaStream_t s, const float *tau = nullptr, int32_t *exact = nullptr,
-                bool learned = false)
+                bool learned = false, const int32_t *kq = nullptr, const int64_t *kout = nullptr)
     {
         bm25k::TileArgs a{};
         a.indptr = (const long long *)d_indptr_;
@@ -807,27 +941,70 @@ class Engine {
             sa.out_ids = out_ids;
             sa.status = status;
             sa.stats = plan_.kernel == BM25_KERNEL_TILE_GROUP ? d_stats_ : nullptr;
+            // the retry pass answers the queries on the fail list: those whose starting bound proved
+            // too high, and (K > 32) those whose candidate buffer overflowed
+            // a batch with a K per query (kq): k is its largest K, each final select takes its queries
+            sa.kq = kq;
+            sa.kout = (const long long *)kout;
+            // pass 1 lists the queries it could not answer; retry pass 1 searches them on the plain
+            // path; with K > 32 a query whose buffer overflowed there (its slots were weak: a pruned
+            // first pass fell short) is searched once more from the slots that pass filled
+            const bool retry = tau != nullptr || k > bm25k::kMaxSmallK;
+            const bool retry2 = k > bm25k::kMaxSmallK;
+            int *list_a = d_fail_list_, *list_b = d_fail_list_ + opts_.query_capacity;
+            if (retry) {
+                sa.fail_out = list_a;
+                sa.fail_out_count = d_fail_count_;
+                Cuda(cudaMemsetAsync(d_fail_count_, 0, 2 * sizeof(unsigned), s), "fail count reset");
+            }
             if (learned) {  // tau is this session's bound array, written here
-                const bm25k::LearnedArgs la = LearnedArgsFor(q, k, qoffsets, words);
-                bm25k::LearnedBoundKernel<<<(q + bm25k::kLearnedThreads - 1) / bm25k::kLearnedThreads,
-                                            bm25k::kLearnedThreads, 0, s>>>(la);
+                bm25k::LearnedArgs la = LearnedArgsFor(q, k, qoffsets, words);
+                la.kq = kq;
+                bm25k::LearnedBoundKernel<<<q, bm25k::kLearnedThreads, 0, s>>>(la);
                 Cuda(cudaGetLastError(), "learned bound kernel launch");
             }
             if (tau) {
-                sa.dir_max = d_dir_max_;
-                sa.wbound = wbound_;
+                sa.boff = d_boff_;
+                sa.bmax = d_bmax_;
                 sa.tau = tau;
                 sa.exact = exact;
-                sa.fail_list = d_fail_list_;
-                sa.fail_count = d_fail_count_;
+                sa.items = d_items_;
+                sa.wrow = d_wrow_;
+                sa.item_count = d_item_count_;
+                sa.item_cap = item_cap_;
             }
             bm25k::PlanKernel<<<bm25k::PlanGrid(opts_.word_capacity, plan_.tiles, sms_), bm25k::kPlanThreads, 0, s>>>(sa);
             Cuda(cudaGetLastError(), "plan kernel launch");
+            const long long claims = (long long)q * ((plan_.tiles + bm25k::kWgWarps - 1) / bm25k::kWgWarps);
+            const int wg_grid = (int)std::max<long long>(1, std::min<long long>(plan_.grid, claims));
+            auto tile_group = [&](const bm25k::StreamArgs &args) {
+                if (plan_.tile_docs == 2048)
+                    bm25k::TileGroupKernel<2048><<<wg_grid, bm25k::kWgThreads, smem_bytes_, s>>>(args);
+                else
+                    bm25k::TileGroupKernel<1024><<<wg_grid, bm25k::kWgThreads, smem_bytes_, s>>>(args);
+            };
+            auto final_select = [&](const bm25k::StreamArgs &args) {
+                if (k <= bm25k::kMaxSmallK || kq)
+                    bm25k::FinalSelectKernel<<<q, bm25k::kFinalThreads, 0, s>>>(args);
+                if (k > bm25k::kMaxSmallK)
+                    bm25k::FinalSelectLargeKernel<<<q, bm25k::kLargeThreads, 0, s>>>(args);
+            };
             if (tau) {
-                bm25k::SeedBoundKernel<<<(q + 255) / 256, 256, 0, s>>>(sa);
-                Cuda(cudaGetLastError(), "seed kernel launch");
-            }
-            if (plan_.kernel == 0) {
+                // block-max pruned pass: bounds per (query, tile, block), then the kept blocks
+                const dim3 bgrid((plan_.tiles + bm25k::kBbThreads - 1) / bm25k::kBbThreads, q);
+                if (plan_.tile_docs == 2048)
+                    bm25k::BlockBoundKernel<2048><<<bgrid, bm25k::kBbThreads, 0, s>>>(sa);
+                else
+                    bm25k::BlockBoundKernel<1024><<<bgrid, bm25k::kBbThreads, 0, s>>>(sa);
+                Cuda(cudaGetLastError(), "block bound kernel launch");
+                MarkKernel(0, s);
+                if (plan_.tile_docs == 2048)
+                    bm25k::BlockScoreKernel<2048><<<bs_grid_, bm25k::kBsThreads, bs_smem_, s>>>(sa);
+                else
+                    bm25k::BlockScoreKernel<1024><<<bs_grid_, bm25k::kBsThreads, bs_smem_, s>>>(sa);
+                Cuda(cudaGetLastError(), "block score kernel launch");
+                MarkKernel(1, s);
+            } else if (plan_.kernel == 0) {
                 const int grid = (int)std::min<long long>(
                     plan_.grid, ((long long)q * plan_.tiles + bm25k::kTaskBatch - 1) / bm25k::kTaskBatch);
                 MarkKernel(0, s);
@@ -835,36 +1012,39 @@ class Engine {
                 Cuda(cudaGetLastError(), "stream kernel launch");
                 MarkKernel(1, s);
             } else {
-                // one claim per CTA at least, at most the resident grid
-                const long long claims = (long long)q * ((plan_.tiles + bm25k::kWgWarps - 1) / bm25k::kWgWarps);
-                const int grid = (int)std::max<long long>(1, std::min<long long>(plan_.grid, claims));
                 MarkKernel(0, s);
-                if (plan_.tile_docs == 2048)
-                    bm25k::TileGroupKernel<2048><<<grid, bm25k::kWgThreads, smem_bytes_, s>>>(sa);
-                else
-                    bm25k::TileGroupKernel<1024><<<grid, bm25k::kWgThreads, smem_bytes_, s>>>(sa);
+                tile_group(sa);
                 Cuda(cudaGetLastError(), "tile group kernel launch");
                 MarkKernel(1, s);
             }
-            bm25k::FinalSelectKernel<<<q, bm25k::kFinalThreads, 0, s>>>(sa);
-            if (tau) {
-                // retry pass: the queries whose bound proved too high, on the plain path (an
-                // empty fail list ends both kernels at once)
-                Cuda(cudaGetLastError(), "final select launch");
+            final_select(sa);
+            Cuda(cudaGetLastError(), "final select launch");
+            if (retry) {
+                // retry pass on the plain path (an empty fail list ends both kernels at once)
                 bm25k::StreamArgs ra = sa;
-                ra.wbound = nullptr;
-                ra.dir_max = nullptr;
                 ra.tau = nullptr;
                 ra.exact = nullptr;
+                ra.items = nullptr;
+                ra.wrow = nullptr;
+                ra.item_count = nullptr;
                 ra.retry = 1;
-                const long long claims = (long long)q * ((plan_.tiles + bm25k::kWgWarps - 1) / bm25k::kWgWarps);
-                const int grid = (int)std::max<long long>(1, std::min<long long>(plan_.grid, claims));
-                if (plan_.tile_docs == 2048)
-                    bm25k::TileGroupKernel<2048><<<grid, bm25k::kWgThreads, smem_bytes_, s>>>(ra);
-                else
-                    bm25k::TileGroupKernel<1024><<<grid, bm25k::kWgThreads, smem_bytes_, s>>>(ra);
+                ra.fail_in = list_a;
+                ra.fail_in_count = d_fail_count_;
+                ra.fail_out = retry2 ? list_b : nullptr;
+                ra.fail_out_count = retry2 ? d_fail_count_ + 1 : nullptr;
+                tile_group(ra);
                 Cuda(cudaGetLastError(), "retry kernel launch");
-                bm25k::FinalSelectKernel<<<q, bm25k::kFinalThreads, 0, s>>>(ra);
+                final_select(ra);
+                if (retry2) {
+                    bm25k::StreamArgs rb = ra;
+                    rb.fail_in = list_b;
+                    rb.fail_in_count = d_fail_count_ + 1;
+                    rb.fail_out = nullptr;
+                    rb.fail_out_count = nullptr;
+                    tile_group(rb);
+                    Cuda(cudaGetLastError(), "second retry kernel launch");
+                    final_select(rb);
+                }
             }
         }
         Cuda(cudaGetLastError(), "search kernel launch");
@@ -888,11 +1068,13 @@ class Engine {
         timed_ = 0;
     }
 
-    static constexpr int kModePlain = 0, kModePruned = 1, kModeLearned = 2;
+    static constexpr int kModePlain = 0, kModePruned = 1, kModeLearned = 2, kModeMixed = 4;
 
     cudaGraphExec_t GraphFor(int q, int k, int mode = kModePlain)
     {
         const auto key = std::make_tuple(q, k, mode);
+        const bool mixed = (mode & kModeMixed) != 0;
+        mode &= ~kModeMixed;
         const bool pruned = mode != kModePlain;
         auto it = graphs_.find(key);
         if (it != graphs_.end())
@@ -902,7 +1084,9 @@ class Engine {
         Cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin graph capture");
         try {
             // the plain Search sends the query packet; the pruned one adds the bounds after it
-            Cuda(cudaMemcpyAsync(d_in_, h_in_, mode == kModePruned ? tau_offset_ + (size_t)q * sizeof(float) : tau_offset_,
+            Cuda(cudaMemcpyAsync(d_in_, h_in_,
+                                 mixed ? in_bytes_
+                                       : (mode == kModePruned ? tau_offset_ + (size_t)q * sizeof(float) : tau_offset_),
                                  cudaMemcpyHostToDevice, stream_),
                  "query H2D");
             unsigned *status = reinterpret_cast<unsigned *>(d_out_ + StatusOffset(q, k));
@@ -913,10 +1097,13 @@ class Engine {
                    mode == kModePruned ? reinterpret_cast<const float *>(d_in_ + tau_offset_)
                                        : (mode == kModeLearned ? d_tau_ : nullptr),
                    pruned ? reinterpret_cast<int32_t *>(d_out_ + ExactOffset(q, k)) : nullptr,
-                   mode == kModeLearned);
-            Cuda(cudaMemcpyAsync(h_out_, d_out_, pruned ? ExactOffset(q, k) + (size_t)q * 4 : StatusOffset(q, k) + 32,
-                                 cudaMemcpyDeviceToHost, stream_),
-                 "top-K D2H");
+                   mode == kModeLearned, mixed ? reinterpret_cast<const int32_t *>(d_in_ + ks_offset_) : nullptr,
+                   mixed ? reinterpret_cast<const int64_t *>(d_in_ + kout_offset_) : nullptr);
+            if (!mixed)  // a batch's result size varies per call: copied after the replay
+                Cuda(cudaMemcpyAsync(h_out_, d_out_,
+                                     pruned ? ExactOffset(q, k) + (size_t)q * 4 : StatusOffset(q, k) + 32,
+                                     cudaMemcpyDeviceToHost, stream_),
+                     "top-K D2H");
         } catch (...) {
             cudaStreamEndCapture(stream_, &graph);
             if (graph)
@@ -1012,8 +1199,16 @@ class Engine {
     float *d_data_ = nullptr;
     int32_t *d_dir_row_ = nullptr, *d_dir_ = nullptr;
     std::vector<bm25k::Level> levels_;
-    size_t word_offset_ = 0, tau_offset_ = 0, in_bytes_ = 0, out_bytes_ = 0, smem_bytes_ = 0;
-    float *d_dir_max_ = nullptr, *wbound_ = nullptr;
+    size_t word_offset_ = 0, tau_offset_ = 0, ks_offset_ = 0, kout_offset_ = 0, in_bytes_ = 0, out_bytes_ = 0,
+           smem_bytes_ = 0;
+    unsigned short *d_boff_ = nullptr;
+    float *d_bmax_ = nullptr;
+    uint4 *d_items_ = nullptr;
+    int *d_wrow_ = nullptr;
+    unsigned *d_item_count_ = nullptr;
+    long long item_cap_ = 0;
+    size_t bs_smem_ = 0;
+    int bs_grid_ = 0;
     void *h_in_ = nullptr, *h_out_ = nullptr;
     unsigned char *d_in_ = nullptr, *d_out_ = nullptr;
     unsigned *d_dev_status_ = nullptr;
@@ -1250,6 +1445,53 @@ int bm25_search_learned_device(bm25_handle *h, const int64_t *qoffsets, const in
                 throw bm25b200::InvalidState("BM25 is not initialized");
             h->engine->SearchPrunedDevice(qoffsets, words, nullptr, q, k, out_scores, out_ids, out_exact,
                                           static_cast<cudaStream_t>(stream));
+        },
+        h->error, h->code);
+}
+
+int bm25_search_batch(bm25_handle *h, const int64_t *qoffsets, const int32_t *words, const int32_t *ks, int64_t q,
+                      float *out_scores, int32_t *out_ids)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            h->engine->SearchBatch(qoffsets, words, ks, q, false, out_scores, out_ids, nullptr);
+        },
+        h->error, h->code);
+}
+
+int bm25_search_batch_learned(bm25_handle *h, const int64_t *qoffsets, const int32_t *words, const int32_t *ks,
+                              int64_t q, float *out_scores, int32_t *out_ids, int32_t *out_exact)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            h->engine->SearchBatch(qoffsets, words, ks, q, true, out_scores, out_ids, out_exact);
+        },
+        h->error, h->code);
+}
+
+int bm25_search_batch_device(bm25_handle *h, const int64_t *qoffsets, const int32_t *words, const int32_t *ks,
+                             const int64_t *kout, int64_t q, int32_t kmax, int32_t learned, float *out_scores,
+                             int32_t *out_ids, int32_t *out_exact, void *stream)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            h->engine->SearchBatchDevice(qoffsets, words, ks, kout, q, kmax, learned != 0, out_scores, out_ids,
+                                         out_exact, static_cast<cudaStream_t>(stream));
         },
         h->error, h->code);
 }

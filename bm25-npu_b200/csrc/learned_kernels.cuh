@@ -5,17 +5,20 @@
 //   document frequency) and its mean posting score.
 // QueryFeatures -- 32 features of one query from those statistics (the
 //   query's four strongest words by top score, sums and extremes over all its
-//   words, K), plus the query's safe bound: the largest, over its words, of the
-//   word's K-th largest posting score.  K documents each hold that word with at
-//   least that score, and every FP32 sum of non-negative contributions is at
-//   least each of its terms (rounded addition is monotone), so K documents
-//   reach the safe bound: it never makes a query fall back.
+//   words, K), plus the query's safe bound: for K <= 32 the largest, over its
+//   words, of the word's K-th largest posting score (K documents each hold that
+//   word with at least that score, and every FP32 sum of non-negative
+//   contributions is at least each of its terms -- rounded addition is
+//   monotone -- so K documents reach it and it never makes a query fall back);
+//   0 for K > 32; -1 when the query's words hold fewer than K postings in all
+//   (fewer than K documents can match: such a query is not pruned).
 // LearnedBoundKernel -- features -> threshold MLP (log of the K-th score) ->
 //   tau = max(exp(prediction - margin), safe bound); without a model tau is the
-//   safe bound.  A query whose safe bound is 0 (no word with K postings) gets
-//   tau = 0 and is not pruned.
+//   safe bound; tau = 0 where the safe bound is -1.
 #pragma once
 #include "mlp.cuh"
+#include <cfloat>
+#include <climits>
 #include "tile_kernels.cuh"
 
 namespace bm25k {
@@ -56,6 +59,7 @@ struct LearnedArgs {
     const long long *qoffsets;
     const int *words;
     int q, k;
+    const int *kq;  // [q] K per query, or nullptr: every query takes k
     long long word_cap;
     const float *params;  // threshold MLP, or nullptr: safe bounds only
     float margin;
@@ -66,114 +70,179 @@ struct LearnedArgs {
 
 __device__ __forceinline__ float LogScore(float x) { return log1pf(fmaxf(x, 0.0f)); }
 
-// Features of query q (layout: 4 strongest words x [log1p top, log1p K-th, log1p mean,
-// log1p(df) / 16], then valid words / 8, log1p of the sums of tops, K-ths and means, log1p
-// of the largest K-th, log(K) / 4, summed and least log1p(df), log1p of the largest and of the
-// summed (K+1)/2-th scores, out-of-vocabulary words / 8, a constant 1, four zeros).
-__device__ __forceinline__ float QueryFeatures(const LearnedArgs &a, int q, float *f)
+// Features of query q, computed by one warp (lane l takes the query's words l and l + 32; sums
+// and extremes are warp reductions in a fixed order, so the result is deterministic).  Layout:
+// 4 strongest words by top score (an earlier word ahead of an equal one) x [log1p top, log1p
+// K-th, log1p mean, log1p(df) / 16], then valid words / 8, log1p of the sums of tops, K-ths and
+// means, log1p of the largest K-th, log(K) / 4, summed and least log1p(df), log1p of the largest
+// and of the summed (K+1)/2-th scores, out-of-vocabulary words / 8, a constant 1, four zeros;
+// the K-th and (K+1)/2-th scores are taken at min(K, 32).  Lane 0 writes f and returns the safe
+// bound (every lane returns it).
+__device__ __forceinline__ float QueryFeaturesWarp(const LearnedArgs &a, int q, float *f, int lane)
 {
     const long long qb = a.qoffsets[q], qe = a.qoffsets[q + 1];
-    long long n = qe - qb;
-    if (n < 0 || n > kMaxTerms || qb < 0 || qb + n > a.word_cap)
-        n = 0;  // the Search reports the malformed query
-    const int k = a.k, h = (k - 1) / 2;
-    float sum_top = 0.0f, sum_kth = 0.0f, max_kth = 0.0f, sum_mean = 0.0f, sum_ldf = 0.0f, min_ldf = 0.0f;
-    float max_half = 0.0f, sum_half = 0.0f;
+    long long nl = qe - qb;
+    if (nl < 0 || nl > kMaxTerms || qb < 0 || qb + nl > a.word_cap)
+        nl = 0;  // the Search reports the malformed query
+    const int n = (int)nl;
+    const int k = a.kq ? min(max(a.kq[q], 1), a.k) : a.k, kk = min(k, kTermTop), h = (kk - 1) / 2;
+    long long postings = 0;
+    float sum_top = 0.0f, sum_kth = 0.0f, max_kth = 0.0f, sum_mean = 0.0f, sum_ldf = 0.0f;
+    float min_ldf = FLT_MAX, max_half = 0.0f, sum_half = 0.0f;
     int valid = 0, oov = 0;
-    int best[4] = {-1, -1, -1, -1};
-    float best_top[4] = {-1.0f, -1.0f, -1.0f, -1.0f};
-    for (long long i = 0; i < n; ++i) {
+    float top_of[2] = {-1.0f, -1.0f};  // this lane's words (position lane, lane + 32)
+    int word_of[2] = {-1, -1};
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        const int i = lane + 32 * u;
+        if (i >= n)
+            continue;
         const int w = a.words[qb + i];
         if (w < 0 || w >= a.vocab) {
             ++oov;
             continue;
         }
         const float *t = a.top + (long long)w * kTermTop;
-        const float mx = t[0], kth = t[k - 1], half = t[h];
-        const float ldf = log1pf((float)(a.indptr[w + 1] - a.indptr[w]));
+        const float mx = t[0], kth = t[kk - 1], half = t[h];
+        const long long df = a.indptr[w + 1] - a.indptr[w];
+        postings += df;
+        const float ldf = log1pf((float)df);
         sum_top += mx;
         sum_kth += kth;
         max_kth = fmaxf(max_kth, kth);
         sum_mean += a.mean[w];
         sum_ldf += ldf;
-        min_ldf = valid ? fminf(min_ldf, ldf) : ldf;
+        min_ldf = fminf(min_ldf, ldf);
         max_half = fmaxf(max_half, half);
         sum_half += half;
         ++valid;
-        int pos = 4;  // strongest words first; an earlier word stays ahead of an equal one
-        while (pos > 0 && mx > best_top[pos - 1])
-            --pos;
-        if (pos < 4) {
-            for (int j = 3; j > pos; --j) {
-                best_top[j] = best_top[j - 1];
-                best[j] = best[j - 1];
-            }
-            best_top[pos] = mx;
-            best[pos] = w;
-        }
+        top_of[u] = mx;
+        word_of[u] = w;
     }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        postings += __shfl_xor_sync(kFull, postings, o);
+        sum_top += __shfl_xor_sync(kFull, sum_top, o);
+        sum_kth += __shfl_xor_sync(kFull, sum_kth, o);
+        max_kth = fmaxf(max_kth, __shfl_xor_sync(kFull, max_kth, o));
+        sum_mean += __shfl_xor_sync(kFull, sum_mean, o);
+        sum_ldf += __shfl_xor_sync(kFull, sum_ldf, o);
+        min_ldf = fminf(min_ldf, __shfl_xor_sync(kFull, min_ldf, o));
+        max_half = fmaxf(max_half, __shfl_xor_sync(kFull, max_half, o));
+        sum_half += __shfl_xor_sync(kFull, sum_half, o);
+        valid += __shfl_xor_sync(kFull, valid, o);
+        oov += __shfl_xor_sync(kFull, oov, o);
+    }
+    // the four strongest words: four rounds of a warp arg-max on (top desc, position asc)
+#pragma unroll
     for (int j = 0; j < 4; ++j) {
-        const int w = best[j];
-        if (w < 0) {
-            f[4 * j] = f[4 * j + 1] = f[4 * j + 2] = f[4 * j + 3] = 0.0f;
-            continue;
+        const int u = top_of[1] > top_of[0] ? 1 : 0;  // position lane + 32u; ties keep the earlier
+        float bt = top_of[u];
+        int bp = word_of[u] >= 0 ? lane + 32 * u : INT_MAX;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const float ot = __shfl_xor_sync(kFull, bt, o);
+            const int op = __shfl_xor_sync(kFull, bp, o);
+            if (ot > bt || (ot == bt && op < bp)) {
+                bt = ot;
+                bp = op;
+            }
         }
-        const float *t = a.top + (long long)w * kTermTop;
-        f[4 * j] = LogScore(t[0]);
-        f[4 * j + 1] = LogScore(t[k - 1]);
-        f[4 * j + 2] = LogScore(a.mean[w]);
-        f[4 * j + 3] = log1pf((float)(a.indptr[w + 1] - a.indptr[w])) / 16.0f;
+        int w = -1;
+        if (bp != INT_MAX && bt >= 0.0f && (bp & 31) == lane) {  // the owner drops its winner
+            w = word_of[bp >> 5];
+            top_of[bp >> 5] = -1.0f;
+            word_of[bp >> 5] = -1;
+        }
+        w = __shfl_sync(kFull, w, bp != INT_MAX && bt >= 0.0f ? (bp & 31) : 0);
+        if (lane == 0) {
+            if (bp == INT_MAX || bt < 0.0f || w < 0) {
+                f[4 * j] = f[4 * j + 1] = f[4 * j + 2] = f[4 * j + 3] = 0.0f;
+            } else {
+                const float *t = a.top + (long long)w * kTermTop;
+                f[4 * j] = LogScore(t[0]);
+                f[4 * j + 1] = LogScore(t[kk - 1]);
+                f[4 * j + 2] = LogScore(a.mean[w]);
+                f[4 * j + 3] = log1pf((float)(a.indptr[w + 1] - a.indptr[w])) / 16.0f;
+            }
+        }
     }
-    f[16] = valid / 8.0f;
-    f[17] = LogScore(sum_top);
-    f[18] = LogScore(sum_kth);
-    f[19] = LogScore(max_kth);
-    f[20] = LogScore(sum_mean);
-    f[21] = logf((float)k) / 4.0f;
-    f[22] = sum_ldf / 64.0f;
-    f[23] = min_ldf / 16.0f;
-    f[24] = LogScore(max_half);
-    f[25] = LogScore(sum_half);
-    f[26] = oov / 8.0f;
-    f[27] = 1.0f;
-    f[28] = f[29] = f[30] = f[31] = 0.0f;
-    return max_kth;
+    if (lane == 0) {
+        f[16] = valid / 8.0f;
+        f[17] = LogScore(sum_top);
+        f[18] = LogScore(sum_kth);
+        f[19] = LogScore(max_kth);
+        f[20] = LogScore(sum_mean);
+        f[21] = logf((float)k) / 4.0f;
+        f[22] = sum_ldf / 64.0f;
+        f[23] = valid ? min_ldf / 16.0f : 0.0f;
+        f[24] = LogScore(max_half);
+        f[25] = LogScore(sum_half);
+        f[26] = oov / 8.0f;
+        f[27] = 1.0f;
+        f[28] = f[29] = f[30] = f[31] = 0.0f;
+    }
+    __syncwarp();
+    if (postings < k)
+        return -1.0f;
+    return k <= kTermTop ? max_kth : 0.0f;
 }
 
+// One warp per query.
 __global__ void QueryFeaturesKernel(const LearnedArgs a)
 {
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < a.q; q += gridDim.x * blockDim.x) {
-        float f[kFeatures];
-        const float safe = QueryFeatures(a, q, f);
-        for (int i = 0; i < kFeatures; ++i)
-            a.features[(long long)q * kFeatures + i] = f[i];
-        if (a.safe)
+    __shared__ float fs[8][kFeatures];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int q = blockIdx.x * (blockDim.x >> 5) + warp; q < a.q; q += gridDim.x * (blockDim.x >> 5)) {
+        float *f = fs[warp];
+        const float safe = QueryFeaturesWarp(a, q, f, lane);
+        a.features[(long long)q * kFeatures + lane] = f[lane];
+        if (a.safe && lane == 0)
             a.safe[q] = safe;
+        __syncwarp();
     }
 }
 
-constexpr int kLearnedThreads = 64;
+constexpr int kLearnedThreads = bm25mlp::kH;
 
+// One CTA per query: warp 0 builds the features, thread i computes hidden unit i of each
+// layer (the same fmaf chain, in the same order, as bm25mlp::Forward, so the prediction is
+// bit-identical to the training kernels' forward pass), thread 0 the output and the bound.
 __global__ void __launch_bounds__(kLearnedThreads) LearnedBoundKernel(const LearnedArgs a)
 {
-    __shared__ float p[bm25mlp::kParams];
-    if (a.params) {
-        for (int i = threadIdx.x; i < bm25mlp::kParams; i += kLearnedThreads)
-            p[i] = a.params[i];
+    using namespace bm25mlp;
+    __shared__ float f[kFeatures], h1[kH], h2[kH];
+    __shared__ float safe_s;
+    const int q = blockIdx.x, i = threadIdx.x;
+    if (i < 32) {
+        const float safe = QueryFeaturesWarp(a, q, f, i);
+        if (i == 0)
+            safe_s = safe;
     }
     __syncthreads();
-    const int q = blockIdx.x * kLearnedThreads + threadIdx.x;
-    if (q >= a.q)
+    const float safe = safe_s;
+    if (!a.params || safe < 0.0f) {  // uniform
+        if (i == 0)
+            a.tau[q] = fmaxf(safe, 0.0f);
         return;
-    float f[kFeatures];
-    const float safe = QueryFeatures(a, q, f);
-    float tau = safe;
-    if (a.params && safe > 0.0f) {
-        float h1[bm25mlp::kH], h2[bm25mlp::kH];
-        const float y = bm25mlp::Forward(p, f, h1, h2);
-        tau = fmaxf(expf(y - a.margin), safe);  // a NaN prediction leaves the safe bound
     }
-    a.tau[q] = tau;
+    const float *p = a.params;
+    float acc = __ldg(p + kOffB1 + i);
+    for (int j = 0; j < kIn; ++j)
+        acc = fmaf(__ldg(p + kOffW1 + i * kIn + j), f[j], acc);
+    h1[i] = fmaxf(acc, 0.0f);
+    __syncthreads();
+    acc = __ldg(p + kOffB2 + i);
+    for (int j = 0; j < kH; ++j)
+        acc = fmaf(__ldg(p + kOffW2 + i * kH + j), h1[j], acc);
+    h2[i] = fmaxf(acc, 0.0f);
+    __syncthreads();
+    if (i == 0) {
+        float y = __ldg(p + kOffB3);
+        for (int j = 0; j < kH; ++j)
+            y = fmaf(__ldg(p + kOffW3 + j), h2[j], y);
+        a.tau[q] = fmaxf(expf(y - a.margin), safe);  // a NaN prediction leaves the safe bound
+    }
 }
 
 } // namespace bm25k

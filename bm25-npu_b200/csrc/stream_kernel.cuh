@@ -45,6 +45,7 @@
 #include "tile_kernels.cuh"
 
 #include <algorithm>
+#include <climits>
 
 namespace bm25k {
 
@@ -64,6 +65,18 @@ constexpr int kPlanThreads = 256;
 enum : uint32_t {
     kStatusTimeout = 16u,       // a bounded wait gave up
     kStatusCandOverflow = 32u,  // a query's candidate buffer was too small
+};
+
+// Search counters (StreamArgs::stats): tile-group claims, tiles and postings copied into the
+// rings; block path: tiles scored, 128-document blocks kept, postings read.
+enum : int {
+    kStatClaims = 0,
+    kStatTilesScanned = 1,
+    kStatPostingsCopied = 2,
+    kStatItems = 3,
+    kStatBlocksKept = 4,
+    kStatPostingsRead = 5,
+    kStats = 6,
 };
 
 enum : int {
@@ -105,18 +118,38 @@ struct StreamArgs {
     float *out_scores;
     int *out_ids;
     unsigned *status;
-    // pruned Search (tile-group kernel): nullptr on the plain path
-    const float *dir_max;  // [dir row][tile] largest posting score of the row's term in the tile
-    float *wbound;         // [word][tile] upper bound of the word's score in the tile (PlanKernel output)
-    const float *tau;      // [Q] starting bound guesses
-    int *exact;            // [Q] 1 where K candidates reached tau
-    int *fail_list;        // queries whose pruned pass fell short, in the order found
-    unsigned *fail_count;  // their count (reset by SeedBoundKernel)
-    int retry;             // nonzero: this pass searches the fail_list queries on the plain path
-    // tile-group kernel counters, accumulated (nullptr: not kept): claims taken, claims dropped
-    // whole by their bounds, tiles scanned, postings copied into the rings
-    unsigned long long *stats;
+    // pruned Search (block kernels): nullptr on the plain path
+    const unsigned short *boff;  // [dir row][tile][block] posting offset of the block from the tile's start
+    const float *bmax;           // [dir row][tile][block] largest posting score of the row's term in the block
+    const float *tau;            // [Q] starting bound guesses
+    int *exact;                  // [Q] 1 where K candidates reached tau
+    uint4 *items;                // (query | kept-block mask << 16, tile, first word, words) per tile to score
+    int *wrow;                   // [word] directory row of the word's term, -1 none, -2 not a valid term
+    unsigned *item_count;        // [2]: items listed, items taken (both reset by PlanKernel)
+    long long item_cap;
+    // retry passes: a pass appends to fail_out the queries it could not answer (a pruned pass that
+    // fell short of K, a K > 32 candidate buffer that overflowed); a retry pass (retry != 0)
+    // searches the queries of fail_in on the plain path.  Counts are reset before the Search.
+    const int *fail_in;
+    const unsigned *fail_in_count;
+    int *fail_out;
+    unsigned *fail_out_count;
+    int retry;
+    unsigned long long *stats;   // [kStats] counters, accumulated (nullptr: not kept)
+    // a batch with a K per query (tile-group kernel): nullptr when every query takes a.k
+    const int *kq;               // [Q] K of each query (a.k is their maximum)
+    const long long *kout;       // [Q] first output slot of each query (packed rows)
 };
+
+// K of query q, and the first output slot of its row.
+__device__ __forceinline__ int QueryK(const StreamArgs &a, int q)
+{
+    return a.kq ? min(max(__ldg(a.kq + q), 1), a.k) : a.k;
+}
+__device__ __forceinline__ long long OutRow(const StreamArgs &a, int q)
+{
+    return a.kout ? __ldg(a.kout + q) : (long long)q * a.k;
+}
 
 struct __align__(16) StageMeta {
     long long base;  // posting position of ring element 0
@@ -453,6 +486,8 @@ __device__ __forceinline__ long long WarpLowerBoundGlobal(const int *ids, long l
 __global__ void __launch_bounds__(kPlanThreads) PlanKernel(const StreamArgs a)
 {
     __shared__ long long range[2];
+    if (a.item_count && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < 2)
+        a.item_count[threadIdx.x] = 0u;  // the block path's work list of this Search starts empty
     long long total = a.qoffsets[a.q];
     if (total < 0 || total > a.word_cap) {
         if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
@@ -467,33 +502,25 @@ __global__ void __launch_bounds__(kPlanThreads) PlanKernel(const StreamArgs a)
     for (long long w = blockIdx.x; w < total; w += gridDim.x) {
         const int term = a.words[w];
         PlanEntry *out = a.plan + w * a.tiles;
-        float *wb = a.wbound ? a.wbound + w * a.tiles : nullptr;
+        if (a.wrow && blockIdx.y == 0 && tid == 0)
+            a.wrow[w] = term < 0 || term >= a.vocab ? -2 : (a.dir_row ? a.dir_row[term] : -1);
         if (term < 0 || term >= a.vocab) {
             if (term < 0 && tid == 0 && blockIdx.y == 0)
                 atomicOr(a.status, kStatusBadWord);
-            for (int t = t0 + tid; t < t1; t += kPlanThreads) {
+            for (int t = t0 + tid; t < t1; t += kPlanThreads)
                 out[t] = PlanEntry{0, 0};
-                if (wb)
-                    wb[t] = 0.0f;
-            }
             continue;
         }
         const long long s = a.indptr[term], e = a.indptr[term + 1];
         const int r = a.dir_row ? a.dir_row[term] : -1;
         if (r >= 0) {
             const int *d = a.dir + (long long)r * a.dir_stride;
-            for (int t = t0 + tid; t < t1; t += kPlanThreads) {
+            for (int t = t0 + tid; t < t1; t += kPlanThreads)
                 out[t] = PlanEntry{s + d[t], s + d[t + 1]};
-                if (wb)
-                    wb[t] = a.dir_max[(long long)r * a.tiles + t];
-            }
             continue;
         }
-        for (int t = t0 + tid; t < t1; t += kPlanThreads) {
+        for (int t = t0 + tid; t < t1; t += kPlanThreads)
             out[t] = PlanEntry{0, 0};
-            if (wb)
-                wb[t] = 0.0f;
-        }
         if (tid < 32) {
             // lists up to kPlanScanAll postings are scanned whole by every CTA of the word; a
             // longer one (a list left out of the directory by its byte budget) is first cut to
@@ -518,8 +545,6 @@ __global__ void __launch_bounds__(kPlanThreads) PlanKernel(const StreamArgs a)
                 out[t].b = i;
             if (i == e - 1 || __ldg(a.indices + i + 1) / a.tile_docs != t)
                 out[t].e = i + 1;
-            if (wb)  // bits of scores >= 0 order like the values (a negative one is bounded by 0)
-                atomicMax(reinterpret_cast<unsigned *>(wb + t), __float_as_uint(fmaxf(__ldg(a.data + i), 0.0f)));
         }
         __syncthreads();  // range[] is rewritten for the next word
     }
@@ -836,11 +861,13 @@ __global__ void __launch_bounds__(kFinalThreads) FinalSelectKernel(const StreamA
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     int q = blockIdx.x;
     if (a.retry) {  // block b answers the b-th query of the fail list
-        if ((unsigned)q >= __ldcg(a.fail_count))
+        if ((unsigned)q >= __ldcg(a.fail_in_count))
             return;
-        q = __ldcg(a.fail_list + q);
+        q = __ldcg(a.fail_in + q);
     }
-    const int k = a.k;
+    const int k = QueryK(a, q);
+    if (k > kMaxSmallK)
+        return;  // FinalSelectLargeKernel's query
     const unsigned appended = __ldcg(a.cand_count + q);
     const int n = (int)min((long long)appended, a.cand_cap);
     if (tid == 0 && (long long)appended > a.cand_cap)
@@ -976,50 +1003,331 @@ __global__ void __launch_bounds__(kFinalThreads) FinalSelectKernel(const StreamA
             }
         }
         if (lane < k) {
-            a.out_scores[(long long)q * k + lane] = ls;
-            a.out_ids[(long long)q * k + lane] = li;
+            a.out_scores[OutRow(a, q) + lane] = ls;
+            a.out_ids[OutRow(a, q) + lane] = li;
         }
-        if (a.exact && !a.retry && lane == 0) {  // K results at or above the starting bound, or no bound
-            const int ok = cnt == k || !(a.tau[q] > 0.0f) ? 1 : 0;
-            a.exact[q] = ok;
-            if (!ok)
-                a.fail_list[atomicAdd(a.fail_count, 1u)] = q;
+        // K results at or above the starting bound, or no bound: the pruned result stands.  A
+        // query that fell short keeps its group slots (real documents' scores, so still lower
+        // bounds) for the retry pass; its threshold, which started at the guess, is dropped.
+        const bool failed = a.exact && !a.retry && !(cnt == k || !(a.tau[q] > 0.0f));
+        if (a.exact && !a.retry && lane == 0) {
+            a.exact[q] = failed ? 0 : 1;
+            if (failed)
+                a.fail_out[atomicAdd(a.fail_out_count, 1u)] = q;
         }
         if (lane == 0) {
             a.cand_count[q] = 0u;
             a.threshold[q] = 0u;
         }
+        if (!failed)
+            a.tslots[(long long)q * 32 + lane] = 0u;
+    }
+}
+
+// ---- final selection for K > 32 -------------------------------------------------
+//
+// One CTA per query over the query's candidate buffer (every document a tile
+// appended at or above the running bound): candidates below the final floor are
+// dropped, the K-th largest FP32 key (bit pattern of a positive score) is found by
+// three radix passes (11/10/10 bits) of a shared-memory histogram, the documents
+// above it are taken whole and the ties at it by ascending id (sorted in shared
+// memory, or by a second radix select on ids when they do not fit), then the K
+// results are sorted by (score desc, id asc) with a bitonic network and the
+// zero-score fill takes the smallest free ids.  A query whose buffer overflowed is
+// put on the fail list; a retry pass searches it again from its group slots (real
+// documents' scores: its first pass has filled them).
+constexpr int kLargeThreads = 512;
+constexpr int kLargeMaxK = 1024;
+constexpr int kLargeEqCap = 2048;
+constexpr int kRadixBins = 2048;
+
+struct LargeShared {
+    unsigned hist[kRadixBins];
+    float sel_s[kLargeMaxK];
+    int sel_i[kLargeMaxK];
+    int eq[kLargeEqCap];
+    unsigned wsum[kLargeThreads / 32];
+    unsigned fill[kLargeMaxK / 32];
+    unsigned sel_count, eq_count, total;
+    int bucket;
+    unsigned above;
+};
+
+// Every thread calls.  Histogram of bits [shift, shift + log2 bins) of the keys that match
+// `prefix` on `mask`; returns the bin holding the need-th largest such key and, in *above,
+// the count of matching keys in higher bins (need >= 1 and at most the matching count).
+template <class KeyOf>
+__device__ int RadixStep(LargeShared &sh, int n, const KeyOf &key_of, unsigned prefix, unsigned mask, int shift,
+                         int bins, unsigned need, unsigned *above)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < bins; i += kLargeThreads)
+        sh.hist[i] = 0u;
+    __syncthreads();
+    for (int i = tid; i < n; i += kLargeThreads) {
+        unsigned key;
+        if (key_of(i, &key) && (key & mask) == prefix)
+            atomicAdd(&sh.hist[(key >> shift) & (unsigned)(bins - 1)], 1u);
+    }
+    __syncthreads();
+    // thread t owns bins [hi - per, hi), hi = bins - t * per: thread 0 holds the top bins
+    const int per = bins / kLargeThreads;
+    const int hi = bins - tid * per;
+    unsigned local = 0;
+    for (int b = hi - 1; b >= hi - per; --b)
+        local += sh.hist[b];
+    unsigned incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned v = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o)
+            incl += v;
+    }
+    if (lane == 31)
+        sh.wsum[warp] = incl;
+    __syncthreads();
+    for (int w = 0; w < warp; ++w)
+        incl += sh.wsum[w];
+    const unsigned excl = incl - local;
+    if (excl < need && need <= incl) {
+        unsigned c = excl;
+        for (int b = hi - 1; b >= hi - per; --b) {
+            if (c + sh.hist[b] >= need) {
+                sh.bucket = b;
+                sh.above = c;
+                break;
+            }
+            c += sh.hist[b];
+        }
+    }
+    __syncthreads();
+    *above = sh.above;
+    const int bucket = sh.bucket;
+    __syncthreads();  // hist and the results are rewritten by the next step
+    return bucket;
+}
+
+// The need-th largest 31-bit key among the candidates key_of accepts (three passes).
+template <class KeyOf>
+__device__ unsigned RadixSelect31(LargeShared &sh, int n, const KeyOf &key_of, unsigned need, unsigned *rest)
+{
+    unsigned above, prefix = 0, mask = 0;
+    int b = RadixStep(sh, n, key_of, prefix, mask, 20, 2048, need, &above);
+    prefix |= (unsigned)b << 20;
+    mask |= 0x7ffu << 20;
+    need -= above;
+    b = RadixStep(sh, n, key_of, prefix, mask, 10, 1024, need, &above);
+    prefix |= (unsigned)b << 10;
+    mask |= 0x3ffu << 10;
+    need -= above;
+    b = RadixStep(sh, n, key_of, prefix, mask, 0, 1024, need, &above);
+    prefix |= (unsigned)b;
+    need -= above;
+    *rest = need;  // keys equal to the result still to take (>= 1)
+    return prefix;
+}
+
+// Bitonic sort of p (a power of two <= 2048) entries in shared memory; `before(i, j)`
+// orders entry i ahead of entry j; `swap(i, j)` exchanges them.  Every thread calls.
+template <class Before, class Swap>
+__device__ void BlockBitonic(int p, const Before &before, const Swap &swap)
+{
+    for (int size = 2; size <= p; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = threadIdx.x; i < p; i += kLargeThreads) {
+                const int j = i ^ stride;
+                if (j > i) {
+                    const bool up = (i & size) == 0;
+                    if (up ? before(j, i) : before(i, j))
+                        swap(i, j);
+                }
+            }
+            __syncthreads();
+        }
+}
+
+__global__ void __launch_bounds__(kLargeThreads) FinalSelectLargeKernel(const StreamArgs a)
+{
+    __shared__ LargeShared sh;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    int q = blockIdx.x;
+    if (a.retry) {
+        if ((unsigned)q >= __ldcg(a.fail_in_count))
+            return;
+        q = __ldcg(a.fail_in + q);
+    }
+    const int k = QueryK(a, q);
+    if (k <= kMaxSmallK)
+        return;  // FinalSelectKernel's query
+    const unsigned appended = __ldcg(a.cand_count + q);
+    // floor: the query's threshold, or the least of the 32 slots (32 m >= K documents reach it)
+    if (warp == 0) {
+        const unsigned m = __reduce_min_sync(kFull, __ldcg(a.tslots + (long long)q * 32 + lane));
+        if (lane == 0) {
+            sh.above = m;
+            sh.sel_count = 0u;
+            sh.eq_count = 0u;
+            sh.total = 0u;
+        }
+    }
+    __syncthreads();
+    const float floor = fmaxf(__uint_as_float(__ldcg(a.threshold + q)), __uint_as_float(sh.above));
+    if ((long long)appended > a.cand_cap) {
+        if (a.fail_out) {
+            // search the query again: its group slots (real documents' scores) stay as the
+            // starting bound; the threshold may hold a guess and is dropped
+            if (tid == 0) {
+                a.threshold[q] = 0u;
+                a.cand_count[q] = 0u;
+                if (a.exact && !a.retry)
+                    a.exact[q] = 0;
+                a.fail_out[atomicAdd(a.fail_out_count, 1u)] = q;
+            }
+            return;
+        }
+        if (tid == 0)
+            atomicOr(a.status, kStatusCandOverflow);
+    }
+    const int n = (int)min((long long)appended, a.cand_cap);
+    const float *cs = a.cand_scores + (long long)q * a.cand_cap;
+    const int *ci = a.cand_ids + (long long)q * a.cand_cap;
+    auto score_key = [&](int i, unsigned *key) -> bool {
+        const float s = __ldcg(cs + i);
+        *key = __float_as_uint(s);
+        return s > 0.0f && s >= floor;
+    };
+    {
+        unsigned c = 0, key;
+        for (int i = tid; i < n; i += kLargeThreads)
+            c += score_key(i, &key);
+        c = __reduce_add_sync(kFull, c);
+        if (lane == 0)
+            atomicAdd(&sh.total, c);
+    }
+    __syncthreads();
+    const unsigned total = sh.total;
+    unsigned kth_key = 0, need = 0;
+    if (total > (unsigned)k)
+        kth_key = RadixSelect31(sh, n, score_key, (unsigned)k, &need);
+    // documents above the K-th key (all of them when no more than K qualify); ties at it apart
+    for (int i = tid; i < n; i += kLargeThreads) {
+        unsigned key;
+        if (!score_key(i, &key))
+            continue;
+        if (total <= (unsigned)k || key > kth_key) {
+            const unsigned at = atomicAdd(&sh.sel_count, 1u);
+            if (at < (unsigned)kLargeMaxK) {  // at most K - 1 by the radix select
+                sh.sel_s[at] = __uint_as_float(key);
+                sh.sel_i[at] = __ldcg(ci + i);
+            }
+        } else if (key == kth_key) {
+            const unsigned at = atomicAdd(&sh.eq_count, 1u);
+            if (at < (unsigned)kLargeEqCap)
+                sh.eq[at] = __ldcg(ci + i);
+        }
+    }
+    __syncthreads();
+    if (total > (unsigned)k) {
+        const unsigned eqn = sh.eq_count;
+        const unsigned base = sh.sel_count;  // k - need
+        if (eqn <= (unsigned)kLargeEqCap) {
+            // the need smallest ids among the ties
+            int p = 1;
+            while (p < (int)eqn)
+                p <<= 1;
+            for (int i = (int)eqn + tid; i < p; i += kLargeThreads)
+                sh.eq[i] = INT_MAX;
+            __syncthreads();
+            BlockBitonic(
+                p, [&](int i, int j) { return sh.eq[i] < sh.eq[j]; },
+                [&](int i, int j) {
+                    const int t = sh.eq[i];
+                    sh.eq[i] = sh.eq[j];
+                    sh.eq[j] = t;
+                });
+            for (unsigned i = tid; i < need && base + i < (unsigned)kLargeMaxK && i < (unsigned)p; i += kLargeThreads) {
+                sh.sel_s[base + i] = __uint_as_float(kth_key);
+                sh.sel_i[base + i] = sh.eq[i];
+            }
+        } else {
+            // too many ties to sort here: the need-th smallest id by a radix select on
+            // 0x7fffffff - id over the tied candidates, then every tie at or below it
+            auto id_key = [&](int i, unsigned *key) -> bool {
+                const float s = __ldcg(cs + i);
+                *key = 0x7fffffffu - (unsigned)__ldcg(ci + i);
+                return __float_as_uint(s) == kth_key && s >= floor;
+            };
+            unsigned rest;
+            const unsigned cut = 0x7fffffffu - RadixSelect31(sh, n, id_key, need, &rest);
+            if (tid == 0)
+                sh.eq_count = 0u;
+            __syncthreads();
+            for (int i = tid; i < n; i += kLargeThreads) {
+                unsigned key;
+                if (id_key(i, &key) && 0x7fffffffu - key <= cut) {
+                    const unsigned at = base + atomicAdd(&sh.eq_count, 1u);
+                    if (at < (unsigned)kLargeMaxK) {
+                        sh.sel_s[at] = __uint_as_float(kth_key);
+                        sh.sel_i[at] = (int)(0x7fffffffu - key);
+                    }
+                }
+            }
+        }
+        if (tid == 0)
+            sh.sel_count = (unsigned)k;
+    }
+    __syncthreads();
+    const int c = (int)min(sh.sel_count, (unsigned)k);
+    int p = 1;
+    while (p < c)
+        p <<= 1;
+    for (int i = c + tid; i < p; i += kLargeThreads) {
+        sh.sel_s[i] = -1.0f;
+        sh.sel_i[i] = INT_MAX;
+    }
+    for (int i = tid; i < kLargeMaxK / 32; i += kLargeThreads)
+        sh.fill[i] = 0u;
+    __syncthreads();
+    BlockBitonic(
+        p, [&](int i, int j) { return Better(sh.sel_s[i], sh.sel_i[i], sh.sel_s[j], sh.sel_i[j]); },
+        [&](int i, int j) {
+            const float ts = sh.sel_s[i];
+            const int ti = sh.sel_i[i];
+            sh.sel_s[i] = sh.sel_s[j];
+            sh.sel_i[i] = sh.sel_i[j];
+            sh.sel_s[j] = ts;
+            sh.sel_i[j] = ti;
+        });
+    float *os = a.out_scores + OutRow(a, q);
+    int *oi = a.out_ids + OutRow(a, q);
+    for (int i = tid; i < c; i += kLargeThreads) {
+        os[i] = sh.sel_s[i];
+        oi[i] = sh.sel_i[i];
+        if (sh.sel_i[i] < k)
+            atomicOr(&sh.fill[sh.sel_i[i] >> 5], 1u << (sh.sel_i[i] & 31));
+    }
+    __syncthreads();
+    if (c < k && tid == 0) {  // zero-score fill, smallest free ids first (all below k)
+        int r = c;
+        for (int d = 0; r < k && d < a.num_docs; ++d)
+            if (!((sh.fill[d >> 5] >> (d & 31)) & 1u)) {
+                os[r] = 0.0f;
+                oi[r] = d;
+                ++r;
+            }
+    }
+    const bool failed = a.exact && !a.retry && !(c == k || !(a.tau[q] > 0.0f));
+    if (tid == 0) {
+        if (a.exact && !a.retry) {
+            a.exact[q] = failed ? 0 : 1;
+            if (failed)
+                a.fail_out[atomicAdd(a.fail_out_count, 1u)] = q;
+        }
+        a.cand_count[q] = 0u;
+        a.threshold[q] = 0u;
+    }
+    if (warp == 0 && !failed)  // a failed query keeps its slots for the retry pass
         a.tslots[(long long)q * 32 + lane] = 0u;
-    }
-}
-
-// Pruned Search: each query's running bound starts at its guess tau[q] (>= 0).
-__global__ void SeedBoundKernel(const StreamArgs a)
-{
-    if (blockIdx.x == 0 && threadIdx.x == 0)
-        *a.fail_count = 0u;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < a.q; q += gridDim.x * blockDim.x) {
-        const float t = a.tau[q];
-        a.threshold[q] = t > 0.0f ? __float_as_uint(t) : 0u;  // NaN or negative: no bound
-    }
-}
-
-// dir_max[r][t] = largest posting score of directory row r's term inside tile t.
-__global__ void BuildDirMaxKernel(const long long *indptr, const float *data, const int *dir_terms, const int *dir,
-                                  long long rows, int tiles, long long stride, float *dir_max)
-{
-    const long long total = rows * (long long)tiles;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const long long r = i / tiles;
-        const int t = (int)(i % tiles);
-        const long long s = indptr[dir_terms[r]];
-        const int *d = dir + r * stride;
-        float m = 0.0f;
-        for (long long p = s + d[t]; p < s + d[t + 1]; ++p)
-            m = fmaxf(m, data[p]);
-        dir_max[i] = m;
-    }
 }
 
 } // namespace bm25k

@@ -29,14 +29,10 @@
 // group, so every query gets tiles early and words that queries share are read
 // from DRAM once and from L2 after.  FinalSelectKernel finishes every query.
 //
-// Pruned Search (a.wbound set): the running bound starts at the query's guess
-// tau, and the producer adds, per tile of a claim, the query words' per-tile
-// score maxima in query-word order -- an FP32 upper bound of every document's
-// sum in that tile, since rounded addition is monotone in both operands -- and
-// drops the tiles whose bound is below the claim's running bound (a whole
-// claim when all eight are).  A dropped tile holds no document scoring at or
-// above the bound, so it holds none of the top K whenever K documents reach
-// tau; FinalSelectKernel reports whether they did.
+// A retry pass (a.retry) covers only the queries on the fail list: those whose
+// pruned pass fell short of K documents, or whose K > 32 candidate buffer
+// overflowed (their running bound then starts at the final bound of the first
+// pass).
 #pragma once
 #include "stream_kernel.cuh"
 
@@ -84,17 +80,12 @@ inline size_t TileGroupSmem(int stages, int chunk, int tile_docs)
            sizeof(WgShared);
 }
 
-// Top-k of a warp's row (32 * kVec float4, lane-interleaved: element e of a lane
-// is document base_id + 4 * (lane + 32 * (e / 4)) + e % 4) among scores >= thr
-// and > 0, sorted best first into ws.sel with global ids.  The row is read into
-// registers and cleared in one pass.  Returns the count; *kth receives the
-// row's k-th score when it is known exactly (k candidates, none filtered below
-// it), else 0.
+// Moves a warp's row (32 * kVec float4, lane-interleaved: element e of a lane is
+// document base_id + 4 * (lane + 32 * (e / 4)) + e % 4) into registers x and
+// clears it, in one pass.
 template <int kVec>
-__device__ __forceinline__ int WarpRowSelect(WarpSel &ws, float4 *reg4, float thr, int k, int base_id, int lane,
-                                             float *kth)
+__device__ __forceinline__ void WarpTakeRow(float4 *reg4, int lane, float *x)
 {
-    float x[4 * kVec];
 #pragma unroll
     for (int j = 0; j < kVec; ++j) {
         const float4 v = reg4[lane + 32 * j];
@@ -106,8 +97,19 @@ __device__ __forceinline__ int WarpRowSelect(WarpSel &ws, float4 *reg4, float th
 #pragma unroll
     for (int j = 0; j < kVec; ++j)
         reg4[lane + 32 * j] = make_float4(0.f, 0.f, 0.f, 0.f);
-    // "x >= thr and x > 0" is "x >= max(thr, least positive float)" for thr >= 0
-    constexpr float kLeastPositive = 1.40129846e-45f;
+}
+
+// "x >= thr and x > 0" is "x >= max(thr, least positive float)" for thr >= 0
+constexpr float kLeastPositive = 1.40129846e-45f;
+
+// Top-k (k <= 32) of a warp's row held in registers (layout of WarpTakeRow) among
+// scores >= thr and > 0, sorted best first into ws.sel with global ids.  Returns
+// the count; *kth receives the row's k-th score when it is known exactly (k
+// candidates, none filtered below it), else 0.
+template <int kVec>
+__device__ __forceinline__ int WarpSelectRegs(WarpSel &ws, const float *x, float thr, int k, int base_id, int lane,
+                                              float *kth)
+{
     float tmax = 0.0f;
 #pragma unroll
     for (int e = 0; e < 4 * kVec; ++e)
@@ -185,6 +187,99 @@ __device__ __forceinline__ int WarpRowSelect(WarpSel &ws, float4 *reg4, float th
     return n;
 }
 
+// WarpTakeRow + WarpSelectRegs.
+template <int kVec>
+__device__ __forceinline__ int WarpRowSelect(WarpSel &ws, float4 *reg4, float thr, int k, int base_id, int lane,
+                                             float *kth)
+{
+    float x[4 * kVec];
+    WarpTakeRow<kVec>(reg4, lane, x);
+    return WarpSelectRegs<kVec>(ws, x, thr, k, base_id, lane, kth);
+}
+
+// End of a tile: takes the warp's row (clearing it) and appends its documents at or
+// above the bound `thr` to query q's candidate buffer -- the top K for K <= 32, every
+// one for K > 32 -- and raises the query's threshold and group slots.  Returns status
+// bits.  Every lane of the warp calls.
+template <int kTile>
+__device__ __forceinline__ unsigned TileSelectAppend(const StreamArgs &a, WarpSel &ws, float4 *row4, float thr, int q,
+                                                     int tile, int lane)
+{
+    const int base_doc = tile * kTile;
+    unsigned bad = 0;
+    const int k = QueryK(a, q);
+    if (k <= 32) {
+        float kth;
+        const int sel = WarpRowSelect<kTile / 128>(ws, row4, thr, k, base_doc, lane, &kth);
+        if (sel > 0) {
+            if (!(ws.sel_s[0] <= FLT_MAX))
+                bad |= kStatusOverflow;  // an overflowed sum would be the tile's best score
+            unsigned at = 0;
+            if (lane == 0) {
+                at = atomicAdd(a.cand_count + q, (unsigned)sel);
+                if (kth > thr)
+                    atomicMax(a.threshold + q, __float_as_uint(kth));
+                atomicMax(a.tslots + (long long)q * 32 + tile % k, __float_as_uint(ws.sel_s[0]));
+            }
+            at = __shfl_sync(kFull, at, 0);
+            if (lane < sel) {
+                if ((long long)at + lane < a.cand_cap) {
+                    const long long o = (long long)q * a.cand_cap + at + lane;
+                    a.cand_scores[o] = ws.sel_s[lane];
+                    a.cand_ids[o] = ws.sel_i[lane];
+                } else {
+                    bad |= kStatusCandOverflow;
+                }
+            }
+        }
+    } else {
+        // K > 32: slot tile % 32 takes the tile's m-th best (m = ceil(K / 32)), so the 32
+        // slots stand for 32 m >= K documents; every document at or above the bound is
+        // appended (the final select ranks them; a query whose buffer overflows is
+        // searched again from its final bound)
+        constexpr int kElems = kTile / 32;
+        float x[kElems];
+        WarpTakeRow<kTile / 128>(row4, lane, x);
+        const int m = (k + 31) >> 5;
+        float mth;
+        const int sel = WarpSelectRegs<kTile / 128>(ws, x, thr, m, base_doc, lane, &mth);
+        if (sel > 0 && !(ws.sel_s[0] <= FLT_MAX))
+            bad |= kStatusOverflow;
+        if (sel == m && lane == 0)
+            atomicMax(a.tslots + (long long)q * 32 + tile % 32, __float_as_uint(mth));
+        const float tau = fmaxf(thr, kLeastPositive);
+        int pass = 0;
+#pragma unroll
+        for (int e = 0; e < kElems; ++e)
+            pass += x[e] >= tau;
+        const int total = __reduce_add_sync(kFull, pass);
+        if (total) {
+            int at = pass;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(kFull, at, o);
+                if (lane >= o)
+                    at += v;
+            }
+            unsigned base = 0;
+            if (lane == 0)
+                base = atomicAdd(a.cand_count + q, (unsigned)total);
+            long long o = (long long)__shfl_sync(kFull, base, 0) + at - pass;
+#pragma unroll
+            for (int e = 0; e < kElems; ++e)
+                if (x[e] >= tau) {
+                    if (o < a.cand_cap) {
+                        const long long g = (long long)q * a.cand_cap + o;
+                        a.cand_scores[g] = x[e];
+                        a.cand_ids[g] = base_doc + 4 * (lane + 32 * (e >> 2)) + (e & 3);
+                    }
+                    ++o;
+                }
+        }
+    }
+    return bad;
+}
+
 // A claim as the producer holds it: uniform fields plus one plan entry pair per lane.
 struct WgClaim {
     bool valid;
@@ -193,14 +288,12 @@ struct WgClaim {
     unsigned thr_bits;   // the query's threshold
     unsigned slot_bits;  // lane g < k: group slot g (others: all ones)
     int2 p0, p1;         // lane l: word l / 8 (p0) and 4 + l / 8 (p1) in tile tile0 + l % 8; .x = b, .y = e
-    float b0, b1;        // pruned Search: the same words' score bounds in the same tiles
 };
 
-// Range of word s (>= kWgPlanWords, warp-uniform) in tile j of the claim, from the plan;
-// empty for a tile outside the kept set `keep` (bit j).
-__device__ __forceinline__ int2 WgFarRange(const StreamArgs &a, const WgClaim &c, int s, int j, unsigned keep)
+// Range of word s (>= kWgPlanWords, warp-uniform) in tile j of the claim, from the plan.
+__device__ __forceinline__ int2 WgFarRange(const StreamArgs &a, const WgClaim &c, int s, int j)
 {
-    if (c.tile0 + j >= a.tiles || !((keep >> j) & 1u))
+    if (c.tile0 + j >= a.tiles)
         return make_int2(0, 0);
     const PlanEntry pe = a.plan[(c.qb + s) * a.tiles + c.tile0 + j];
     return make_int2((int)pe.b, (int)pe.e);
@@ -232,7 +325,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
     volatile int *abort = &sh.abort;
     const unsigned groups = (unsigned)((a.tiles + kWgWarps - 1) / kWgWarps);
     // a retry pass covers only the queries on the fail list (possibly none)
-    const unsigned nq = a.retry ? __ldcg(a.fail_count) : (unsigned)a.q;
+    const unsigned nq = a.retry ? __ldcg(a.fail_in_count) : (unsigned)a.q;
     const unsigned claims = nq * groups;
 
     if (warp == kWgWarps) {
@@ -242,7 +335,8 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
         unsigned wraps = 0;        // times the ring has wrapped
         unsigned bad = 0;
         bool dead = false;
-        unsigned long long n_claims = 0, n_dropped = 0, n_tiles = 0, n_copied = 0;  // lane 0's counts
+        unsigned n_claims = 0, n_tiles = 0;  // lane 0's counts
+        unsigned long long n_copied = 0;
         // Waits until stage pst is free (its previous use released).
         auto claim_stage = [&]() -> bool {
             int ok = 1;
@@ -266,13 +360,12 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
             w.valid = c < claims;
             w.q = w.valid ? (int)(c % nq) : 0;
             if (a.retry && w.valid)
-                w.q = __ldcg(a.fail_list + w.q);
+                w.q = __ldcg(a.fail_in + w.q);
             w.tile0 = w.valid ? (int)(c / nq) * kWgWarps : 0;
             w.n = 0;
             w.qb = w.qe = 0;
             w.p0 = make_int2(0, 0);
             w.p1 = make_int2(0, 0);
-            w.b0 = w.b1 = 0.0f;
             w.thr_bits = 0u;
             w.slot_bits = 0xffffffffu;
         };
@@ -296,17 +389,13 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
             if (tile_ok && s0 < w.n) {
                 const PlanEntry pe = a.plan[(w.qb + s0) * a.tiles + w.tile0 + j];
                 w.p0 = make_int2((int)pe.b, (int)pe.e);
-                if (a.wbound)
-                    w.b0 = a.wbound[(w.qb + s0) * a.tiles + w.tile0 + j];
             }
             if (tile_ok && s0 + 4 < w.n) {
                 const PlanEntry pe = a.plan[(w.qb + s0 + 4) * a.tiles + w.tile0 + j];
                 w.p1 = make_int2((int)pe.b, (int)pe.e);
-                if (a.wbound)
-                    w.b1 = a.wbound[(w.qb + s0 + 4) * a.tiles + w.tile0 + j];
             }
             w.thr_bits = __ldcg(a.threshold + w.q);
-            if (lane < a.k)
+            if (lane < QueryK(a, w.q))
                 w.slot_bits = __ldcg(a.tslots + (long long)w.q * 32 + lane);
         };
         auto take_claim = [&]() -> unsigned {
@@ -333,33 +422,8 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
 
             const float thr =
                 fmaxf(__uint_as_float(cur.thr_bits), __uint_as_float(__reduce_min_sync(kFull, cur.slot_bits)));
-            unsigned keep = 0xffu;
             ++n_claims;
-            if (a.wbound) {
-                // lane l bounds tile l % 8: the words' tile maxima added in query-word order
-                const int j = lane & 7;
-                float bound = 0.0f;
-                for (int s = 0; s < cur.n; ++s) {
-                    float b;
-                    if (s < 4)
-                        b = __shfl_sync(kFull, cur.b0, s * 8 + j);
-                    else if (s < kWgPlanWords)
-                        b = __shfl_sync(kFull, cur.b1, (s - 4) * 8 + j);
-                    else
-                        b = cur.tile0 + j < a.tiles ? a.wbound[(cur.qb + s) * a.tiles + cur.tile0 + j] : 0.0f;
-                    bound = __fadd_rn(bound, b);
-                }
-                keep = __ballot_sync(kFull, !(bound < thr)) & 0xffu;
-                if (!((keep >> j) & 1u)) {
-                    cur.p0 = make_int2(0, 0);
-                    cur.p1 = make_int2(0, 0);
-                }
-                if (!keep) {
-                    ++n_dropped;
-                    continue;  // no tile of the claim can reach the bound
-                }
-            }
-            n_tiles += __popc(keep & (a.tiles - cur.tile0 >= kWgWarps ? 0xffu : (1u << (a.tiles - cur.tile0)) - 1u));
+            n_tiles += (unsigned)min(kWgWarps, a.tiles - cur.tile0);
             // each word's run over the group, reduced within its 8 lanes
             const bool ne0 = cur.p0.x < cur.p0.y, ne1 = cur.p1.x < cur.p1.y;
             int lo0 = ne0 ? cur.p0.x : 0x7fffffff, hi0 = ne0 ? cur.p0.y : -1;
@@ -376,7 +440,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
             int last_word = -1;
             for (int s = cur.n - 1; s >= kWgPlanWords && last_word < 0; --s)
                 for (int j = 0; j < kWgWarps; ++j) {
-                    const int2 r = WgFarRange(a, cur, s, j, keep);
+                    const int2 r = WgFarRange(a, cur, s, j);
                     if (r.x < r.y) {
                         last_word = s;
                         break;
@@ -400,7 +464,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
                     lo = 0x7fffffff;
                     hi = -1;
                     for (int j = 0; j < kWgWarps; ++j) {
-                        const int2 r = WgFarRange(a, cur, s, j, keep);
+                        const int2 r = WgFarRange(a, cur, s, j);
                         if (r.x < r.y) {
                             lo = min(lo, r.x);
                             hi = max(hi, r.y);
@@ -423,7 +487,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
                         if ((lane >> 3) == (s & 3))
                             m.be[lane & 7] = s < 4 ? cur.p0 : cur.p1;
                     } else if (lane < kWgWarps) {
-                        m.be[lane] = WgFarRange(a, cur, s, lane, keep);
+                        m.be[lane] = WgFarRange(a, cur, s, lane);
                     }
                     if (lane == 0) {
                         m.span = make_int4((int)c0, (int)(c1 - c0), cur.q, cur.tile0);
@@ -461,10 +525,9 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
             if (bad)
                 atomicOr(a.status, bad);
             if (a.stats) {
-                atomicAdd(a.stats, n_claims);
-                atomicAdd(a.stats + 1, n_dropped);
-                atomicAdd(a.stats + 2, n_tiles);
-                atomicAdd(a.stats + 3, n_copied);
+                atomicAdd(a.stats + kStatClaims, (unsigned long long)n_claims);
+                atomicAdd(a.stats + kStatTilesScanned, (unsigned long long)n_tiles);
+                atomicAdd(a.stats + kStatPostingsCopied, n_copied);
             }
             // the last producer to run dry resets the work counter for the next Search
             const unsigned d = atomicAdd(&a.ctrl->done, 1u);
@@ -555,29 +618,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
         touched = false;
 
         // ---- end of the claim: select this warp's tile ----
-        float kth;
-        const int sel = WarpRowSelect<kTile / 128>(ws, row4, thr, a.k, base_doc, lane, &kth);
-        if (sel > 0) {
-            if (!(ws.sel_s[0] <= FLT_MAX))
-                bad |= kStatusOverflow;  // an overflowed sum would be the tile's best score
-            unsigned at = 0;
-            if (lane == 0) {
-                at = atomicAdd(a.cand_count + q, (unsigned)sel);
-                if (kth > thr)
-                    atomicMax(a.threshold + q, __float_as_uint(kth));
-                atomicMax(a.tslots + (long long)q * 32 + tile % a.k, __float_as_uint(ws.sel_s[0]));
-            }
-            at = __shfl_sync(kFull, at, 0);
-            if (lane < sel) {
-                if ((long long)at + lane < a.cand_cap) {
-                    const long long o = (long long)q * a.cand_cap + at + lane;
-                    a.cand_scores[o] = ws.sel_s[lane];
-                    a.cand_ids[o] = ws.sel_i[lane];
-                } else {
-                    bad |= kStatusCandOverflow;
-                }
-            }
-        }
+        bad |= TileSelectAppend<kTile>(a, ws, row4, thr, q, tile, lane);
         __syncwarp();
     }
     bad = __reduce_or_sync(kFull, bad);

@@ -148,11 +148,12 @@ def predict(params, features, device='cuda:0'):
 
 
 def bounds(pred, safe, margin):
-    """The starting bounds the device computes: max(exp(y - margin), safe), 0 where safe is 0."""
+    """The starting bounds the device computes: max(exp(y - margin), safe), 0 where safe is -1
+    (the query's words hold fewer than K postings)."""
     pred = np.asarray(pred, dtype=np.float32)
     safe = np.asarray(safe, dtype=np.float32)
     tau = np.maximum(np.exp(pred - np.float32(margin)).astype(np.float32), safe)
-    return np.where(safe > 0, tau, np.float32(0)).astype(np.float32)
+    return np.where(safe < 0, np.float32(0), tau).astype(np.float32)
 
 
 def fallback_rate(pred, safe, kth, margin):
@@ -188,11 +189,10 @@ def fit(session, index_offsets, *, queries=200_000, ks=(10, 32), lo=2, hi=10, se
         safes.append(s)
         kths.append(t)
     f, s, t = np.concatenate(feats), np.concatenate(safes), np.concatenate(kths)
-    use = t > 0  # queries with fewer than K matching documents have no K-th score to learn
-    f, s, t = f[use], s[use], t[use]
     order = np.random.default_rng(seed).permutation(t.size)
     nval = max(1, int(t.size * val_share))
     val, tr = order[:nval], order[nval:]
+    tr = tr[t[tr] > 0]  # a query with fewer than K matching documents has no K-th score to learn
     params, loss = train(f[tr], np.log(t[tr]), steps=steps, batch=batch, lr=lr, over_weight=over_weight,
                          seed=seed, device=device)
     pred = predict(params, f[val], device)
@@ -201,7 +201,7 @@ def fit(session, index_offsets, *, queries=200_000, ks=(10, 32), lo=2, hi=10, se
         'train_queries': int(tr.size), 'val_queries': int(val.size), 'first_loss': float(loss[0]),
         'last_loss': float(np.mean(loss[-50:])), 'margin': float(margin),
         'val_fallback': fallback_rate(pred, s[val], t[val], margin),
-        'val_safe_share_of_kth': float(np.mean(s[val] / t[val])),
-        'val_tau_share_of_kth': float(np.mean(bounds(pred, s[val], margin) / t[val])),
+        'val_safe_share_of_kth': float(np.mean(np.maximum(s[val], 0)[t[val] > 0] / t[val][t[val] > 0])),
+        'val_tau_share_of_kth': float(np.mean(bounds(pred, s[val], margin)[t[val] > 0] / t[val][t[val] > 0])),
     }
     return ThresholdModel(params, float(margin), report)

@@ -70,7 +70,7 @@ def pack_queries(queries):
 
 
 def _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes, stream,
-             kernel=4, ring_stages=0, ring_chunk=0, prune=False):
+             kernel=4, ring_stages=0, ring_chunk=0, prune=False, candidate_capacity=0):
     o = n.Options()
     n.engine_library().bm25_default_options(ctypes.byref(o))
     o.device_id = device_id
@@ -85,6 +85,7 @@ def _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_f
     o.ring_stages = ring_stages
     o.ring_chunk = ring_chunk
     o.prune = int(bool(prune))
+    o.candidate_capacity = candidate_capacity
     return o
 
 
@@ -100,7 +101,7 @@ class Bm25Session:
     @classmethod
     def from_csc(cls, indptr, indices, data, num_docs, *, query_capacity=8, word_capacity=24, max_k=10,
                  device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0, stream=None, kernel=4, ring_stages=0,
-                 ring_chunk=0, prune=False):
+                 ring_chunk=0, prune=False, candidate_capacity=0):
         """Eager CSC index (bm25s layout): indptr int64 [V+1], indices int32 [M], data float32 [M]."""
         lib = n.engine_library()
         indptr = np.ascontiguousarray(indptr, dtype=np.int64)
@@ -110,7 +111,7 @@ class Bm25Session:
         if vocab < 1 or indices.size != indptr[-1] or data.size != indices.size:
             raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'Index dimensions/endpoints differ')
         o = _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes,
-                     stream, kernel, ring_stages, ring_chunk, prune)
+                     stream, kernel, ring_stages, ring_chunk, prune, candidate_capacity)
         h = c_void_p()
         status = lib.bm25_create(n.ptr(indptr, c_int64), n.ptr(indices, c_int32), n.ptr(data, c_float), vocab,
                                  int(num_docs), ctypes.byref(o), ctypes.byref(h))
@@ -120,7 +121,7 @@ class Bm25Session:
     @classmethod
     def from_lazy(cls, term_offsets, posting_doc_ids, posting_tf, doc_norm, idf, *, k1=1.2, query_capacity=8,
                   word_capacity=24, max_k=10, device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0,
-                  stream=None, kernel=4, ring_stages=0, ring_chunk=0, prune=False):
+                  stream=None, kernel=4, ring_stages=0, ring_chunk=0, prune=False, candidate_capacity=0):
         """The reference's resident index (common/bm25/index_data.h:9-42); posting scores built on the GPU."""
         lib = n.engine_library()
         offsets = np.ascontiguousarray(term_offsets, dtype=np.int64)
@@ -132,7 +133,7 @@ class Bm25Session:
         if offsets.size != vocab + 1 or docs.size != tf.size or offsets[-1] != docs.size:
             raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'Index dimensions/endpoints differ')
         o = _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes,
-                     stream, kernel, ring_stages, ring_chunk, prune)
+                     stream, kernel, ring_stages, ring_chunk, prune, candidate_capacity)
         h = c_void_p()
         status = lib.bm25_create_lazy(n.ptr(offsets, c_int64), n.ptr(docs, c_int32), n.ptr(tf, c_float),
                                       n.ptr(norm, c_float), n.ptr(idf, c_float), vocab, norm.size, float(k1),
@@ -194,6 +195,46 @@ class Bm25Session:
                                                      c_void_p(ids_ptr), c_void_p(exact_ptr), c_void_p(stream_ptr))
         _raise(self._lib, status, self._handle)
 
+    def search_batch(self, queries, ks, *, learned=False):
+        """A batch with a K per query (one graph replay).  Returns (scores, ids, koff[, exact]):
+        query i's results are scores[koff[i]:koff[i + 1]] and ids[...] (packed rows); exact is
+        returned when learned is set (learned bounds, as search_learned)."""
+        if isinstance(queries, tuple):
+            offsets = np.ascontiguousarray(queries[0], dtype=np.int64)
+            words = np.ascontiguousarray(queries[1], dtype=np.int32)
+        else:
+            offsets, words = pack_queries(queries)
+        q = offsets.size - 1
+        ks = np.ascontiguousarray(ks, dtype=np.int32)
+        if ks.shape != (q,):
+            raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'ks must hold one K per query')
+        koff = np.zeros(q + 1, dtype=np.int64)
+        np.cumsum(ks, out=koff[1:])
+        scores = np.empty(int(koff[-1]), dtype=np.float32)
+        ids = np.empty(int(koff[-1]), dtype=np.int32)
+        if words.size == 0:
+            words = np.zeros(1, dtype=np.int32)
+        if learned:
+            exact = np.empty(q, dtype=np.int32)
+            status = self._lib.bm25_search_batch_learned(self._handle, n.ptr(offsets, c_int64), n.ptr(words, c_int32),
+                                                         n.ptr(ks, c_int32), q, n.ptr(scores, c_float),
+                                                         n.ptr(ids, c_int32), n.ptr(exact, c_int32))
+            _raise(self._lib, status, self._handle)
+            return scores, ids, koff, exact
+        status = self._lib.bm25_search_batch(self._handle, n.ptr(offsets, c_int64), n.ptr(words, c_int32),
+                                             n.ptr(ks, c_int32), q, n.ptr(scores, c_float), n.ptr(ids, c_int32))
+        _raise(self._lib, status, self._handle)
+        return scores, ids, koff
+
+    def search_batch_device(self, qoffsets_ptr, words_ptr, ks_ptr, kout_ptr, q, kmax, scores_ptr, ids_ptr,
+                            exact_ptr=None, learned=False, stream_ptr=None):
+        """Device-resident batch with a K per query (see bm25_search_batch_device); asynchronous."""
+        status = self._lib.bm25_search_batch_device(self._handle, c_void_p(qoffsets_ptr), c_void_p(words_ptr),
+                                                    c_void_p(ks_ptr), c_void_p(kout_ptr), q, kmax, int(bool(learned)),
+                                                    c_void_p(scores_ptr), c_void_p(ids_ptr), c_void_p(exact_ptr),
+                                                    c_void_p(stream_ptr))
+        _raise(self._lib, status, self._handle)
+
     def set_threshold_model(self, model):
         """Threshold model of the learned bounds (a ThresholdModel, or None for the safe bounds alone)."""
         if model is None:
@@ -236,10 +277,12 @@ class Bm25Session:
         _raise(self._lib, status, self._handle)
 
     def search_stats(self, reset=True):
-        """Tile-group counters since the last reset: claims, claims dropped, tiles scanned, postings copied."""
-        out = (ctypes.c_uint64 * 4)()
+        """Search counters since the last reset (tile-group kernel: claims, tiles scanned, postings
+        copied; block-max pruned pass: tiles scored, blocks kept, postings read)."""
+        out = (ctypes.c_uint64 * 6)()
         _raise(self._lib, self._lib.bm25_search_stats(self._handle, out, int(bool(reset))), self._handle)
-        return {'claims': out[0], 'claims_dropped': out[1], 'tiles_scanned': out[2], 'postings_copied': out[3]}
+        names = ('claims', 'tiles_scanned', 'postings_copied', 'block_tiles', 'blocks_kept', 'postings_read')
+        return dict(zip(names, out))
 
     def search_device(self, qoffsets_ptr, words_ptr, q, k, scores_ptr, ids_ptr, stream_ptr=None):
         """Device-resident Search on raw device pointers (e.g. torch ``data_ptr()``); asynchronous."""

@@ -51,8 +51,10 @@ typedef struct bm25_options {
     int32_t ring_stages;     /* posting-ring depth of the ring kernels (0 and 4), 2..8; 0 = automatic */
     int32_t ring_chunk;      /* postings per ring stage of the tile-group kernel, 512..4096, a multiple of 4;
                                 0 = automatic */
-    int32_t prune;           /* nonzero: prepare per-(word, tile) score bounds for bm25_search_pruned_device
-                                (tile-group kernel only; costs one float per directory row and tile) */
+    int32_t prune;           /* nonzero: build the 128-document block-max index and the term statistics of
+                                the pruned and learned Searches (tile-group kernel only) */
+    int64_t candidate_capacity; /* max_k > 32: candidates kept per query (0 = automatic, 256 K and at least
+                                   2^18); a query that overflows it is searched again from its final bound */
 } bm25_options;
 
 /* Search kernels (bm25_options.kernel):
@@ -139,6 +141,29 @@ int bm25_search_pruned(bm25_handle *handle, const int64_t *qoffsets, const int32
                        int64_t q, int32_t k, float *out_scores, int32_t *out_ids, int32_t *out_exact);
 
 /*
+ * A batch with a K per query (no counterpart in the reference; the tile-group
+ * kernel): ks int32 [q], each in [1, min(max_k, N)].  Results are packed by
+ * query: query i's ks[i] (score, id) pairs start at ks[0] + ... + ks[i-1].
+ * One graph replay covers the whole batch.
+ */
+int bm25_search_batch(bm25_handle *handle, const int64_t *qoffsets, const int32_t *words, const int32_t *ks,
+                      int64_t q, float *out_scores, int32_t *out_ids);
+
+/* bm25_search_batch with the learned bounds; out_exact int32 [q] as bm25_search_pruned. */
+int bm25_search_batch_learned(bm25_handle *handle, const int64_t *qoffsets, const int32_t *words, const int32_t *ks,
+                              int64_t q, float *out_scores, int32_t *out_ids, int32_t *out_exact);
+
+/*
+ * Device-resident batch with a K per query: ks int32 [q] and kout int64 [q] (query
+ * i's first output slot) on the device; kmax (host) at least every ks[i]; the
+ * output buffers hold kout[i] + ks[i] entries for every i.  learned != 0: learned
+ * bounds and out_exact int32 [q].  Asynchronous on stream.
+ */
+int bm25_search_batch_device(bm25_handle *handle, const int64_t *qoffsets, const int32_t *words, const int32_t *ks,
+                             const int64_t *kout, int64_t q, int32_t kmax, int32_t learned, float *out_scores,
+                             int32_t *out_ids, int32_t *out_exact, void *stream);
+
+/*
  * Learned starting bounds.  A prune session keeps, per term, its 32 largest
  * posting scores and its mean posting score (computed on the device at
  * creation).  From them each query gets 32 features and a safe bound (the
@@ -162,10 +187,11 @@ int bm25_search_learned_device(bm25_handle *handle, const int64_t *qoffsets, con
                                int32_t k, float *out_scores, int32_t *out_ids, int32_t *out_exact, void *stream);
 
 /*
- * Tile-group kernel counters summed over Searches since the last reset (waits for
- * the handle's work): out[0] claims (query x 8-tile groups) taken, out[1] claims
- * dropped whole by their bounds, out[2] tiles scanned, out[3] postings copied
- * from HBM into the staging rings.
+ * Search counters summed over Searches since the last reset (waits for the
+ * handle's work), out[6]: tile-group kernel -- [0] claims (query x 8-tile
+ * groups), [1] tiles scanned, [2] postings copied from HBM into the staging
+ * rings; block-max pruned pass -- [3] tiles scored, [4] 128-document blocks
+ * kept, [5] postings read.
  */
 int bm25_search_stats(bm25_handle *handle, uint64_t *out, int32_t reset);
 

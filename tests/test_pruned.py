@@ -1,4 +1,4 @@
-"""Pruned Search (tile bounds + a starting bound per query) against the oracle.
+"""Pruned Search (128-document block bounds + a starting bound per query) against the oracle.
 
 Every row must equal the oracle's top-K bit for bit, and the exactness flag is
 predictable from the oracle's full score rows: 1 exactly when at least K
@@ -12,32 +12,33 @@ import pytest
 from helpers import assert_same_topk, mixed_queries, pack
 
 
-def tile_bounds(indptr, indices, data, words, tile_docs, tiles):
-    """Per query word and tile: the largest posting score of the word in the tile (0 if none)."""
-    out = np.zeros((len(words), tiles), dtype=np.float32)
+def block_bounds(indptr, indices, data, words, block_docs, blocks):
+    """Per query word and block: the largest posting score of the word in the block (0 if none)."""
+    out = np.zeros((len(words), blocks), dtype=np.float32)
     vocab = indptr.size - 1
     for w, term in enumerate(words):
         if 0 <= term < vocab:
             s, e = indptr[term], indptr[term + 1]
-            np.maximum.at(out[w], indices[s:e] // tile_docs, np.maximum(data[s:e], 0))
+            np.maximum.at(out[w], indices[s:e] // block_docs, np.maximum(data[s:e], 0))
     return out
 
 
-def test_tile_bound_covers_every_document(pkg, oracle_mod):
-    """FP32 sums of per-tile maxima in query-word order bound every document's FP32 sum in the tile."""
+@pytest.mark.parametrize('block_docs', [128, 1024])
+def test_block_bound_covers_every_document(pkg, oracle_mod, block_docs):
+    """FP32 sums of per-block maxima in query-word order bound every document's FP32 sum in the block."""
     spec = pkg.CorpusSpec(docs=20_000, vocab=3_000, seed=5, k1=1.2)
     index = pkg.synthetic_index(spec)
     data = oracle_mod.contributions(index, spec.k1)
     rows = mixed_queries(index.vocab, np.random.default_rng(1), 24, 1, 12, oov=True)
     offsets, words = pack(rows)
     _, _, full = oracle_mod.search(index.offsets, index.docs, data, index.num_docs, offsets, words, 10, full=True)
-    tile_docs, tiles = 1024, (index.num_docs + 1023) // 1024
+    blocks = (index.num_docs + block_docs - 1) // block_docs
     for q in range(len(rows)):
-        wb = tile_bounds(index.offsets, index.docs, data, words[offsets[q]:offsets[q + 1]], tile_docs, tiles)
-        bound = np.zeros(tiles, dtype=np.float32)
+        wb = block_bounds(index.offsets, index.docs, data, words[offsets[q]:offsets[q + 1]], block_docs, blocks)
+        bound = np.zeros(blocks, dtype=np.float32)
         for b in wb:  # query-word order, FP32 rounding at every step
             bound = (bound + b).astype(np.float32)
-        per_doc = np.repeat(bound, tile_docs)[:index.num_docs]
+        per_doc = np.repeat(bound, block_docs)[:index.num_docs]
         assert np.all(full[q] <= per_doc)
 
 
