@@ -5,7 +5,7 @@ missing the import fails loudly -- there is no CPU or Python fallback.
 """
 
 import ctypes
-from ctypes import POINTER, c_char_p, c_float, c_int, c_int32, c_int64, c_size_t, c_uint32, c_void_p
+from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_int32, c_int64, c_size_t, c_uint32, c_uint64, c_void_p
 from pathlib import Path
 
 PACKAGE = Path(__file__).resolve().parent
@@ -16,6 +16,16 @@ BM25_OK = 0
 BM25_ERR_INVALID_PARAM = 1
 BM25_ERR_ILLEGAL_OPERATION = 2
 BM25_ERR_INNER_ERROR = 3
+
+
+class ServerOptions(ctypes.Structure):
+    _fields_ = [
+        ('max_batch', c_int32),
+        ('learned', c_int32),
+        ('max_wait_us', c_int32),
+        ('reserved', c_int32),
+        ('candidate_budget', c_int64),
+    ]
 
 
 class Options(ctypes.Structure):
@@ -56,6 +66,10 @@ class Info(ctypes.Structure):
         ('grid', c_int32),
         ('smem_bytes', c_int32),
         ('ring_chunk', c_int32),
+        ('query_capacity', c_int32),
+        ('word_capacity', c_int32),
+        ('max_k', c_int32),
+        ('prune', c_int32),
     ]
 
 
@@ -85,6 +99,20 @@ SIGNATURES = {
                                           c_void_p]),
     'bm25_search_batch_device': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_int32,
                                          c_void_p, c_void_p, c_void_p, c_void_p]),
+    'bm25_merge_topk': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_int32, c_int64, c_int32,
+                                c_void_p, c_void_p, c_void_p]),
+    'bm25_default_server_options': (None, [c_void_p]),
+    'bm25_server_create': (c_int, [c_void_p, c_void_p, c_void_p]),
+    'bm25_server_submit': (c_int, [c_void_p, c_void_p, c_int32, c_int32, c_void_p]),
+    'bm25_server_wait': (c_int, [c_void_p, c_uint64, c_void_p, c_void_p, c_void_p, c_void_p]),
+    'bm25_server_stats': (c_int, [c_void_p, c_void_p, c_void_p]),
+    'bm25_server_destroy': (c_int, [c_void_p]),
+    'bm25_server_last_error': (c_int, [c_void_p, c_size_t]),
+    'bm25_serve_poisson': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_double, c_int64,
+                                   c_uint64, c_void_p, c_void_p, c_void_p]),
+    'bm25_build_index': (c_int, [c_void_p, c_void_p, c_int64, c_int64, c_double, c_double, c_int32, c_void_p,
+                                 c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    'bm25_build_last_error': (c_int, [c_void_p, c_size_t]),
     'bm25_set_threshold_model': (c_int, [c_void_p, c_void_p, c_float]),
     'bm25_query_features_device': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p,
                                            c_void_p]),

@@ -174,3 +174,31 @@ def write_bm25s_dir(indptr, indices, data, num_docs, path, k1=1.5, b=0.75):
     np.save(path / 'indptr.csc.index.npy', np.ascontiguousarray(indptr, dtype=np.int64))
     (path / 'params.index.json').write_text(json.dumps({'k1': k1, 'b': b, 'method': 'lucene', 'num_docs': int(num_docs)},
                                                        indent=4))
+
+
+def build_index(doc_offsets, tokens, vocab, k1=1.2, b=0.75, device_id=0):
+    """The reference's lazy index from documents given as token ids, built on the GPU
+    (bm25_build_index: key sort and run-length counts on the device, idf and norms in double
+    on the host, as standalone/large_corpus.py:95-190 does in Python)."""
+    lib = n.engine_library()
+    doc_offsets = np.ascontiguousarray(doc_offsets, dtype=np.int64)
+    tokens = np.ascontiguousarray(tokens, dtype=np.int32)
+    num_docs = doc_offsets.size - 1
+    cap = max(1, int(doc_offsets[-1]))
+    offsets = np.empty(vocab + 1, dtype=np.int64)
+    docs = np.empty(cap, dtype=np.int32)
+    tf = np.empty(cap, dtype=np.float32)
+    norm = np.empty(num_docs, dtype=np.float32)
+    idf = np.empty(vocab, dtype=np.float32)
+    m = ctypes.c_int64(0)
+    status = lib.bm25_build_index(n.ptr(doc_offsets, c_int64), n.ptr(tokens, c_int32) if tokens.size else None,
+                                  num_docs, vocab, ctypes.c_double(k1), ctypes.c_double(b), device_id,
+                                  n.ptr(offsets, c_int64), n.ptr(docs, c_int32), n.ptr(tf, c_float),
+                                  n.ptr(norm, c_float), n.ptr(idf, c_float), ctypes.byref(m))
+    if status != n.BM25_OK:
+        buf = ctypes.create_string_buffer(512)
+        lib.bm25_build_last_error(buf, len(buf))
+        raise ValueError(f'index build failed ({status}): {buf.value.decode()}')
+    k = m.value
+    return LazyIndex(offsets, docs[:k].copy(), tf[:k].copy(), norm, idf,
+                     np.diff(doc_offsets).astype(np.int32))

@@ -11,6 +11,7 @@
 #include "bm25_b200.h"
 #include "block_kernels.cuh"
 #include "learned_kernels.cuh"
+#include "merge_kernel.cuh"
 #include "stream_kernel.cuh"
 #include "tile_group_kernel.cuh"
 #include "tile_kernels.cuh"
@@ -611,6 +612,10 @@ class Engine {
         info->ring_chunk = plan_.chunk;
         info->grid = plan_.grid;
         info->smem_bytes = (int32_t)smem_bytes_;
+        info->query_capacity = opts_.query_capacity;
+        info->word_capacity = opts_.word_capacity;
+        info->max_k = opts_.max_k;
+        info->prune = opts_.prune ? 1 : 0;
     }
 
   private:
@@ -1494,6 +1499,24 @@ int bm25_search_batch_device(bm25_handle *h, const int64_t *qoffsets, const int3
                                          out_exact, static_cast<cudaStream_t>(stream));
         },
         h->error, h->code);
+}
+
+int bm25_merge_topk(const float *scores, const int32_t *ids, const int32_t *bases, int64_t q, int32_t shards,
+                    int32_t k, int64_t num_docs, int32_t shard_major, float *out_scores, int32_t *out_ids,
+                    void *stream)
+{
+    return Invoke(
+        [&] {
+            bm25b200::Check(scores && ids && out_scores && out_ids, "Null device buffer");
+            bm25b200::Check(q >= 1 && q <= INT32_MAX, "Query count outside [1, 2^31)");
+            bm25b200::Check(shards >= 1 && k >= 1 && (int64_t)shards * k <= (int64_t(1) << 30),
+                            "Shard count or K outside range");
+            bm25b200::Check(num_docs >= 1 && num_docs <= INT32_MAX, "Document count outside [1, 2^31)");
+            bm25k::MergeArgs a{scores, ids, bases, (int)q, shards, k, num_docs, out_scores, out_ids, shard_major != 0};
+            bm25k::MergeShardsKernel<<<(unsigned)q, bm25k::kMergeThreads, 0, static_cast<cudaStream_t>(stream)>>>(a);
+            bm25b200::Cuda(cudaGetLastError(), "merge kernel launch");
+        },
+        g_create_error, g_create_code);
 }
 
 int bm25_set_threshold_model(bm25_handle *h, const float *params, float margin)

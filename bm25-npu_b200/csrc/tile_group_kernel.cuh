@@ -310,6 +310,8 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
     float *ring_vals = reinterpret_cast<float *>(ring_ids + (size_t)a.stages * chunk);
     WgShared &sh = *reinterpret_cast<WgShared *>(ring_vals + (size_t)a.stages * chunk);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (a.retry && __ldcg(a.fail_in_count) == 0u)
+        return;  // nothing to retry: the work counter is left untouched
 
     if (tid == 0) {
         for (int i = 0; i < a.stages; ++i) {

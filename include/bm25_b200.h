@@ -164,6 +164,21 @@ int bm25_search_batch_device(bm25_handle *handle, const int64_t *qoffsets, const
                              int32_t *out_ids, int32_t *out_exact, void *stream);
 
 /*
+ * Exact merge of per-shard top-K lists on device buffers (replaces the reference's
+ * MergePrepare / bm25_top_k_merge, ascendhost/src/bm25/fused_runtime.h:33-34,
+ * ops/ascendc/bm25/merge/op_kernel/bm25_top_k_merge.cpp:10-86): scores/ids
+ * [q][shards][k] ([shards][q][k] when shard_major, an all-gather's layout), each
+ * list sorted by (score desc, id asc) over a disjoint document range; bases int32
+ * [shards] (device) is added to each list's ids, or NULL when the ids are already
+ * global; out [q][k].  A list that is not a valid
+ * strict ranking makes that query's output row -1.  Asynchronous on stream;
+ * errors are read with bm25_last_error(NULL, ...).
+ */
+int bm25_merge_topk(const float *scores, const int32_t *ids, const int32_t *bases, int64_t q, int32_t shards,
+                    int32_t k, int64_t num_docs, int32_t shard_major, float *out_scores, int32_t *out_ids,
+                    void *stream);
+
+/*
  * Learned starting bounds.  A prune session keeps, per term, its 32 largest
  * posting scores and its mean posting score (computed on the device at
  * creation).  From them each query gets 32 features and a safe bound (the
@@ -268,6 +283,65 @@ int bm25_mlp_gradient(const float *params, const float *features, const float *t
 int bm25_mlp_adam(float *params, float *m, float *v, const float *grad, float lr, int32_t step, void *stream);
 int bm25_mlp_last_error(char *buffer, size_t length);
 
+/*
+ * Continuous-batching server over one session (no counterpart in the reference):
+ * queries are submitted one at a time from any thread; a worker thread runs the
+ * waiting queries as one Search with a K per query (bm25_search_batch, or the
+ * learned variant) whenever the previous batch returns.  Admission: arrival
+ * order, at most max_batch queries (<= the session's query_capacity), the
+ * session's word capacity, and a candidate budget (sum of the batch's K; 0 = no
+ * limit).  max_wait_us > 0 lets a partial batch wait that long for more
+ * arrivals.  Needs a tile-group session (prune = 1 for learned).
+ */
+typedef struct bm25_server bm25_server;
+typedef struct bm25_server_options {
+    int32_t max_batch;
+    int32_t learned;
+    int32_t max_wait_us;
+    int32_t reserved;
+    int64_t candidate_budget;
+} bm25_server_options;
+void bm25_default_server_options(bm25_server_options *options);
+int bm25_server_create(bm25_handle *handle, const bm25_server_options *options, bm25_server **out);
+/* words int32 [n] (n <= 64), K in [1, max_k]; *ticket identifies the query for bm25_server_wait. */
+int bm25_server_submit(bm25_server *server, const int32_t *words, int32_t n, int32_t k, uint64_t *ticket);
+/* Blocks until the query's batch returns: scores/ids [k] (may be NULL), exact (learned; may be NULL),
+ * latency_us from submission to the batch's return. */
+int bm25_server_wait(bm25_server *server, uint64_t ticket, float *scores, int32_t *ids, int32_t *exact,
+                     double *latency_us);
+int bm25_server_stats(bm25_server *server, int64_t *batches, int64_t *served);
+/* Stops after the queued queries are served. */
+int bm25_server_destroy(bm25_server *server);
+int bm25_server_last_error(char *buffer, size_t length);
+/*
+ * Open-loop Poisson load on a server made with `options`: `total` arrivals at
+ * rate_qps (exponential gaps, seeded), query i taken from the pool (qoffsets
+ * [pool + 1], words, ks [pool]) at i % pool; latency_us [total] from each
+ * scheduled arrival to its batch's return; elapsed_s from the start to the last
+ * return; *batches Searches run.
+ */
+int bm25_serve_poisson(bm25_handle *handle, const bm25_server_options *options, const int64_t *qoffsets,
+                       const int32_t *words, const int32_t *ks, int64_t pool, double rate_qps, int64_t total,
+                       uint64_t seed, double *latency_us, double *elapsed_s, int64_t *batches);
+
+/*
+ * Index builder on the GPU (replaces the reference's Python builder,
+ * standalone/large_corpus.py:95-297): documents as token ids (doc_offsets int64
+ * [num_docs + 1], tokens int32, each in [0, vocab)) -> the lazy index of
+ * standalone/resident_index.py:12-18 in host buffers: term_offsets [vocab + 1],
+ * posting_doc_ids and posting_tf (room for doc_offsets[num_docs] postings; term
+ * frequencies as FP32), doc_norm [num_docs] = f32(k1 (1 - b + b len / avgdl))
+ * and idf [vocab] = f32(log1p((N - df + 0.5) / (df + 0.5))), both evaluated in
+ * double as the reference's Python does (it uses k1 = 1.2, b = 0.75);
+ * *postings receives the posting count.  The postings of a term are in
+ * ascending document order.  Feed the result to bm25_create_lazy.  Error
+ * details: bm25_build_last_error.
+ */
+int bm25_build_index(const int64_t *doc_offsets, const int32_t *tokens, int64_t num_docs, int64_t vocab, double k1,
+                     double b, int32_t device_id, int64_t *term_offsets, int32_t *posting_doc_ids, float *posting_tf,
+                     float *doc_norm, float *idf, int64_t *postings);
+int bm25_build_last_error(char *buffer, size_t length);
+
 /* Engine facts for reports and tests. */
 typedef struct bm25_info {
     int64_t num_docs, vocab, postings;
@@ -276,6 +350,7 @@ typedef struct bm25_info {
     int64_t index_bytes, device_bytes;
     int64_t graph_replays, searches;
     int32_t kernel, ring_stages, grid, smem_bytes, ring_chunk;
+    int32_t query_capacity, word_capacity, max_k, prune;
 } bm25_info;
 int bm25_get_info(const bm25_handle *handle, bm25_info *info);
 

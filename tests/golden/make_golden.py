@@ -7,7 +7,8 @@ REFERENCE_ROOT); the fixtures are committed so tests never need the reference.
                           original-document FP32 oracle) on 2048 docs, vocab 1024, seed 2026,
                           with the reference's query sets fixtures/A.txt and fixtures/B.txt, K 10:
                           the lazy index arrays, both query batches, expected_scores rows and
-                          expected top-K ids / scores.
+                          expected top-K ids / scores, and the generated documents' token ids
+                          (doc_offsets, tokens: the input of the GPU index builder).
   bm25s_tiny.npz          the vendored bm25s (reference_only/bm25s_original, pinned commit
                           03eac5a8) eager index of a seeded 2000-doc token-id corpus (vocab 1500) (k1 1.5,
                           b 0.75, lucene): its CSC arrays, 16 queries, the query step's full score
@@ -51,6 +52,10 @@ def large_corpus():
             arrays[f'{case}_top_ids'] = np.fromfile(out / case / 'expected_top_ids.bin', dtype='<i4').reshape(q, k)
             arrays[f'{case}_top_scores'] = np.fromfile(out / case / 'expected_top_scores.bin',
                                                        dtype='<f4').reshape(q, k)
+    # the documents themselves (the reference's generator), for the GPU index builder
+    docs = list(lc.documents(n, vocab, seed, None))
+    arrays['doc_offsets'] = np.cumsum([0] + [len(d) for d in docs]).astype(np.int64)
+    arrays['tokens'] = np.array([t for d in docs for t in d], dtype=np.int32)
     arrays['meta'] = np.array([n, vocab, seed, k], dtype=np.int64)
     np.savez_compressed(HERE / 'large_corpus_n2048.npz', **arrays)
 
