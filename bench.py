@@ -431,6 +431,52 @@ def mix_leg(pkg, args, local, world, flush, stream, rank):
     return out
 
 
+SERVE_RATES = (5000, 10000, 20000, 50000)
+SERVE_TERMS, SERVE_KS, SERVE_POOL = (1, 16), (10, 100, 1000), 4096
+
+
+def serve_leg(pkg, args, spec, index, local):
+    """The serving loop on the 10M-doc index: open-loop Poisson arrivals at 5k-50k queries/s of
+    1-16 terms (drawn by df) and K from {10, 100, 1000}; the continuous-batching server (learned
+    pruning on, every result exact) against the plain engine serving one query per Search."""
+    lo, hi = SERVE_TERMS
+    qo, w = pkg.synthetic_queries(index.offsets, SERVE_POOL, lo, hi, 4242)
+    ks = np.random.default_rng(4243).choice(SERVE_KS, SERVE_POOL).astype(np.int32)
+    kmax = max(SERVE_KS)
+    t = time.perf_counter()
+    cap = 1024
+    trainer = pkg.Bm25Session.from_lazy(index.offsets, index.docs, index.tf, index.norm, index.idf, k1=spec.k1,
+                                        query_capacity=cap, word_capacity=cap * hi, max_k=kmax, device_id=local,
+                                        prune=True)
+    model = pkg.learned.fit(trainer, index.offsets, queries=args.mix_train_queries, ks=SERVE_KS, lo=lo, hi=hi,
+                            seed=args.train_seed, steps=args.train_steps, batch=4096, gen_batch=cap,
+                            target_fallback=args.target_fallback, device=f'cuda:{local}')
+    trainer.close()
+    log(f'serving model trained in {time.perf_counter() - t:.1f}s: {model.report}')
+    session = pkg.Bm25Session.from_lazy(index.offsets, index.docs, index.tf, index.norm, index.idf, k1=spec.k1,
+                                        query_capacity=256, word_capacity=256 * hi, max_k=kmax, device_id=local,
+                                        prune=True)
+    session.set_threshold_model(model)
+    out = {'workload': WORKLOAD, 'arrivals': 'Poisson (open loop), seeded', 'terms': f'U{{{lo}..{hi}}} drawn by df',
+           'k': 'per query from {10, 100, 1000}', 'query_pool': SERVE_POOL, 'runs': []}
+    configs = (('plain, one query per Search', dict(max_batch=1, learned=False)),
+               ('continuous batching, plain', dict(max_batch=256, learned=False, candidate_budget=64_000)),
+               ('continuous batching, learned pruning', dict(max_batch=256, learned=True, candidate_budget=64_000)))
+    for rate in SERVE_RATES:
+        total = int(min(rate * args.serve_seconds, 40_000))
+        for label, opts in configs:
+            if opts['max_batch'] == 1 and rate > 10_000:
+                continue  # saturated far below these rates: its queue only grows
+            lat, st = pkg.serving.serve_poisson(session, qo, w, ks, rate_qps=rate, total=total, seed=rate, **opts)
+            row = {'config': label, 'offered_qps': rate, 'queries': total, 'achieved_qps': st['achieved_qps'],
+                   'p50_ms': st['p50_us'] / 1e3, 'p95_ms': st['p95_us'] / 1e3, 'p99_ms': st['p99_us'] / 1e3,
+                   'mean_batch': st['mean_batch']}
+            out['runs'].append(row)
+            log(f'serve {row}')
+    session.close()
+    return out
+
+
 def run_reference(args):
     rank, world, _ = setup_dist(args.gpus)
     if rank != 0:
@@ -474,6 +520,8 @@ def main():
     ap.add_argument('--target-fallback', type=float, default=0.02)
     ap.add_argument('--no-mix', action='store_true', help='skip the batched 256-query mix')
     ap.add_argument('--mix-train-queries', type=int, default=120_000)
+    ap.add_argument('--serve', action='store_true', help='also run the serving loop (Poisson arrivals)')
+    ap.add_argument('--serve-seconds', type=float, default=1.0)
     args = ap.parse_args()
     if args.impl == 'reference':
         return run_reference(args)
@@ -581,6 +629,10 @@ def main():
         learned['e2e_speedup_vs_plain'] = learned['learned']['e2e']['value'] / e2e_value
         learned['plain_per_search'] = {key: v / args.steps for key, v in plain_stats.items()}
 
+    serving = None
+    if info['kernel'] == 4 and args.serve and world == 1:
+        serving = serve_leg(pkg, args, spec, index, local)
+
     mix = None
     if info['kernel'] == 4 and not args.no_mix and not (args.docs or args.vocab):
         session.close()  # frees the 10M index before the mix corpus is resident
@@ -625,6 +677,8 @@ def main():
             line['learned_pruned'] = learned
         if mix is not None:
             line['batched_mix'] = mix
+        if serving is not None:
+            line['serving'] = serving
         if cpu is not None:
             line['cpu_baseline'] = cpu
         print(json.dumps(line), flush=True)

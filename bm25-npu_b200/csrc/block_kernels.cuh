@@ -212,56 +212,69 @@ __global__ void __launch_bounds__(kBsThreads, kTile == 1024 ? 3 : 2) BlockScoreK
     const unsigned count = (unsigned)min((long long)__ldcg(a.item_count), a.item_cap);
     unsigned bad = 0;
     unsigned long long read = 0;
-    // items are taken from a counter two at a time, the next pair's atomic in flight while the
-    // current pair is scored
-    unsigned grab = 0;
-    if (lane == 0)
-        grab = atomicAdd(a.item_count + 1, 2u);
-    unsigned it = __shfl_sync(kFull, grab, 0), pair_end = it + 2;
-    if (lane == 0)
-        grab = atomicAdd(a.item_count + 1, 2u);
-    for (; it < count; ++it) {
-        if (it == pair_end) {
-            it = __shfl_sync(kFull, grab, 0);
-            pair_end = it + 2;
-            if (it >= count)
-                break;
-            if (lane == 0)
-                grab = atomicAdd(a.item_count + 1, 2u);
+    // Word metadata of one item, lane l holding word s0 + l: plan range, directory row (-2: not a
+    // valid term) and block offsets.  fetch_rows issues the first loads, fetch_offsets the
+    // dependent block offsets; items are software-pipelined: while item i's postings are in
+    // flight, item i + 1's metadata loads are, and item i + 2's record.
+    struct Meta {
+        int pb, pe, r;
+        unsigned o[kNb / 2];
+        unsigned slot, thr;
+    };
+    auto fetch_rows = [&](const uint4 item, int s0, Meta &m) {
+        const int n = (int)item.w, q = (int)(item.x & 0xffffu), t = (int)item.y;
+        const long long qb = (long long)item.z;
+        const int s = s0 + lane;
+        m.pb = m.pe = 0;
+        m.r = -2;
+#pragma unroll
+        for (int j = 0; j < kNb / 2; ++j)
+            m.o[j] = 0u;
+        if (s < n) {
+            m.r = __ldcg(a.wrow + qb + s);
+            const PlanEntry e = a.plan[(qb + s) * a.tiles + t];
+            m.pb = (int)e.b;
+            m.pe = (int)e.e;
         }
-        const uint4 item = __ldcg(a.items + it);
+        m.slot = lane < QueryK(a, q) ? __ldcg(a.tslots + (long long)q * 32 + lane) : 0xffffffffu;
+        m.thr = __ldcg(a.threshold + q);
+    };
+    auto fetch_offsets = [&](const uint4 item, Meta &m) {
+        if (m.r >= 0 && m.pb < m.pe) {
+            const uint4 *src = reinterpret_cast<const uint4 *>(a.boff + ((long long)m.r * a.tiles + item.y) * kNb);
+#pragma unroll
+            for (int j = 0; j < kNb / 8; ++j) {
+                const uint4 v = __ldg(src + j);
+                m.o[4 * j] = v.x;
+                m.o[4 * j + 1] = v.y;
+                m.o[4 * j + 2] = v.z;
+                m.o[4 * j + 3] = v.w;
+            }
+        }
+    };
+    const unsigned stride = gridDim.x * kBsWarps;
+    unsigned it = blockIdx.x * kBsWarps + warp;
+    const uint4 none = make_uint4(0u, 0u, 0u, 0u);
+    uint4 item = it < count ? __ldcg(a.items + it) : none;
+    Meta cur;
+    fetch_rows(item, 0, cur);
+    fetch_offsets(item, cur);
+    uint4 next = it + stride < count ? __ldcg(a.items + it + stride) : none;
+    for (; it < count; it += stride) {
+        const bool more = it + stride < count;
+        Meta nxt;
+        fetch_rows(next, 0, nxt);  // loads in flight while this item is scored
+        const uint4 after = it + 2 * stride < count ? __ldcg(a.items + it + 2 * stride) : none;
         const int q = (int)(item.x & 0xffffu), t = (int)item.y, n = (int)item.w;
         const unsigned mask = item.x >> 16;
-        const long long qb = (long long)item.z;
-        const int k = QueryK(a, q);
         // running bound: the threshold (seeded with tau) or the least group slot when higher
-        const unsigned slot = lane < k ? __ldcg(a.tslots + (long long)q * 32 + lane) : 0xffffffffu;
-        const float thr = fmaxf(__uint_as_float(__ldcg(a.threshold + q)), __uint_as_float(__reduce_min_sync(kFull, slot)));
+        const float thr = fmaxf(__uint_as_float(cur.thr), __uint_as_float(__reduce_min_sync(kFull, cur.slot)));
         const int base = t * kTile;
         for (int s0 = 0; s0 < n; s0 += 32) {
-            // lane l fetches word s0 + l: its range in the tile, directory row and block offsets
-            const int s = s0 + lane;
-            int pb = 0, pe = 0, r = -2;
-            unsigned o[kNb / 2];  // block offsets, two uint16 per register
-#pragma unroll
-            for (int j = 0; j < kNb / 2; ++j)
-                o[j] = 0u;
-            if (s < n) {
-                r = __ldcg(a.wrow + qb + s);
-                const PlanEntry e = a.plan[(qb + s) * a.tiles + t];
-                pb = (int)e.b;
-                pe = (int)e.e;
-                if (r >= 0 && pb < pe) {
-                    const uint4 *src = reinterpret_cast<const uint4 *>(a.boff + ((long long)r * a.tiles + t) * kNb);
-#pragma unroll
-                    for (int j = 0; j < kNb / 8; ++j) {
-                        const uint4 v = __ldg(src + j);
-                        o[4 * j] = v.x;
-                        o[4 * j + 1] = v.y;
-                        o[4 * j + 2] = v.z;
-                        o[4 * j + 3] = v.w;
-                    }
-                }
+            Meta m = cur;
+            if (s0 > 0) {  // more than 32 words: the next ones' metadata, fetched here
+                fetch_rows(item, s0, m);
+                fetch_offsets(item, m);
             }
             // Stage the words' kept postings in query-word order with asynchronous copies, all in
             // flight at once; a flush waits for them and adds them word by word (lane i holds the
@@ -284,16 +297,16 @@ __global__ void __launch_bounds__(kBsThreads, kTile == 1024 ? 3 : 2) BlockScoreK
                 fill = 0;
                 staged = 0;
             };
-            const int m = min(32, n - s0);
-            for (int w = 0; w < m; ++w) {  // query-word order
-                const int b = __shfl_sync(kFull, pb, w), e = __shfl_sync(kFull, pe, w);
-                const int rw = __shfl_sync(kFull, r, w);
+            const int words = min(32, n - s0);
+            for (int w = 0; w < words; ++w) {  // query-word order
+                const int b = __shfl_sync(kFull, m.pb, w), e = __shfl_sync(kFull, m.pe, w);
+                const int rw = __shfl_sync(kFull, m.r, w);
                 if (b >= e || rw == -2)
                     continue;
                 unsigned off[kNb / 2];
 #pragma unroll
                 for (int j = 0; j < kNb / 2; ++j)
-                    off[j] = __shfl_sync(kFull, o[j], w);
+                    off[j] = __shfl_sync(kFull, m.o[j], w);
                 int start = fill;
                 for (unsigned mk = rw >= 0 ? mask : 1u; mk; mk &= mk - 1) {
                     int lo = b, hi = e;  // a short list: all its postings in the tile, filtered when added
@@ -339,9 +352,13 @@ __global__ void __launch_bounds__(kBsThreads, kTile == 1024 ? 3 : 2) BlockScoreK
                 if (staged == 32)
                     flush();
             }
+            if (s0 == 0 && more)
+                fetch_offsets(next, nxt);  // its rows have arrived by now; its offsets fly with our postings
             if (staged)
                 flush();
         }
+        if (n == 0 && more)
+            fetch_offsets(next, nxt);
         // a short list's postings outside the kept blocks were staged too: clear them before the
         // select (kept blocks only hold real sums)
         if (mask != (1u << kNb) - 1u) {
@@ -354,6 +371,9 @@ __global__ void __launch_bounds__(kBsThreads, kTile == 1024 ? 3 : 2) BlockScoreK
         }
         bad |= TileSelectAppend<kTile>(a, wsel[warp], row4, thr, q, t, lane);
         __syncwarp();
+        item = next;
+        cur = nxt;
+        next = after;
     }
     bad = __reduce_or_sync(kFull, bad);
     if (lane == 0) {

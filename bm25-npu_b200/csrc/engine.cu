@@ -965,7 +965,8 @@ class Engine {
             if (learned) {  // tau is this session's bound array, written here
                 bm25k::LearnedArgs la = LearnedArgsFor(q, k, qoffsets, words);
                 la.kq = kq;
-                bm25k::LearnedBoundKernel<<<q, bm25k::kLearnedThreads, 0, s>>>(la);
+                bm25k::LearnedBoundKernel<<<(q + bm25k::kLearnedQueries - 1) / bm25k::kLearnedQueries,
+                                            bm25k::kLearnedThreads, 0, s>>>(la);
                 Cuda(cudaGetLastError(), "learned bound kernel launch");
             }
             if (tau) {

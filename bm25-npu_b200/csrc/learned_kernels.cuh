@@ -92,6 +92,7 @@ __device__ __forceinline__ float QueryFeaturesWarp(const LearnedArgs &a, int q, 
     int valid = 0, oov = 0;
     float top_of[2] = {-1.0f, -1.0f};  // this lane's words (position lane, lane + 32)
     int word_of[2] = {-1, -1};
+    float feat_of[2][4] = {};  // their four per-word features
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
         const int i = lane + 32 * u;
@@ -118,6 +119,10 @@ __device__ __forceinline__ float QueryFeaturesWarp(const LearnedArgs &a, int q, 
         ++valid;
         top_of[u] = mx;
         word_of[u] = w;
+        feat_of[u][0] = LogScore(mx);
+        feat_of[u][1] = LogScore(kth);
+        feat_of[u][2] = LogScore(a.mean[w]);
+        feat_of[u][3] = ldf / 16.0f;
     }
 #pragma unroll
     for (int o = 16; o; o >>= 1) {
@@ -148,24 +153,23 @@ __device__ __forceinline__ float QueryFeaturesWarp(const LearnedArgs &a, int q, 
                 bp = op;
             }
         }
-        int w = -1;
-        if (bp != INT_MAX && bt >= 0.0f && (bp & 31) == lane) {  // the owner drops its winner
-            w = word_of[bp >> 5];
-            top_of[bp >> 5] = -1.0f;
-            word_of[bp >> 5] = -1;
+        const bool found = bp != INT_MAX && bt >= 0.0f;
+        float g[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        if (found && (bp & 31) == lane) {  // the owner hands over its winner's features and drops it
+            const int slot = bp >> 5;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                g[c] = slot ? feat_of[1][c] : feat_of[0][c];
+            top_of[slot] = -1.0f;
+            word_of[slot] = -1;
         }
-        w = __shfl_sync(kFull, w, bp != INT_MAX && bt >= 0.0f ? (bp & 31) : 0);
-        if (lane == 0) {
-            if (bp == INT_MAX || bt < 0.0f || w < 0) {
-                f[4 * j] = f[4 * j + 1] = f[4 * j + 2] = f[4 * j + 3] = 0.0f;
-            } else {
-                const float *t = a.top + (long long)w * kTermTop;
-                f[4 * j] = LogScore(t[0]);
-                f[4 * j + 1] = LogScore(t[kk - 1]);
-                f[4 * j + 2] = LogScore(a.mean[w]);
-                f[4 * j + 3] = log1pf((float)(a.indptr[w + 1] - a.indptr[w])) / 16.0f;
-            }
-        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            g[c] = __shfl_sync(kFull, g[c], found ? (bp & 31) : 0);
+        if (lane == 0)
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                f[4 * j + c] = found ? g[c] : 0.0f;
     }
     if (lane == 0) {
         f[16] = valid / 8.0f;
@@ -203,45 +207,71 @@ __global__ void QueryFeaturesKernel(const LearnedArgs a)
     }
 }
 
-constexpr int kLearnedThreads = bm25mlp::kH;
+constexpr int kLearnedQueries = 4;                            // queries per CTA
+constexpr int kLearnedThreads = kLearnedQueries * bm25mlp::kH;  // a hidden unit per thread and query
 
-// One CTA per query: warp 0 builds the features, thread i computes hidden unit i of each
-// layer (the same fmaf chain, in the same order, as bm25mlp::Forward, so the prediction is
-// bit-identical to the training kernels' forward pass), thread 0 the output and the bound.
+// kLearnedQueries queries per CTA.  The parameters are staged in shared memory with both weight
+// matrices transposed (unit i's weight j at [j][i]: consecutive threads read consecutive words);
+// warp j builds query j's features; thread i of a query's group computes hidden unit i of each
+// layer with the same fmaf chain, in the same order, as bm25mlp::Forward, so the prediction is
+// bit-identical to the training kernels' forward pass; the group's first thread the output.
 __global__ void __launch_bounds__(kLearnedThreads) LearnedBoundKernel(const LearnedArgs a)
 {
     using namespace bm25mlp;
-    __shared__ float f[kFeatures], h1[kH], h2[kH];
-    __shared__ float safe_s;
-    const int q = blockIdx.x, i = threadIdx.x;
-    if (i < 32) {
-        const float safe = QueryFeaturesWarp(a, q, f, i);
-        if (i == 0)
-            safe_s = safe;
+    __shared__ float w1t[kIn][kH], w2t[kH][kH], b1[kH], b2[kH], w3[kH];
+    __shared__ float b3;
+    __shared__ float f[kLearnedQueries][kFeatures], h1[kLearnedQueries][kH], h2[kLearnedQueries][kH];
+    __shared__ float safe_s[kLearnedQueries];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = tid / kH, i = tid % kH;  // query slot in the CTA, hidden unit
+    const int q0 = blockIdx.x * kLearnedQueries;
+    if (a.params) {
+        const float *p = a.params;
+        for (int x = tid; x < kH * kIn; x += kLearnedThreads)
+            w1t[x % kIn][x / kIn] = __ldg(p + kOffW1 + x);
+        for (int x = tid; x < kH * kH; x += kLearnedThreads)
+            w2t[x % kH][x / kH] = __ldg(p + kOffW2 + x);
+        for (int x = tid; x < kH; x += kLearnedThreads) {
+            b1[x] = __ldg(p + kOffB1 + x);
+            b2[x] = __ldg(p + kOffB2 + x);
+            w3[x] = __ldg(p + kOffW3 + x);
+        }
+        if (tid == 0)
+            b3 = __ldg(p + kOffB3);
+    }
+    if (warp < kLearnedQueries && q0 + warp < a.q) {
+        const float safe = QueryFeaturesWarp(a, q0 + warp, f[warp], lane);
+        if (lane == 0)
+            safe_s[warp] = safe;
     }
     __syncthreads();
-    const float safe = safe_s;
-    if (!a.params || safe < 0.0f) {  // uniform
-        if (i == 0)
-            a.tau[q] = fmaxf(safe, 0.0f);
-        return;
+    const int q = q0 + g;
+    const bool live = q < a.q;
+    const float safe = live ? safe_s[g] : -1.0f;
+    const bool run = a.params && safe >= 0.0f;  // uniform within a query's group
+    if (run) {
+        float acc = b1[i];
+        for (int j = 0; j < kIn; ++j)
+            acc = fmaf(w1t[j][i], f[g][j], acc);
+        h1[g][i] = fmaxf(acc, 0.0f);
     }
-    const float *p = a.params;
-    float acc = __ldg(p + kOffB1 + i);
-    for (int j = 0; j < kIn; ++j)
-        acc = fmaf(__ldg(p + kOffW1 + i * kIn + j), f[j], acc);
-    h1[i] = fmaxf(acc, 0.0f);
     __syncthreads();
-    acc = __ldg(p + kOffB2 + i);
-    for (int j = 0; j < kH; ++j)
-        acc = fmaf(__ldg(p + kOffW2 + i * kH + j), h1[j], acc);
-    h2[i] = fmaxf(acc, 0.0f);
-    __syncthreads();
-    if (i == 0) {
-        float y = __ldg(p + kOffB3);
+    if (run) {
+        float acc = b2[i];
         for (int j = 0; j < kH; ++j)
-            y = fmaf(__ldg(p + kOffW3 + j), h2[j], y);
-        a.tau[q] = fmaxf(expf(y - a.margin), safe);  // a NaN prediction leaves the safe bound
+            acc = fmaf(w2t[j][i], h1[g][j], acc);
+        h2[g][i] = fmaxf(acc, 0.0f);
+    }
+    __syncthreads();
+    if (live && i == 0) {
+        float tau = fmaxf(safe, 0.0f);
+        if (run) {
+            float y = b3;
+            for (int j = 0; j < kH; ++j)
+                y = fmaf(w3[j], h2[g][j], y);
+            tau = fmaxf(expf(y - a.margin), safe);  // a NaN prediction leaves the safe bound
+        }
+        a.tau[q] = tau;
     }
 }
 

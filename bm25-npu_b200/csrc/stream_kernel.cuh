@@ -537,14 +537,35 @@ __global__ void __launch_bounds__(kPlanThreads) PlanKernel(const StreamArgs a)
         }
         __syncthreads();  // the empty marks land before the bounds; range is published
         const long long b = range[0], en = range[1];
-        for (long long i = b + tid; i < en; i += kPlanThreads) {
-            const int t = __ldg(a.indices + i) / a.tile_docs;
-            if (t < t0 || t >= t1)
-                continue;
-            if (i == s || __ldg(a.indices + i - 1) / a.tile_docs != t)
-                out[t].b = i;
-            if (i == e - 1 || __ldg(a.indices + i + 1) / a.tile_docs != t)
-                out[t].e = i + 1;
+        // four postings per thread per round, their loads issued before any store (the stores
+        // could otherwise alias the loads and serialise them)
+        const int *__restrict__ ids = a.indices;
+        constexpr int kU = 4;
+        for (long long i0 = b + tid; i0 < en; i0 += kPlanThreads * kU) {
+            int cur[kU], prv[kU], nxt[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const long long i = i0 + (long long)u * kPlanThreads;
+                cur[u] = prv[u] = nxt[u] = -1;
+                if (i < en) {
+                    cur[u] = __ldg(ids + i);
+                    prv[u] = i == s ? -1 : __ldg(ids + i - 1);
+                    nxt[u] = i == e - 1 ? -1 : __ldg(ids + i + 1);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const long long i = i0 + (long long)u * kPlanThreads;
+                if (i >= en)
+                    continue;
+                const int t = cur[u] / a.tile_docs;
+                if (t < t0 || t >= t1)
+                    continue;
+                if (prv[u] < 0 || prv[u] / a.tile_docs != t)
+                    out[t].b = i;
+                if (nxt[u] < 0 || nxt[u] / a.tile_docs != t)
+                    out[t].e = i + 1;
+            }
         }
         __syncthreads();  // range[] is rewritten for the next word
     }
