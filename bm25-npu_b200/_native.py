@@ -43,6 +43,7 @@ class Options(ctypes.Structure):
         ('ring_chunk', c_int32),
         ('prune', c_int32),
         ('candidate_capacity', c_int64),
+        ('prune_route', c_float),
     ]
 
 

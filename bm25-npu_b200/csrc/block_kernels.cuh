@@ -147,6 +147,11 @@ __global__ void __launch_bounds__(kBbThreads) BlockBoundKernel(const StreamArgs 
             if (bound[j] > 0.0f && bound[j] >= tau)
                 keep |= 1u << j;
     }
+    if (a.qkept) {  // this CTA's kept blocks, one atomic per warp
+        const unsigned kept = __reduce_add_sync(kFull, (unsigned)__popc(keep));
+        if (lane == 0 && kept)
+            atomicAdd(a.qkept + q, kept);
+    }
     // warp-aggregated append of the tiles with a kept block
     const unsigned has = __ballot_sync(kFull, keep != 0);
     if (!has)
@@ -265,11 +270,14 @@ __global__ void __launch_bounds__(kBsThreads, kTile == 1024 ? 3 : 2) BlockScoreK
         Meta nxt;
         fetch_rows(next, 0, nxt);  // loads in flight while this item is scored
         const uint4 after = it + 2 * stride < count ? __ldcg(a.items + it + 2 * stride) : none;
-        const int q = (int)(item.x & 0xffffu), t = (int)item.y, n = (int)item.w;
+        const int q = (int)(item.x & 0xffffu), t = (int)item.y;
+        // a routed query is streamed by the tile-group kernel: its items are skipped
+        const int n = a.route_limit && __ldcg(a.qkept + q) > a.route_limit ? 0 : (int)item.w;
         const unsigned mask = item.x >> 16;
         // running bound: the threshold (seeded with tau) or the least group slot when higher
         const float thr = fmaxf(__uint_as_float(cur.thr), __uint_as_float(__reduce_min_sync(kFull, cur.slot)));
         const int base = t * kTile;
+        bool shortw = false;  // a short list (no block offsets) added postings of every block
         for (int s0 = 0; s0 < n; s0 += 32) {
             Meta m = cur;
             if (s0 > 0) {  // more than 32 words: the next ones' metadata, fetched here
@@ -307,6 +315,7 @@ __global__ void __launch_bounds__(kBsThreads, kTile == 1024 ? 3 : 2) BlockScoreK
 #pragma unroll
                 for (int j = 0; j < kNb / 2; ++j)
                     off[j] = __shfl_sync(kFull, m.o[j], w);
+                shortw |= rw < 0;
                 int start = fill;
                 for (unsigned mk = rw >= 0 ? mask : 1u; mk; mk &= mk - 1) {
                     int lo = b, hi = e;  // a short list: all its postings in the tile, filtered when added
@@ -359,17 +368,16 @@ __global__ void __launch_bounds__(kBsThreads, kTile == 1024 ? 3 : 2) BlockScoreK
         }
         if (n == 0 && more)
             fetch_offsets(next, nxt);
-        // a short list's postings outside the kept blocks were staged too: clear them before the
-        // select (kept blocks only hold real sums)
-        if (mask != (1u << kNb) - 1u) {
+        // a short list's postings outside the kept blocks were staged too: clear them (the select
+        // reads the kept blocks only, and every block must be zero for the next item)
+        if (shortw && mask != (1u << kNb) - 1u) {
 #pragma unroll
             for (int j = 0; j < kNb; ++j)
                 if (!((mask >> j) & 1u))
-                    for (int x = lane; x < kBlockDocs; x += 32)
-                        row[j * kBlockDocs + x] = 0.0f;
+                    row4[lane + 32 * j] = make_float4(0.f, 0.f, 0.f, 0.f);
             __syncwarp();
         }
-        bad |= TileSelectAppend<kTile>(a, wsel[warp], row4, thr, q, t, lane);
+        bad |= TileSelectAppend<kTile>(a, wsel[warp], row4, thr, q, t, lane, mask);
         __syncwarp();
         item = next;
         cur = nxt;
@@ -382,6 +390,19 @@ __global__ void __launch_bounds__(kBsThreads, kTile == 1024 ? 3 : 2) BlockScoreK
         if (a.stats && read)
             atomicAdd(a.stats + kStatPostingsRead, read);
     }
+}
+
+// One CTA: the queries that keep more than route_limit blocks, for the tile-group kernel.
+__global__ void RouteKernel(const StreamArgs a)
+{
+    unsigned routed = 0;
+    for (int q = threadIdx.x; q < a.q; q += blockDim.x)
+        if (__ldcg(a.qkept + q) > a.route_limit) {
+            a.route_list[atomicAdd(a.route_count, 1u)] = q;
+            ++routed;
+        }
+    if (a.stats && routed)
+        atomicAdd(a.stats + kStatRouted, (unsigned long long)routed);
 }
 
 inline const void *BlockScoreKernelFor(int tile_docs)

@@ -844,6 +844,7 @@ class Engine {
             // bound by the retry pass.
             cand_cap_ = (long long)tiles_z * per_tile;
             if (opts_.max_k > bm25k::kMaxSmallK) {
+                cand_cap_ = (long long)tiles_z * plan_.tile_docs;  // every document: the worst case
                 Check(opts_.candidate_capacity == 0 || opts_.candidate_capacity >= opts_.max_k,
                       "candidate_capacity must be 0 or at least max_k");
                 cand_cap_ = std::min<long long>(cand_cap_, opts_.candidate_capacity
@@ -851,9 +852,11 @@ class Engine {
                                                                : std::max<long long>(1 << 18, 256LL * opts_.max_k));
             }
             if (opts_.prune || opts_.max_k > bm25k::kMaxSmallK) {
-                d_fail_list_ = static_cast<int *>(Alloc(2 * qc * sizeof(int), "cudaMalloc fail lists"));
-                d_fail_count_ = static_cast<unsigned *>(Alloc(2 * sizeof(unsigned), "cudaMalloc fail counts"));
-                Cuda(cudaMemset(d_fail_count_, 0, 2 * sizeof(unsigned)), "cudaMemset");
+                // lists: retry pass 1, retry pass 2, routed queries
+                d_fail_list_ = static_cast<int *>(Alloc(3 * qc * sizeof(int), "cudaMalloc fail lists"));
+                d_fail_count_ = static_cast<unsigned *>(Alloc(3 * sizeof(unsigned), "cudaMalloc fail counts"));
+                Cuda(cudaMemset(d_fail_count_, 0, 3 * sizeof(unsigned)), "cudaMemset");
+                d_qkept_ = static_cast<unsigned *>(Alloc(qc * sizeof(unsigned), "cudaMalloc kept counts"));
             }
             if (opts_.prune) {
                 bs_smem_ = bm25k::BlockScoreSmem(plan_.tile_docs);
@@ -960,7 +963,19 @@ class Engine {
             if (retry) {
                 sa.fail_out = list_a;
                 sa.fail_out_count = d_fail_count_;
-                Cuda(cudaMemsetAsync(d_fail_count_, 0, 2 * sizeof(unsigned), s), "fail count reset");
+                Cuda(cudaMemsetAsync(d_fail_count_, 0, 3 * sizeof(unsigned), s), "fail count reset");
+            }
+            // routing (pruned batches of 32 queries or more): the queries whose bounds keep too many
+            // blocks are streamed by the tile-group kernel, the others scored block by block
+            const float route = opts_.prune_route == 0.0f ? 0.3f : opts_.prune_route;
+            const bool routing = tau != nullptr && q >= 32 && route > 0.0f && route < 1.0f;
+            if (routing) {
+                sa.qkept = d_qkept_;
+                sa.route_limit =
+                    (unsigned)std::max(1.0, (double)route * plan_.tiles * (plan_.tile_docs / bm25k::kBlockDocs));
+                sa.route_list = d_fail_list_ + 2 * (size_t)opts_.query_capacity;
+                sa.route_count = d_fail_count_ + 2;
+                Cuda(cudaMemsetAsync(d_qkept_, 0, (size_t)q * sizeof(unsigned), s), "kept count reset");
             }
             if (learned) {  // tau is this session's bound array, written here
                 bm25k::LearnedArgs la = LearnedArgsFor(q, k, qoffsets, words);
@@ -1003,6 +1018,10 @@ class Engine {
                 else
                     bm25k::BlockBoundKernel<1024><<<bgrid, bm25k::kBbThreads, 0, s>>>(sa);
                 Cuda(cudaGetLastError(), "block bound kernel launch");
+                if (routing) {
+                    bm25k::RouteKernel<<<1, 256, 0, s>>>(sa);
+                    Cuda(cudaGetLastError(), "route kernel launch");
+                }
                 MarkKernel(0, s);
                 if (plan_.tile_docs == 2048)
                     bm25k::BlockScoreKernel<2048><<<bs_grid_, bm25k::kBsThreads, bs_smem_, s>>>(sa);
@@ -1010,6 +1029,14 @@ class Engine {
                     bm25k::BlockScoreKernel<1024><<<bs_grid_, bm25k::kBsThreads, bs_smem_, s>>>(sa);
                 Cuda(cudaGetLastError(), "block score kernel launch");
                 MarkKernel(1, s);
+                if (routing) {  // the routed queries, streamed from their starting bound
+                    bm25k::StreamArgs xa = sa;
+                    xa.retry = 1;
+                    xa.fail_in = sa.route_list;
+                    xa.fail_in_count = sa.route_count;
+                    tile_group(xa);
+                    Cuda(cudaGetLastError(), "routed tile group launch");
+                }
             } else if (plan_.kernel == 0) {
                 const int grid = (int)std::min<long long>(
                     plan_.grid, ((long long)q * plan_.tiles + bm25k::kTaskBatch - 1) / bm25k::kTaskBatch);
@@ -1229,7 +1256,7 @@ class Engine {
     float *d_term_top_ = nullptr, *d_term_mean_ = nullptr, *d_model_ = nullptr, *d_tau_ = nullptr;
     unsigned long long *d_stats_ = nullptr;
     int *d_fail_list_ = nullptr;
-    unsigned *d_fail_count_ = nullptr;
+    unsigned *d_fail_count_ = nullptr, *d_qkept_ = nullptr;
     bool has_model_ = false;
     float margin_ = 0.0f;
     bool closed_ = false, failed_ = false;

@@ -76,7 +76,8 @@ enum : int {
     kStatItems = 3,
     kStatBlocksKept = 4,
     kStatPostingsRead = 5,
-    kStats = 6,
+    kStatRouted = 6,
+    kStats = 7,
 };
 
 enum : int {
@@ -127,6 +128,12 @@ struct StreamArgs {
     int *wrow;                   // [word] directory row of the word's term, -1 none, -2 not a valid term
     unsigned *item_count;        // [2]: items listed, items taken (both reset by PlanKernel)
     long long item_cap;
+    // routing: a query keeping more than route_limit blocks is streamed by the tile-group kernel
+    // instead (route_limit 0: never); qkept [Q] counts its kept blocks, route_list its queries
+    unsigned *qkept;
+    unsigned route_limit;
+    int *route_list;
+    unsigned *route_count;
     // retry passes: a pass appends to fail_out the queries it could not answer (a pruned pass that
     // fell short of K, a K > 32 candidate buffer that overflowed); a retry pass (retry != 0)
     // searches the queries of fail_in on the plain path.  Counts are reset before the Search.

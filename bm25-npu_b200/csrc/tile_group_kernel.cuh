@@ -99,6 +99,25 @@ __device__ __forceinline__ void WarpTakeRow(float4 *reg4, int lane, float *x)
         reg4[lane + 32 * j] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
+// WarpTakeRow over the 128-document blocks of `mask` only (block j is float4 j of every lane);
+// the other blocks read as 0 and are left as they are (the caller keeps them zero).
+template <int kVec>
+__device__ __forceinline__ void WarpTakeRowMasked(float4 *reg4, int lane, float *x, unsigned mask)
+{
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) {
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if ((mask >> j) & 1u) {  // uniform
+            v = reg4[lane + 32 * j];
+            reg4[lane + 32 * j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        x[4 * j] = v.x;
+        x[4 * j + 1] = v.y;
+        x[4 * j + 2] = v.z;
+        x[4 * j + 3] = v.w;
+    }
+}
+
 // "x >= thr and x > 0" is "x >= max(thr, least positive float)" for thr >= 0
 constexpr float kLeastPositive = 1.40129846e-45f;
 
@@ -187,13 +206,16 @@ __device__ __forceinline__ int WarpSelectRegs(WarpSel &ws, const float *x, float
     return n;
 }
 
-// WarpTakeRow + WarpSelectRegs.
+// WarpTakeRow (of the blocks of `mask`) + WarpSelectRegs.
 template <int kVec>
 __device__ __forceinline__ int WarpRowSelect(WarpSel &ws, float4 *reg4, float thr, int k, int base_id, int lane,
-                                             float *kth)
+                                             float *kth, unsigned mask = ~0u)
 {
     float x[4 * kVec];
-    WarpTakeRow<kVec>(reg4, lane, x);
+    if (mask == ~0u)
+        WarpTakeRow<kVec>(reg4, lane, x);
+    else
+        WarpTakeRowMasked<kVec>(reg4, lane, x, mask);
     return WarpSelectRegs<kVec>(ws, x, thr, k, base_id, lane, kth);
 }
 
@@ -203,14 +225,14 @@ __device__ __forceinline__ int WarpRowSelect(WarpSel &ws, float4 *reg4, float th
 // bits.  Every lane of the warp calls.
 template <int kTile>
 __device__ __forceinline__ unsigned TileSelectAppend(const StreamArgs &a, WarpSel &ws, float4 *row4, float thr, int q,
-                                                     int tile, int lane)
+                                                     int tile, int lane, unsigned mask = ~0u)
 {
     const int base_doc = tile * kTile;
     unsigned bad = 0;
     const int k = QueryK(a, q);
     if (k <= 32) {
         float kth;
-        const int sel = WarpRowSelect<kTile / 128>(ws, row4, thr, k, base_doc, lane, &kth);
+        const int sel = WarpRowSelect<kTile / 128>(ws, row4, thr, k, base_doc, lane, &kth, mask);
         if (sel > 0) {
             if (!(ws.sel_s[0] <= FLT_MAX))
                 bad |= kStatusOverflow;  // an overflowed sum would be the tile's best score
@@ -239,7 +261,10 @@ __device__ __forceinline__ unsigned TileSelectAppend(const StreamArgs &a, WarpSe
         // searched again from its final bound)
         constexpr int kElems = kTile / 32;
         float x[kElems];
-        WarpTakeRow<kTile / 128>(row4, lane, x);
+        if (mask == ~0u)
+            WarpTakeRow<kTile / 128>(row4, lane, x);
+        else
+            WarpTakeRowMasked<kTile / 128>(row4, lane, x, mask);
         const int m = (k + 31) >> 5;
         float mth;
         const int sel = WarpSelectRegs<kTile / 128>(ws, x, thr, m, base_doc, lane, &mth);

@@ -70,7 +70,7 @@ def pack_queries(queries):
 
 
 def _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes, stream,
-             kernel=4, ring_stages=0, ring_chunk=0, prune=False, candidate_capacity=0):
+             kernel=4, ring_stages=0, ring_chunk=0, prune=False, candidate_capacity=0, prune_route=0.0):
     o = n.Options()
     n.engine_library().bm25_default_options(ctypes.byref(o))
     o.device_id = device_id
@@ -86,6 +86,7 @@ def _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_f
     o.ring_chunk = ring_chunk
     o.prune = int(bool(prune))
     o.candidate_capacity = candidate_capacity
+    o.prune_route = prune_route
     return o
 
 
@@ -101,7 +102,7 @@ class Bm25Session:
     @classmethod
     def from_csc(cls, indptr, indices, data, num_docs, *, query_capacity=8, word_capacity=24, max_k=10,
                  device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0, stream=None, kernel=4, ring_stages=0,
-                 ring_chunk=0, prune=False, candidate_capacity=0):
+                 ring_chunk=0, prune=False, candidate_capacity=0, prune_route=0.0):
         """Eager CSC index (bm25s layout): indptr int64 [V+1], indices int32 [M], data float32 [M]."""
         lib = n.engine_library()
         indptr = np.ascontiguousarray(indptr, dtype=np.int64)
@@ -111,7 +112,7 @@ class Bm25Session:
         if vocab < 1 or indices.size != indptr[-1] or data.size != indices.size:
             raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'Index dimensions/endpoints differ')
         o = _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes,
-                     stream, kernel, ring_stages, ring_chunk, prune, candidate_capacity)
+                     stream, kernel, ring_stages, ring_chunk, prune, candidate_capacity, prune_route)
         h = c_void_p()
         status = lib.bm25_create(n.ptr(indptr, c_int64), n.ptr(indices, c_int32), n.ptr(data, c_float), vocab,
                                  int(num_docs), ctypes.byref(o), ctypes.byref(h))
@@ -121,7 +122,8 @@ class Bm25Session:
     @classmethod
     def from_lazy(cls, term_offsets, posting_doc_ids, posting_tf, doc_norm, idf, *, k1=1.2, query_capacity=8,
                   word_capacity=24, max_k=10, device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0,
-                  stream=None, kernel=4, ring_stages=0, ring_chunk=0, prune=False, candidate_capacity=0):
+                  stream=None, kernel=4, ring_stages=0, ring_chunk=0, prune=False, candidate_capacity=0,
+                  prune_route=0.0):
         """The reference's resident index (common/bm25/index_data.h:9-42); posting scores built on the GPU."""
         lib = n.engine_library()
         offsets = np.ascontiguousarray(term_offsets, dtype=np.int64)
@@ -133,7 +135,7 @@ class Bm25Session:
         if offsets.size != vocab + 1 or docs.size != tf.size or offsets[-1] != docs.size:
             raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'Index dimensions/endpoints differ')
         o = _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes,
-                     stream, kernel, ring_stages, ring_chunk, prune, candidate_capacity)
+                     stream, kernel, ring_stages, ring_chunk, prune, candidate_capacity, prune_route)
         h = c_void_p()
         status = lib.bm25_create_lazy(n.ptr(offsets, c_int64), n.ptr(docs, c_int32), n.ptr(tf, c_float),
                                       n.ptr(norm, c_float), n.ptr(idf, c_float), vocab, norm.size, float(k1),
@@ -279,9 +281,10 @@ class Bm25Session:
     def search_stats(self, reset=True):
         """Search counters since the last reset (tile-group kernel: claims, tiles scanned, postings
         copied; block-max pruned pass: tiles scored, blocks kept, postings read)."""
-        out = (ctypes.c_uint64 * 6)()
+        out = (ctypes.c_uint64 * 7)()
         _raise(self._lib, self._lib.bm25_search_stats(self._handle, out, int(bool(reset))), self._handle)
-        names = ('claims', 'tiles_scanned', 'postings_copied', 'block_tiles', 'blocks_kept', 'postings_read')
+        names = ('claims', 'tiles_scanned', 'postings_copied', 'block_tiles', 'blocks_kept', 'postings_read',
+                 'queries_streamed')
         return dict(zip(names, out))
 
     def search_device(self, qoffsets_ptr, words_ptr, q, k, scores_ptr, ids_ptr, stream_ptr=None):

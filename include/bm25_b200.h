@@ -55,6 +55,9 @@ typedef struct bm25_options {
                                 the pruned and learned Searches (tile-group kernel only) */
     int64_t candidate_capacity; /* max_k > 32: candidates kept per query (0 = automatic, 256 K and at least
                                    2^18); a query that overflows it is searched again from its final bound */
+    float prune_route;       /* pruned Searches of 32 queries or more: a query keeping more than this share of
+                                its 128-document blocks is streamed by the tile-group kernel instead
+                                (0 = 0.3; negative = never) */
 } bm25_options;
 
 /* Search kernels (bm25_options.kernel):
@@ -203,10 +206,10 @@ int bm25_search_learned_device(bm25_handle *handle, const int64_t *qoffsets, con
 
 /*
  * Search counters summed over Searches since the last reset (waits for the
- * handle's work), out[6]: tile-group kernel -- [0] claims (query x 8-tile
+ * handle's work), out[7]: tile-group kernel -- [0] claims (query x 8-tile
  * groups), [1] tiles scanned, [2] postings copied from HBM into the staging
  * rings; block-max pruned pass -- [3] tiles scored, [4] 128-document blocks
- * kept, [5] postings read.
+ * kept, [5] postings read, [6] queries streamed instead (prune_route).
  */
 int bm25_search_stats(bm25_handle *handle, uint64_t *out, int32_t reset);
 

@@ -73,8 +73,10 @@ def test_large_k_pruned_matches_oracle(pkg, oracle_mod, corpus, cuda_ok):
     index, data = corpus
     offsets, words = _queries(index, 5, 29)
     q = offsets.size - 1
+    # a buffer that holds every document: no query overflows, so the flags follow tau alone
     with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, query_capacity=64,
-                                  word_capacity=1024, max_k=1000, prune=True) as s:
+                                  word_capacity=1024, max_k=1000, prune=True,
+                                  candidate_capacity=index.num_docs + 2048) as s:
         for k in (100, 1000):
             want_s, want_i, full = oracle_mod.search(index.offsets, index.docs, data, index.num_docs, offsets,
                                                      words, k, full=True)

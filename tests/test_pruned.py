@@ -129,3 +129,29 @@ def test_pruned_needs_prune_session(pkg, corpus, cuda_ok):
             s.search_pruned([[1, 2]], 10, np.zeros(1, np.float32))
     with pytest.raises(pkg.InvalidParam):
         pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, kernel=0, prune=True)
+
+
+@pytest.mark.gpu
+def test_routing_streams_broad_queries_exactly(pkg, oracle_mod, corpus, cuda_ok):
+    """In a pruned batch of 32+ queries, the queries whose bounds keep more than prune_route of their
+    blocks are streamed by the tile-group kernel from their starting bound: still exact."""
+    index, data = corpus
+    rng = np.random.default_rng(77)
+    df = np.diff(index.offsets)
+    common = np.argsort(-df)[:40]
+    rows = [[int(x) for x in rng.choice(common, 6, replace=False)] for _ in range(12)]  # broad
+    rows += mixed_queries(index.vocab, rng, 28, 1, 4, oov=False)
+    offsets, words = pack(rows)
+    q = len(rows)
+    with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, query_capacity=64,
+                                  word_capacity=1024, max_k=32, prune=True, prune_route=0.2) as s:
+        for k in (10, 32):
+            want_s, want_i, full = oracle_mod.search(index.offsets, index.docs, data, index.num_docs, offsets,
+                                                     words, k, full=True)
+            tau = (want_s[:, -1] * np.float32(0.9)).astype(np.float32)
+            s.search_stats(reset=True)
+            got_s, got_i, exact = s.search_pruned((offsets, words), k, tau)
+            st = s.search_stats(reset=True)
+            assert_same_topk(got_s, got_i, want_s, want_i, f'k={k}')
+            assert np.array_equal(exact, expected_exact(full, tau, k))
+            assert 0 < st['queries_streamed'] < q, st
