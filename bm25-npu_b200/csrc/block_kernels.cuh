@@ -76,8 +76,24 @@ template <int kTile>
 __global__ void __launch_bounds__(kBbThreads) BlockBoundKernel(const StreamArgs a)
 {
     constexpr int kNb = kTile / kBlockDocs;
-    const int q = blockIdx.y, t = blockIdx.x * kBbThreads + threadIdx.x, lane = threadIdx.x & 31;
-    const float tau = a.tau[q] > 0.0f ? a.tau[q] : 0.0f;  // NaN or negative: no bound
+    const int t = blockIdx.x * kBbThreads + threadIdx.x, lane = threadIdx.x & 31;
+    int q = blockIdx.y;
+    float tau;
+    if (a.retry) {
+        // a query whose first pass fell short: its bound is now a proven one, the larger of its
+        // group slots' least (real documents' scores) and its safe bound from term statistics
+        if ((unsigned)q >= __ldcg(a.fail_in_count))
+            return;
+        q = __ldcg(a.fail_in + q);
+        const int k = QueryK(a, q), ns = min(k, 32);
+        const unsigned slot = lane < ns ? __ldcg(a.tslots + (long long)q * 32 + lane) : 0xffffffffu;
+        tau = __uint_as_float(__reduce_min_sync(kFull, slot));
+        if (a.safe)
+            tau = fmaxf(tau, a.safe[q]);
+    } else {
+        tau = a.tau[q];
+    }
+    tau = tau > 0.0f ? tau : 0.0f;  // NaN or negative: no bound
     if (t == 0)
         a.threshold[q] = __float_as_uint(tau);
     const long long qb = a.qoffsets[q], qe = a.qoffsets[q + 1];

@@ -768,7 +768,8 @@ class Engine {
             d_items_ = static_cast<uint4 *>(Alloc(item_cap_ * sizeof(uint4), "cudaMalloc block work list"));
             d_wrow_ = static_cast<int *>(Alloc(std::max<size_t>(1, opts_.word_capacity) * sizeof(int),
                                                "cudaMalloc word rows"));
-            d_item_count_ = static_cast<unsigned *>(Alloc(2 * sizeof(unsigned), "cudaMalloc block work count"));
+            d_item_count_ = static_cast<unsigned *>(Alloc(4 * sizeof(unsigned), "cudaMalloc block work count"));
+            d_safe_ = static_cast<float *>(Alloc(opts_.query_capacity * sizeof(float), "cudaMalloc safe bounds"));
             d_term_top_ = static_cast<float *>(Alloc(vocab_ * bm25k::kTermTop * sizeof(float), "cudaMalloc term top"));
             d_term_mean_ = static_cast<float *>(Alloc(vocab_ * sizeof(float), "cudaMalloc term mean"));
             d_model_ = static_cast<float *>(Alloc(bm25mlp::kParams * sizeof(float), "cudaMalloc model"));
@@ -980,6 +981,7 @@ class Engine {
             if (learned) {  // tau is this session's bound array, written here
                 bm25k::LearnedArgs la = LearnedArgsFor(q, k, qoffsets, words);
                 la.kq = kq;
+                la.safe = d_safe_;
                 bm25k::LearnedBoundKernel<<<(q + bm25k::kLearnedQueries - 1) / bm25k::kLearnedQueries,
                                             bm25k::kLearnedThreads, 0, s>>>(la);
                 Cuda(cudaGetLastError(), "learned bound kernel launch");
@@ -1057,19 +1059,40 @@ class Engine {
                 bm25k::StreamArgs ra = sa;
                 ra.tau = nullptr;
                 ra.exact = nullptr;
-                ra.items = nullptr;
-                ra.wrow = nullptr;
-                ra.item_count = nullptr;
                 ra.retry = 1;
                 ra.fail_in = list_a;
                 ra.fail_in_count = d_fail_count_;
                 ra.fail_out = retry2 ? list_b : nullptr;
                 ra.fail_out_count = retry2 ? d_fail_count_ + 1 : nullptr;
-                tile_group(ra);
+                ra.qkept = nullptr;
+                ra.route_limit = 0;
+                if (tau) {
+                    // a pruned first pass: the retry is block-pruned too, from each query's proven
+                    // bound (its slots, its safe bound), so a wrong guess costs little
+                    ra.item_count = d_item_count_ + 2;
+                    ra.safe = learned ? d_safe_ : nullptr;
+                    const dim3 bgrid((plan_.tiles + bm25k::kBbThreads - 1) / bm25k::kBbThreads, q);
+                    if (plan_.tile_docs == 2048) {
+                        bm25k::BlockBoundKernel<2048><<<bgrid, bm25k::kBbThreads, 0, s>>>(ra);
+                        bm25k::BlockScoreKernel<2048><<<bs_grid_, bm25k::kBsThreads, bs_smem_, s>>>(ra);
+                    } else {
+                        bm25k::BlockBoundKernel<1024><<<bgrid, bm25k::kBbThreads, 0, s>>>(ra);
+                        bm25k::BlockScoreKernel<1024><<<bs_grid_, bm25k::kBsThreads, bs_smem_, s>>>(ra);
+                    }
+                } else {
+                    ra.items = nullptr;
+                    ra.wrow = nullptr;
+                    ra.item_count = nullptr;
+                    tile_group(ra);
+                }
                 Cuda(cudaGetLastError(), "retry kernel launch");
                 final_select(ra);
                 if (retry2) {
                     bm25k::StreamArgs rb = ra;
+                    rb.items = nullptr;
+                    rb.wrow = nullptr;
+                    rb.item_count = nullptr;
+                    rb.safe = nullptr;
                     rb.fail_in = list_b;
                     rb.fail_in_count = d_fail_count_ + 1;
                     rb.fail_out = nullptr;
@@ -1238,6 +1261,7 @@ class Engine {
     float *d_bmax_ = nullptr;
     uint4 *d_items_ = nullptr;
     int *d_wrow_ = nullptr;
+    float *d_safe_ = nullptr;
     unsigned *d_item_count_ = nullptr;
     long long item_cap_ = 0;
     size_t bs_smem_ = 0;

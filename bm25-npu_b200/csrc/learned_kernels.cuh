@@ -218,7 +218,9 @@ constexpr int kLearnedThreads = kLearnedQueries * bm25mlp::kH;  // a hidden unit
 __global__ void __launch_bounds__(kLearnedThreads) LearnedBoundKernel(const LearnedArgs a)
 {
     using namespace bm25mlp;
-    __shared__ float w1t[kIn][kH], w2t[kH][kH], b1[kH], b2[kH], w3[kH];
+    // rows padded by one word: the transposing stores and the per-unit reads are both free of
+    // bank conflicts
+    __shared__ float w1t[kIn][kH + 1], w2t[kH][kH + 1], b1[kH], b2[kH], w3[kH];
     __shared__ float b3;
     __shared__ float f[kLearnedQueries][kFeatures], h1[kLearnedQueries][kH], h2[kLearnedQueries][kH];
     __shared__ float safe_s[kLearnedQueries];
@@ -272,6 +274,8 @@ __global__ void __launch_bounds__(kLearnedThreads) LearnedBoundKernel(const Lear
             tau = fmaxf(expf(y - a.margin), safe);  // a NaN prediction leaves the safe bound
         }
         a.tau[q] = tau;
+        if (a.safe)
+            a.safe[q] = safe;
     }
 }
 

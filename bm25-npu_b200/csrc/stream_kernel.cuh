@@ -123,10 +123,11 @@ struct StreamArgs {
     const unsigned short *boff;  // [dir row][tile][block] posting offset of the block from the tile's start
     const float *bmax;           // [dir row][tile][block] largest posting score of the row's term in the block
     const float *tau;            // [Q] starting bound guesses
+    const float *safe;           // [Q] safe bounds (learned Searches; a retry's bound), or nullptr
     int *exact;                  // [Q] 1 where K candidates reached tau
     uint4 *items;                // (query | kept-block mask << 16, tile, first word, words) per tile to score
     int *wrow;                   // [word] directory row of the word's term, -1 none, -2 not a valid term
-    unsigned *item_count;        // [2]: items listed, items taken (both reset by PlanKernel)
+    unsigned *item_count;        // items listed (first pass at [0], retry pass at [2]; reset by PlanKernel)
     long long item_cap;
     // routing: a query keeping more than route_limit blocks is streamed by the tile-group kernel
     // instead (route_limit 0: never); qkept [Q] counts its kept blocks, route_list its queries
@@ -493,8 +494,8 @@ __device__ __forceinline__ long long WarpLowerBoundGlobal(const int *ids, long l
 __global__ void __launch_bounds__(kPlanThreads) PlanKernel(const StreamArgs a)
 {
     __shared__ long long range[2];
-    if (a.item_count && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < 2)
-        a.item_count[threadIdx.x] = 0u;  // the block path's work list of this Search starts empty
+    if (a.item_count && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < 4)
+        a.item_count[threadIdx.x] = 0u;  // the block path's work lists of this Search start empty
     long long total = a.qoffsets[a.q];
     if (total < 0 || total > a.word_cap) {
         if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
