@@ -322,28 +322,46 @@ __global__ void __launch_bounds__(kBsThreads, kTile == 1024 ? 3 : 2) BlockScoreK
                 staged = 0;
             };
             const int words = min(32, n - s0);
+            // 1024-document tiles: the words' block offsets go to a table in the warp's selection
+            // scratch (unused until the select), one 16-byte row per word
+            unsigned short *otab = reinterpret_cast<unsigned short *>(&wsel[warp]);
+            if (kNb == 8) {
+                static_assert(sizeof(WarpSel) >= 32 * 16, "offset table fits the selection scratch");
+                __syncwarp();  // the previous chunk's reads are done
+                reinterpret_cast<uint4 *>(otab)[lane] = make_uint4(m.o[0], m.o[1 % (kNb / 2)], m.o[2 % (kNb / 2)],
+                                                                   m.o[3 % (kNb / 2)]);
+                __syncwarp();
+            }
             for (int w = 0; w < words; ++w) {  // query-word order
                 const int b = __shfl_sync(kFull, m.pb, w), e = __shfl_sync(kFull, m.pe, w);
                 const int rw = __shfl_sync(kFull, m.r, w);
                 if (b >= e || rw == -2)
                     continue;
                 unsigned off[kNb / 2];
+                if (kNb != 8) {
 #pragma unroll
-                for (int j = 0; j < kNb / 2; ++j)
-                    off[j] = __shfl_sync(kFull, m.o[j], w);
+                    for (int j = 0; j < kNb / 2; ++j)
+                        off[j] = __shfl_sync(kFull, m.o[j], w);
+                }
                 shortw |= rw < 0;
                 int start = fill;
                 for (unsigned mk = rw >= 0 ? mask : 1u; mk; mk &= mk - 1) {
                     int lo = b, hi = e;  // a short list: all its postings in the tile, filtered when added
                     if (rw >= 0) {
                         const int j = __ffs(mk) - 1;
+                        if (kNb == 8) {
+                            lo = b + otab[w * 8 + j];
+                            if (j + 1 < kNb)
+                                hi = b + otab[w * 8 + j + 1];
+                        } else {
 #pragma unroll
-                        for (int u = 0; u < kNb; ++u) {  // register-indexed: no local memory
-                            const int ou = (int)((off[u >> 1] >> ((u & 1) * 16)) & 0xffffu);
-                            if (u == j)
-                                lo = b + ou;
-                            if (u == j + 1)
-                                hi = b + ou;
+                            for (int u = 0; u < kNb; ++u) {  // register-indexed: no local memory
+                                const int ou = (int)((off[u >> 1] >> ((u & 1) * 16)) & 0xffffu);
+                                if (u == j)
+                                    lo = b + ou;
+                                if (u == j + 1)
+                                    hi = b + ou;
+                            }
                         }
                     }
                     for (int c = lo; c < hi;) {
