@@ -72,8 +72,21 @@ def build_facade(force=False):
     return target
 
 
+def build_runner(force=False):
+    """bm25_runner: the reference's benchmark runner command line on this engine (csrc/runner.cpp)."""
+    target = PACKAGE / 'bm25_runner'
+    src = CSRC / 'runner.cpp'
+    engine = build_engine(force)
+    deps = [src, INCLUDE / 'bm25_b200.h', engine, Path(__file__)]
+    if not force and not _stale(target, deps):
+        return target
+    _run(['g++', '-O2', '-std=c++17', '-Wall', '-I', INCLUDE, '-I', '/usr/local/cuda/include', '-o', target, src,
+          '-L', PACKAGE, '-lbm25_b200', '-L', '/usr/local/cuda/lib64', '-lcudart', "-Wl,-rpath,$ORIGIN"])
+    return target
+
+
 def build_all(force=False):
-    return build_engine(force), build_synth(force), build_facade(force)
+    return build_engine(force), build_synth(force), build_facade(force), build_runner(force)
 
 
 if __name__ == '__main__':
