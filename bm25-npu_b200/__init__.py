@@ -5,7 +5,7 @@ a Python identifier).  The CUDA engine (libbm25_b200.so) must be built in-tree
 (``python bm25-npu_b200/build.py``); without it the Search API raises ImportError.
 """
 
-from . import _native, learned, serving, sharded
+from . import _native, autotune, learned, serving, sharded
 from .corpus import (CONFIG_SHAPES, INDEX_FILES, CorpusSpec, LazyIndex, build_index, read_bm25s_dir, read_index_dir,
                      read_queries_dir, synthetic_index, synthetic_queries, unpack_queries, write_bm25s_dir,
                      write_index_dir, write_queries_dir)
@@ -18,5 +18,5 @@ __all__ = [
     'synthetic_queries', 'unpack_queries', 'write_index_dir', 'read_queries_dir', 'write_queries_dir',
     'read_bm25s_dir', 'write_bm25s_dir', 'APP_ERR_ILLEGAL_OPERATION', 'APP_ERR_INNER_ERROR',
     'APP_ERR_INVALID_PARAM', 'APP_ERR_OK', 'AscendIndexBm25', 'Bm25Config', 'Bm25Error', 'Bm25SearchResult',
-    'Bm25Session', 'IllegalOperation', 'InnerError', 'InvalidParam', 'pack_queries', '_native', 'learned', 'serving', 'sharded',
+    'Bm25Session', 'IllegalOperation', 'InnerError', 'InvalidParam', 'pack_queries', '_native', 'autotune', 'learned', 'serving', 'sharded',
 ]
