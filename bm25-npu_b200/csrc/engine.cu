@@ -831,6 +831,8 @@ class Engine {
             } else {
                 smem_bytes_ = bm25k::TileGroupSmem(plan_.stages, plan_.chunk, plan_.tile_docs);
                 kernel = bm25k::TileGroupKernelFor(plan_.tile_docs);
+                RaiseSmemCap(bm25k::TileGroupKernelFor(plan_.tile_docs, true),
+                             bm25k::TileGroupSmem(plan_.stages, plan_.chunk, plan_.tile_docs));
                 threads = bm25k::kWgThreads;
                 per_tile = opts_.max_k;
             }
@@ -1011,10 +1013,18 @@ class Engine {
             const long long claims = (long long)q * ((plan_.tiles + bm25k::kWgWarps - 1) / bm25k::kWgWarps);
             const int wg_grid = (int)std::max<long long>(1, std::min<long long>(plan_.grid, claims));
             auto tile_group = [&](const bm25k::StreamArgs &args) {
-                if (plan_.tile_docs == 2048)
-                    bm25k::TileGroupKernel<2048><<<wg_grid, bm25k::kWgThreads, smem_bytes_, s>>>(args);
-                else
-                    bm25k::TileGroupKernel<1024><<<wg_grid, bm25k::kWgThreads, smem_bytes_, s>>>(args);
+                const bool lean = !args.retry && !args.kq && k <= bm25k::kMaxSmallK;
+                if (plan_.tile_docs == 2048) {
+                    if (lean)
+                        bm25k::TileGroupKernel<2048, true><<<wg_grid, bm25k::kWgThreads, smem_bytes_, s>>>(args);
+                    else
+                        bm25k::TileGroupKernel<2048><<<wg_grid, bm25k::kWgThreads, smem_bytes_, s>>>(args);
+                } else {
+                    if (lean)
+                        bm25k::TileGroupKernel<1024, true><<<wg_grid, bm25k::kWgThreads, smem_bytes_, s>>>(args);
+                    else
+                        bm25k::TileGroupKernel<1024><<<wg_grid, bm25k::kWgThreads, smem_bytes_, s>>>(args);
+                }
             };
             auto final_select = [&](const bm25k::StreamArgs &args) {
                 if (k <= bm25k::kMaxSmallK || kq)

@@ -72,6 +72,10 @@ struct WgShared {
     WgMeta meta[kMaxStages];
     WarpSel wsel[kWgWarps];
     int abort;
+    // the producer's counters (in shared memory, not registers: every register of the producer
+    // is one of every consumer thread too)
+    unsigned n_claims, n_tiles;
+    unsigned long long n_copied;
 };
 
 inline size_t TileGroupSmem(int stages, int chunk, int tile_docs)
@@ -223,14 +227,15 @@ __device__ __forceinline__ int WarpRowSelect(WarpSel &ws, float4 *reg4, float th
 // above the bound `thr` to query q's candidate buffer -- the top K for K <= 32, every
 // one for K > 32 -- and raises the query's threshold and group slots.  Returns status
 // bits.  Every lane of the warp calls.
-template <int kTile>
+// kSmallK: every query's K is a.k <= 32 (the lean instantiation of the plain Search).
+template <int kTile, bool kSmallK = false>
 __device__ __forceinline__ unsigned TileSelectAppend(const StreamArgs &a, WarpSel &ws, float4 *row4, float thr, int q,
                                                      int tile, int lane, unsigned mask = ~0u)
 {
     const int base_doc = tile * kTile;
     unsigned bad = 0;
-    const int k = QueryK(a, q);
-    if (k <= 32) {
+    const int k = kSmallK ? a.k : QueryK(a, q);
+    if (kSmallK || k <= 32) {
         float kth;
         const int sel = WarpRowSelect<kTile / 128>(ws, row4, thr, k, base_doc, lane, &kth, mask);
         if (sel > 0) {
@@ -254,7 +259,7 @@ __device__ __forceinline__ unsigned TileSelectAppend(const StreamArgs &a, WarpSe
                 }
             }
         }
-    } else {
+    } else if constexpr (!kSmallK) {
         // K > 32: slot tile % 32 takes the tile's m-th best (m = ceil(K / 32)), so the 32
         // slots stand for 32 m >= K documents; every document at or above the bound is
         // appended (the final select ranks them; a query whose buffer overflows is
@@ -324,8 +329,10 @@ __device__ __forceinline__ int2 WgFarRange(const StreamArgs &a, const WgClaim &c
     return make_int2((int)pe.b, (int)pe.e);
 }
 
-// kTile: documents per tile (a.tile_docs), 1024 or 2048.
-template <int kTile>
+// kTile: documents per tile (a.tile_docs), 1024 or 2048.  kLean: the plain first pass with one
+// K <= 32 for every query (no retry list, no K per query): the instantiation with the fewest
+// registers, so the most resident warps.
+template <int kTile, bool kLean = false>
 __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKernel(const StreamArgs a)
 {
     extern __shared__ __align__(128) unsigned char wg_smem[];
@@ -335,7 +342,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
     float *ring_vals = reinterpret_cast<float *>(ring_ids + (size_t)a.stages * chunk);
     WgShared &sh = *reinterpret_cast<WgShared *>(ring_vals + (size_t)a.stages * chunk);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (a.retry && __ldcg(a.fail_in_count) == 0u)
+    if (!kLean && a.retry && __ldcg(a.fail_in_count) == 0u)
         return;  // nothing to retry: the work counter is left untouched
 
     if (tid == 0) {
@@ -344,6 +351,8 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
             MbarInit(&sh.empty[i], kWgWarps);
         }
         sh.abort = 0;
+        sh.n_claims = sh.n_tiles = 0u;
+        sh.n_copied = 0ull;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int i = tid; i < kWgWarps * kTile / 4; i += kWgThreads)
@@ -352,7 +361,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
     volatile int *abort = &sh.abort;
     const unsigned groups = (unsigned)((a.tiles + kWgWarps - 1) / kWgWarps);
     // a retry pass covers only the queries on the fail list (possibly none)
-    const unsigned nq = a.retry ? __ldcg(a.fail_in_count) : (unsigned)a.q;
+    const unsigned nq = !kLean && a.retry ? __ldcg(a.fail_in_count) : (unsigned)a.q;
     const unsigned claims = nq * groups;
 
     if (warp == kWgWarps) {
@@ -362,8 +371,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
         unsigned wraps = 0;        // times the ring has wrapped
         unsigned bad = 0;
         bool dead = false;
-        unsigned n_claims = 0, n_tiles = 0;  // lane 0's counts
-        unsigned long long n_copied = 0;
+
         // Waits until stage pst is free (its previous use released).
         auto claim_stage = [&]() -> bool {
             int ok = 1;
@@ -386,7 +394,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
         auto decode = [&](unsigned c, WgClaim &w) {
             w.valid = c < claims;
             w.q = w.valid ? (int)(c % nq) : 0;
-            if (a.retry && w.valid)
+            if (!kLean && a.retry && w.valid)
                 w.q = __ldcg(a.fail_in + w.q);
             w.tile0 = w.valid ? (int)(c / nq) * kWgWarps : 0;
             w.n = 0;
@@ -422,7 +430,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
                 w.p1 = make_int2((int)pe.b, (int)pe.e);
             }
             w.thr_bits = __ldcg(a.threshold + w.q);
-            if (lane < QueryK(a, w.q))
+            if (lane < (kLean ? a.k : QueryK(a, w.q)))
                 w.slot_bits = __ldcg(a.tslots + (long long)w.q * 32 + lane);
         };
         auto take_claim = [&]() -> unsigned {
@@ -449,8 +457,10 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
 
             const float thr =
                 fmaxf(__uint_as_float(cur.thr_bits), __uint_as_float(__reduce_min_sync(kFull, cur.slot_bits)));
-            ++n_claims;
-            n_tiles += (unsigned)min(kWgWarps, a.tiles - cur.tile0);
+            if (lane == 0) {
+                ++sh.n_claims;
+                sh.n_tiles += (unsigned)min(kWgWarps, a.tiles - cur.tile0);
+            }
             // each word's run over the group, reduced within its 8 lanes
             const bool ne0 = cur.p0.x < cur.p0.y, ne1 = cur.p1.x < cur.p1.y;
             int lo0 = ne0 ? cur.p0.x : 0x7fffffff, hi0 = ne0 ? cur.p0.y : -1;
@@ -524,7 +534,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
                     __syncwarp();  // the meta is complete before lane 0 starts the stage
                     if (lane == 0) {
                         const unsigned bytes = (unsigned)(c1 - c0) * 4u;
-                        n_copied += (unsigned long long)(c1 - c0);
+                        sh.n_copied += (unsigned long long)(c1 - c0);
                         MbarArriveExpectTx(&sh.full[st], 2u * bytes);
                         BulkLoad(ring_ids + (size_t)st * chunk, a.indices + c0, bytes, &sh.full[st]);
                         BulkLoad(ring_vals + (size_t)st * chunk, a.data + c0, bytes, &sh.full[st]);
@@ -552,9 +562,9 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
             if (bad)
                 atomicOr(a.status, bad);
             if (a.stats) {
-                atomicAdd(a.stats + kStatClaims, (unsigned long long)n_claims);
-                atomicAdd(a.stats + kStatTilesScanned, (unsigned long long)n_tiles);
-                atomicAdd(a.stats + kStatPostingsCopied, n_copied);
+                atomicAdd(a.stats + kStatClaims, (unsigned long long)sh.n_claims);
+                atomicAdd(a.stats + kStatTilesScanned, (unsigned long long)sh.n_tiles);
+                atomicAdd(a.stats + kStatPostingsCopied, sh.n_copied);
             }
             // the last producer to run dry resets the work counter for the next Search
             const unsigned d = atomicAdd(&a.ctrl->done, 1u);
@@ -645,7 +655,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
         touched = false;
 
         // ---- end of the claim: select this warp's tile ----
-        bad |= TileSelectAppend<kTile>(a, ws, row4, thr, q, tile, lane);
+        bad |= TileSelectAppend<kTile, kLean>(a, ws, row4, thr, q, tile, lane);
         __syncwarp();
     }
     bad = __reduce_or_sync(kFull, bad);
@@ -653,8 +663,11 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
         atomicOr(a.status, bad | (*abort ? kStatusTimeout : 0u));
 }
 
-inline const void *TileGroupKernelFor(int tile_docs)
+inline const void *TileGroupKernelFor(int tile_docs, bool lean = false)
 {
+    if (lean)
+        return tile_docs == 2048 ? reinterpret_cast<const void *>(&TileGroupKernel<2048, true>)
+                                 : reinterpret_cast<const void *>(&TileGroupKernel<1024, true>);
     return tile_docs == 2048 ? reinterpret_cast<const void *>(&TileGroupKernel<2048>)
                              : reinterpret_cast<const void *>(&TileGroupKernel<1024>);
 }
