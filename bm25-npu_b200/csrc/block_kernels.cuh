@@ -223,6 +223,9 @@ __global__ void __launch_bounds__(kBsThreads, kTile == 1024 ? 3 : 2) BlockScoreK
     float *stage_vals = reinterpret_cast<float *>(stage_ids + (size_t)kBsWarps * kBsStage);
     WarpSel *wsel = reinterpret_cast<WarpSel *>(stage_vals + (size_t)kBsWarps * kBsStage);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned count = (unsigned)min((long long)__ldcg(a.item_count), a.item_cap);
+    if (blockIdx.x * kBsWarps >= count)
+        return;  // no item for any warp of this CTA (an empty retry list among them)
     for (int i = tid; i < kBsWarps * kTile / 4; i += kBsThreads)
         reinterpret_cast<float4 *>(rows)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     __syncthreads();
@@ -230,7 +233,6 @@ __global__ void __launch_bounds__(kBsThreads, kTile == 1024 ? 3 : 2) BlockScoreK
     float4 *row4 = reinterpret_cast<float4 *>(row);
     int *sid = stage_ids + (size_t)warp * kBsStage;
     float *sval = stage_vals + (size_t)warp * kBsStage;
-    const unsigned count = (unsigned)min((long long)__ldcg(a.item_count), a.item_cap);
     unsigned bad = 0;
     unsigned long long read = 0;
     // Word metadata of one item, lane l holding word s0 + l: plan range, directory row (-2: not a
