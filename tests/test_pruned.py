@@ -65,7 +65,10 @@ def corpus(pkg, oracle_mod):
 def test_pruned_matches_oracle(pkg, oracle_mod, corpus, cuda_ok, tile_docs):
     index, data = corpus
     rng = np.random.default_rng(tile_docs)
-    rows = mixed_queries(index.vocab, rng, 40, 0, 14, oov=True) + [[0, 1, 2], [5] * 12, []]
+    # besides random rows: a duplicated word, an empty query, and 40 words (the block scorer
+    # fetches word metadata 32 words at a time)
+    rows = mixed_queries(index.vocab, rng, 40, 0, 14, oov=True) + [[0, 1, 2], [5] * 12, [],
+                                                                   [int(x) for x in rng.integers(0, 2000, 40)]]
     offsets, words = pack(rows)
     q = len(rows)
     with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, query_capacity=64,
