@@ -210,24 +210,25 @@ def cpu_search_leg(index, sets, k, budget_s, max_steps, warmup=1):
 
 def timed_device(session, step, steps, warmup, flush, stream, world, with_clocks=None):
     """Device-resident steps timed with CUDA events on the launching stream, L2 flushed between
-    steps; returns (step ms, main-kernel ms, clocks)."""
+    steps; returns (step ms, main-kernel ms, clocks).
+
+    Two passes over the same K steps.  The first gives the step times and the clocks: only the
+    step's own events are recorded.  The second also has the engine record an event pair around
+    its main kernel, for that kernel's duration; an event between two kernels keeps the later one
+    from starting while the earlier one runs (programmatic dependent launch), so the second pass
+    is slower and gives no step times.  The engine's counters are those of the second pass."""
     import torch
     import torch.distributed as dist
-    with torch.cuda.stream(stream):
-        for i in range(warmup):
-            step(i)
-        stream.synchronize()
-        status = session.device_status()
-        if status != 0:
-            raise RuntimeError(f'device status {status:#x} set during warm-up')
+
+    def run(marks):
         starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
         ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
-        session.kernel_timing(True)
+        session.kernel_timing(marks)
         session.search_stats(reset=True)
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
-        if with_clocks:
+        if with_clocks and not marks:
             with_clocks.start()
         for i in range(steps):
             flush.zero_()
@@ -235,13 +236,23 @@ def timed_device(session, step, steps, warmup, flush, stream, world, with_clocks
             step(i)
             ends[i].record(stream)
         torch.cuda.synchronize()
-        clock_info = with_clocks.stop() if with_clocks else None
-    status = session.device_status()
-    if status != 0:
-        raise RuntimeError(f'device status {status:#x} set during the timed region')
-    step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
-    kernel_ms = [float(x) for x in session.kernel_times()]
-    session.kernel_timing(False)
+        clocks = with_clocks.stop() if with_clocks and not marks else None
+        status = session.device_status()
+        if status != 0:
+            raise RuntimeError(f'device status {status:#x} set during the timed region')
+        kernel = [float(x) for x in session.kernel_times()] if marks else None
+        session.kernel_timing(False)
+        return [a.elapsed_time(b) for a, b in zip(starts, ends)], kernel, clocks
+
+    with torch.cuda.stream(stream):
+        for i in range(warmup):
+            step(i)
+        stream.synchronize()
+        status = session.device_status()
+        if status != 0:
+            raise RuntimeError(f'device status {status:#x} set during warm-up')
+        step_ms, _, clock_info = run(False)
+        _, kernel_ms, _ = run(True)
     if len(kernel_ms) != steps:
         raise RuntimeError(f'{len(kernel_ms)} kernel timings for {steps} steps')
     return step_ms, kernel_ms, clock_info

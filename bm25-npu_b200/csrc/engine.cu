@@ -72,6 +72,25 @@ static void RaiseSmemCap(const void *kernel, size_t bytes)
 
 static size_t Align32(size_t n) { return (n + 31) & ~size_t(31); }
 
+// Launch with programmatic stream serialization: the kernel may start while the kernel before it
+// in the stream runs (the kernel waits in WaitPrerequisites before reading that kernel's output).
+template <class... Params, class... Args>
+static void LaunchOverlapped(void (*kernel)(Params...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                             Args &&...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    Cuda(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...), "overlapped kernel launch");
+}
+
 constexpr int kPad = 256; // zero elements after the posting arrays for 128-bit tail loads
 
 // ---------------------------------------------------------------------------
@@ -857,6 +876,7 @@ class Engine {
                                                                ? opts_.candidate_capacity
                                                                : std::max<long long>(1 << 18, 256LL * opts_.max_k));
             }
+            cand_cap_ = (cand_cap_ + 3) & ~3LL;  // rows start on 16-byte boundaries (128-bit reads)
             if (opts_.prune || opts_.max_k > bm25k::kMaxSmallK) {
                 // lists: retry pass 1, retry pass 2, routed queries
                 d_fail_list_ = static_cast<int *>(Alloc(3 * qc * sizeof(int), "cudaMalloc fail lists"));
@@ -1020,15 +1040,16 @@ class Engine {
                     else
                         bm25k::TileGroupKernel<2048><<<wg_grid, bm25k::kWgThreads, smem_bytes_, s>>>(args);
                 } else {
-                    if (lean)
-                        bm25k::TileGroupKernel<1024, true><<<wg_grid, bm25k::kWgThreads, smem_bytes_, s>>>(args);
+                    if (lean)  // right after the plan kernel: set up while it runs
+                        LaunchOverlapped(bm25k::TileGroupKernel<1024, true>, wg_grid, bm25k::kWgThreads, smem_bytes_,
+                                         s, args);
                     else
                         bm25k::TileGroupKernel<1024><<<wg_grid, bm25k::kWgThreads, smem_bytes_, s>>>(args);
                 }
             };
             auto final_select = [&](const bm25k::StreamArgs &args) {
                 if (k <= bm25k::kMaxSmallK || kq)
-                    bm25k::FinalSelectKernel<<<q, bm25k::kFinalThreads, 0, s>>>(args);
+                    LaunchOverlapped(bm25k::FinalSelectKernel, q, bm25k::kFinalThreads, 0, s, args);
                 if (k > bm25k::kMaxSmallK)
                     bm25k::FinalSelectLargeKernel<<<q, bm25k::kLargeThreads, 0, s>>>(args);
             };

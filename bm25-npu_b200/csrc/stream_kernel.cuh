@@ -184,6 +184,14 @@ struct StreamShared {
 
 __device__ __forceinline__ unsigned SmemAddr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
+// Programmatic dependent launch.  A kernel launched with programmatic stream serialization may
+// start while the kernel before it in the stream still runs: it waits in WaitPrerequisites
+// (until that kernel has completed and its writes are visible) before reading anything that
+// kernel wrote.  AllowDependents lets the next such kernel start early.  Both are no-ops when
+// no launch in the stream uses the attribute.
+__device__ __forceinline__ void WaitPrerequisites() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void AllowDependents() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
 __device__ __forceinline__ void MbarInit(unsigned long long *bar, unsigned count)
 {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(SmemAddr(bar)), "r"(count) : "memory");
@@ -494,6 +502,7 @@ __device__ __forceinline__ long long WarpLowerBoundGlobal(const int *ids, long l
 __global__ void __launch_bounds__(kPlanThreads) PlanKernel(const StreamArgs a)
 {
     __shared__ long long range[2];
+    AllowDependents();  // the tile-group kernel sets up its shared memory meanwhile
     if (a.item_count && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < 4)
         a.item_count[threadIdx.x] = 0u;  // the block path's work lists of this Search start empty
     long long total = a.qoffsets[a.q];
@@ -522,9 +531,27 @@ __global__ void __launch_bounds__(kPlanThreads) PlanKernel(const StreamArgs a)
         const long long s = a.indptr[term], e = a.indptr[term + 1];
         const int r = a.dir_row ? a.dir_row[term] : -1;
         if (r >= 0) {
-            const int *d = a.dir + (long long)r * a.dir_stride;
-            for (int t = t0 + tid; t < t1; t += kPlanThreads)
-                out[t] = PlanEntry{s + d[t], s + d[t + 1]};
+            // the chunk's tiles, kPlanTileChunk / kPlanThreads per thread, every directory load
+            // issued before the stores (which could otherwise alias them and serialise the loop)
+            const int *__restrict__ d = a.dir + (long long)r * a.dir_stride;
+            constexpr int kU = kPlanTileChunk / kPlanThreads;
+            static_assert(kPlanTileChunk % kPlanThreads == 0, "whole rounds of tiles per plan CTA");
+            int lo[kU], hi[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int t = t0 + tid + u * kPlanThreads;
+                lo[u] = hi[u] = 0;
+                if (t < t1) {
+                    lo[u] = __ldg(d + t);
+                    hi[u] = __ldg(d + t + 1);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int t = t0 + tid + u * kPlanThreads;
+                if (t < t1)
+                    out[t] = PlanEntry{s + lo[u], s + hi[u]};
+            }
             continue;
         }
         for (int t = t0 + tid; t < t1; t += kPlanThreads)
@@ -888,6 +915,7 @@ __global__ void __launch_bounds__(kFinalThreads) FinalSelectKernel(const StreamA
     __shared__ unsigned surv_count;
     __shared__ int sel_count;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    WaitPrerequisites();  // the candidates and bounds of the search kernel before it
     int q = blockIdx.x;
     if (a.retry) {  // block b answers the b-th query of the fail list
         if ((unsigned)q >= __ldcg(a.fail_in_count))
@@ -917,59 +945,93 @@ __global__ void __launch_bounds__(kFinalThreads) FinalSelectKernel(const StreamA
     }
     const float *cs = a.cand_scores + (long long)q * a.cand_cap;
     const int *ci = a.cand_ids + (long long)q * a.cand_cap;
+    // a row that starts on a 16-byte boundary is read 128 bits at a time, four loads in flight
+    // per thread (the engine's rows all do: cand_cap is a multiple of 4); the rest one by one
+    const float4 *cs4 = reinterpret_cast<const float4 *>(cs);
+    const int n4 = (reinterpret_cast<uintptr_t>(cs) & 15u) == 0 ? n >> 2 : 0;
 
-    float tmax = 0.0f;
-    for (int i = tid; i < n; i += kFinalThreads)
-        tmax = fmaxf(tmax, __ldcg(cs + i));
-    const int j = (k + kWarps - 1) / kWarps;
-    float v = tmax, jth = 0.0f;
-    for (int r = 0; r < j; ++r) {
-        float mx = v;
-#pragma unroll
-        for (int o = 16; o; o >>= 1)
-            mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, o));
-        jth = mx;
-        const unsigned who = __ballot_sync(kFull, v == mx);
-        if (lane == __ffs(who) - 1)
-            v = -1.0f;
-    }
-    if (lane == 0)
-        wv[warp] = fmaxf(jth, 0.0f);
-    if (tid == 0)
-        surv_count = 0;
-    __syncthreads();
-    const int m = (k + j - 1) / j;
-    float w[kWarps];
-#pragma unroll
-    for (int i = 0; i < kWarps; ++i)
-        w[i] = wv[i];
-    float tau = 0.0f;
-    for (int r = 0; r < m; ++r) {
-        int best = 0;
-#pragma unroll
-        for (int i = 1; i < kWarps; ++i)
-            if (w[i] > w[best])
-                best = i;
-        tau = w[best];
-#pragma unroll
-        for (int i = 0; i < kWarps; ++i)
-            if (i == best)
-                w[i] = -2.0f;
-    }
-    tau = fmaxf(tau, floor);
-    for (int i = tid; i < n; i += kFinalThreads) {
-        const float s = __ldcg(cs + i);
-        if (s > 0.0f && s >= tau) {
+    auto keep = [&](float s, int i, float bound) {
+        if (s > 0.0f && s >= bound) {
             const unsigned at = atomicAdd(&surv_count, 1u);
             if (at < (unsigned)kSurvCap) {
                 surv_s[at] = s;
                 surv_i[at] = __ldcg(ci + i);
             }
         }
-    }
+    };
+    auto filter = [&](float bound) {  // every candidate at or above bound joins the survivors
+#pragma unroll 4
+        for (int i = tid; i < n4; i += kFinalThreads) {
+            const float4 v = __ldcg(cs4 + i);
+            keep(v.x, 4 * i, bound);
+            keep(v.y, 4 * i + 1, bound);
+            keep(v.z, 4 * i + 2, bound);
+            keep(v.w, 4 * i + 3, bound);
+        }
+        for (int i = 4 * n4 + tid; i < n; i += kFinalThreads)
+            keep(__ldcg(cs + i), i, bound);
+    };
+    // One pass at the floor: each top-k document of the query is a candidate at or above it (its
+    // tile appended its top-k above a lower bound than the floor).  Only when that leaves more
+    // survivors than fit is a higher bound taken from the candidates themselves (below).
+    if (tid == 0)
+        surv_count = 0;
     __syncthreads();
+    filter(floor);
+    __syncthreads();
+    float tau = floor;
+    if (surv_count > (unsigned)kSurvCap) {
+        float tmax = 0.0f;  // the largest of this thread's candidates: distinct threads, distinct documents
+#pragma unroll 4
+        for (int i = tid; i < n4; i += kFinalThreads) {
+            const float4 v = __ldcg(cs4 + i);
+            tmax = fmaxf(tmax, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+        }
+        for (int i = 4 * n4 + tid; i < n; i += kFinalThreads)
+            tmax = fmaxf(tmax, __ldcg(cs + i));
+        const int j = (k + kWarps - 1) / kWarps;
+        float v = tmax, jth = 0.0f;
+        for (int r = 0; r < j; ++r) {
+            float mx = v;
+#pragma unroll
+            for (int o = 16; o; o >>= 1)
+                mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, o));
+            jth = mx;
+            const unsigned who = __ballot_sync(kFull, v == mx);
+            if (lane == __ffs(who) - 1)
+                v = -1.0f;
+        }
+        if (lane == 0)
+            wv[warp] = fmaxf(jth, 0.0f);
+        __syncthreads();
+        if (tid == 0)
+            surv_count = 0;
+        const int m = (k + j - 1) / j;
+        float w[kWarps];
+#pragma unroll
+        for (int i = 0; i < kWarps; ++i)
+            w[i] = wv[i];
+        float bound = 0.0f;
+        for (int r = 0; r < m; ++r) {
+            int best = 0;
+#pragma unroll
+            for (int i = 1; i < kWarps; ++i)
+                if (w[i] > w[best])
+                    best = i;
+            bound = w[best];
+#pragma unroll
+            for (int i = 0; i < kWarps; ++i)
+                if (i == best)
+                    w[i] = -2.0f;
+        }
+        tau = fmaxf(bound, floor);
+        __syncthreads();
+        filter(tau);
+        __syncthreads();
+    }
     const unsigned c = surv_count;
-    if (c <= (unsigned)kSurvCap) {
+    if (c <= 64u) {
+        // a few survivors: each one's exact rank
         for (unsigned i = tid; i < c; i += kFinalThreads) {
             const float s = surv_s[i];
             const int id = surv_i[i];
@@ -980,6 +1042,39 @@ __global__ void __launch_bounds__(kFinalThreads) FinalSelectKernel(const StreamA
                 sel_s[rank] = s;
                 sel_i[rank] = id;
             }
+        }
+        if (tid == 0)
+            sel_count = (int)min(c, (unsigned)k);
+    } else if (c <= (unsigned)kSurvCap) {
+        // up to kSurvCap survivors: a bitonic sort by (score desc, id asc) in shared memory, padded
+        // to a power of two with entries that order after every survivor
+        unsigned p = 128u;
+        while (p < c)
+            p <<= 1;
+        for (unsigned i = c + tid; i < p; i += kFinalThreads) {
+            surv_s[i] = -1.0f;
+            surv_i[i] = INT_MAX;
+        }
+        __syncthreads();
+        for (unsigned size = 2; size <= p; size <<= 1)
+            for (unsigned stride = size >> 1; stride > 0; stride >>= 1) {
+                for (unsigned i = tid; i < p / 2; i += kFinalThreads) {
+                    const unsigned lo = 2 * i - (i & (stride - 1)), hi = lo + stride;
+                    const float ls = surv_s[lo], hs = surv_s[hi];
+                    const int li = surv_i[lo], hid = surv_i[hi];
+                    // runs whose bit `size` is clear end best-first, the others best-last
+                    if (((lo & size) == 0) == Better(hs, hid, ls, li)) {
+                        surv_s[lo] = hs;
+                        surv_i[lo] = hid;
+                        surv_s[hi] = ls;
+                        surv_i[hi] = li;
+                    }
+                }
+                __syncthreads();
+            }
+        for (int i = tid; i < k; i += kFinalThreads) {
+            sel_s[i] = surv_s[i];
+            sel_i[i] = surv_i[i];
         }
         if (tid == 0)
             sel_count = (int)min(c, (unsigned)k);

@@ -342,8 +342,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
     float *ring_vals = reinterpret_cast<float *>(ring_ids + (size_t)a.stages * chunk);
     WgShared &sh = *reinterpret_cast<WgShared *>(ring_vals + (size_t)a.stages * chunk);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (!kLean && a.retry && __ldcg(a.fail_in_count) == 0u)
-        return;  // nothing to retry: the work counter is left untouched
+    AllowDependents();  // the final select may be placed as this kernel's CTAs retire
 
     if (tid == 0) {
         for (int i = 0; i < a.stages; ++i) {
@@ -358,6 +357,9 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
     for (int i = tid; i < kWgWarps * kTile / 4; i += kWgThreads)
         reinterpret_cast<float4 *>(rows)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     __syncthreads();
+    WaitPrerequisites();  // the plan (or the fail list) of the kernel before this one
+    if (!kLean && a.retry && __ldcg(a.fail_in_count) == 0u)
+        return;  // nothing to retry: the work counter is left untouched
     volatile int *abort = &sh.abort;
     const unsigned groups = (unsigned)((a.tiles + kWgWarps - 1) / kWgWarps);
     // a retry pass covers only the queries on the fail list (possibly none)
