@@ -77,6 +77,8 @@ __global__ void __launch_bounds__(kBbThreads) BlockBoundKernel(const StreamArgs 
 {
     constexpr int kNb = kTile / kBlockDocs;
     const int t = blockIdx.x * kBbThreads + threadIdx.x, lane = threadIdx.x & 31;
+    AllowDependents();    // the block scorer may be placed meanwhile
+    WaitPrerequisites();  // the plan, or the fail list of the final select before a retry
     int q = blockIdx.y;
     float tau;
     if (a.retry) {
@@ -223,6 +225,8 @@ __global__ void __launch_bounds__(kBsThreads, kTile == 1024 ? 3 : 2) BlockScoreK
     float *stage_vals = reinterpret_cast<float *>(stage_ids + (size_t)kBsWarps * kBsStage);
     WarpSel *wsel = reinterpret_cast<WarpSel *>(stage_vals + (size_t)kBsWarps * kBsStage);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    AllowDependents();
+    WaitPrerequisites();  // the work list of the block bound kernel
     const unsigned count = (unsigned)min((long long)__ldcg(a.item_count), a.item_cap);
     if (blockIdx.x * kBsWarps >= count)
         return;  // no item for any warp of this CTA (an empty retry list among them)

@@ -75,11 +75,11 @@ static size_t Align32(size_t n) { return (n + 31) & ~size_t(31); }
 // Launch with programmatic stream serialization: the kernel may start while the kernel before it
 // in the stream runs (the kernel waits in WaitPrerequisites before reading that kernel's output).
 template <class... Params, class... Args>
-static void LaunchOverlapped(void (*kernel)(Params...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+static void LaunchOverlapped(void (*kernel)(Params...), dim3 grid, unsigned block, size_t smem, cudaStream_t s,
                              Args &&...args)
 {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
+    cfg.gridDim = grid;
     cfg.blockDim = dim3(block);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
@@ -1057,9 +1057,9 @@ class Engine {
                 // block-max pruned pass: bounds per (query, tile, block), then the kept blocks
                 const dim3 bgrid((plan_.tiles + bm25k::kBbThreads - 1) / bm25k::kBbThreads, q);
                 if (plan_.tile_docs == 2048)
-                    bm25k::BlockBoundKernel<2048><<<bgrid, bm25k::kBbThreads, 0, s>>>(sa);
+                    LaunchOverlapped(bm25k::BlockBoundKernel<2048>, bgrid, bm25k::kBbThreads, 0, s, sa);
                 else
-                    bm25k::BlockBoundKernel<1024><<<bgrid, bm25k::kBbThreads, 0, s>>>(sa);
+                    LaunchOverlapped(bm25k::BlockBoundKernel<1024>, bgrid, bm25k::kBbThreads, 0, s, sa);
                 Cuda(cudaGetLastError(), "block bound kernel launch");
                 if (routing) {
                     bm25k::RouteKernel<<<1, 256, 0, s>>>(sa);
@@ -1067,9 +1067,9 @@ class Engine {
                 }
                 MarkKernel(0, s);
                 if (plan_.tile_docs == 2048)
-                    bm25k::BlockScoreKernel<2048><<<bs_grid_, bm25k::kBsThreads, bs_smem_, s>>>(sa);
+                    LaunchOverlapped(bm25k::BlockScoreKernel<2048>, bs_grid_, bm25k::kBsThreads, bs_smem_, s, sa);
                 else
-                    bm25k::BlockScoreKernel<1024><<<bs_grid_, bm25k::kBsThreads, bs_smem_, s>>>(sa);
+                    LaunchOverlapped(bm25k::BlockScoreKernel<1024>, bs_grid_, bm25k::kBsThreads, bs_smem_, s, sa);
                 Cuda(cudaGetLastError(), "block score kernel launch");
                 MarkKernel(1, s);
                 if (routing) {  // the routed queries, streamed from their starting bound
@@ -1114,11 +1114,11 @@ class Engine {
                     ra.safe = learned ? d_safe_ : nullptr;
                     const dim3 bgrid((plan_.tiles + bm25k::kBbThreads - 1) / bm25k::kBbThreads, q);
                     if (plan_.tile_docs == 2048) {
-                        bm25k::BlockBoundKernel<2048><<<bgrid, bm25k::kBbThreads, 0, s>>>(ra);
-                        bm25k::BlockScoreKernel<2048><<<bs_grid_, bm25k::kBsThreads, bs_smem_, s>>>(ra);
+                        LaunchOverlapped(bm25k::BlockBoundKernel<2048>, bgrid, bm25k::kBbThreads, 0, s, ra);
+                        LaunchOverlapped(bm25k::BlockScoreKernel<2048>, bs_grid_, bm25k::kBsThreads, bs_smem_, s, ra);
                     } else {
-                        bm25k::BlockBoundKernel<1024><<<bgrid, bm25k::kBbThreads, 0, s>>>(ra);
-                        bm25k::BlockScoreKernel<1024><<<bs_grid_, bm25k::kBsThreads, bs_smem_, s>>>(ra);
+                        LaunchOverlapped(bm25k::BlockBoundKernel<1024>, bgrid, bm25k::kBbThreads, 0, s, ra);
+                        LaunchOverlapped(bm25k::BlockScoreKernel<1024>, bs_grid_, bm25k::kBsThreads, bs_smem_, s, ra);
                     }
                 } else {
                     ra.items = nullptr;

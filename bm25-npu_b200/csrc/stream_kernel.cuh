@@ -915,6 +915,7 @@ __global__ void __launch_bounds__(kFinalThreads) FinalSelectKernel(const StreamA
     __shared__ unsigned surv_count;
     __shared__ int sel_count;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    AllowDependents();    // a retry pass may be placed meanwhile
     WaitPrerequisites();  // the candidates and bounds of the search kernel before it
     int q = blockIdx.x;
     if (a.retry) {  // block b answers the b-th query of the fail list
