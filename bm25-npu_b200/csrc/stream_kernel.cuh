@@ -572,10 +572,10 @@ __global__ void __launch_bounds__(kPlanThreads) PlanKernel(const StreamArgs a)
         }
         __syncthreads();  // the empty marks land before the bounds; range is published
         const long long b = range[0], en = range[1];
-        // four postings per thread per round, their loads issued before any store (the stores
-        // could otherwise alias the loads and serialise them)
+        // sixteen postings per thread per round (a list of 4096 in one), their loads issued
+        // before any store (the stores could otherwise alias the loads and serialise them)
         const int *__restrict__ ids = a.indices;
-        constexpr int kU = 4;
+        constexpr int kU = 16;
         for (long long i0 = b + tid; i0 < en; i0 += kPlanThreads * kU) {
             int cur[kU], prv[kU], nxt[kU];
 #pragma unroll
