@@ -442,6 +442,127 @@ def mix_leg(pkg, args, local, world, flush, stream, rank):
     return out
 
 
+BLOCKMAX_WORKLOAD = 'blockmax_4p2m'
+BLOCKMAX_Q, BLOCKMAX_TERMS, BLOCKMAX_KS, BLOCKMAX_EVAL = 250, (2, 10), (10, 100), 10_000
+
+
+def parity_by_k(pkg, index, k1, session, qo, w, ks, kset):
+    """One batch with a K per query against the oracle, one oracle call per K (rank 0 only)."""
+    from oracle import oracle
+    data = oracle.contributions(index, k1)
+    ok = True
+    gs, gi, koff = session.search_batch((qo, w), ks)
+    for k in kset:
+        sel = np.nonzero(ks == k)[0]
+        if sel.size == 0:
+            continue
+        rows = [w[qo[i]:qo[i + 1]] for i in sel]
+        o = np.zeros(len(rows) + 1, np.int64)
+        o[1:] = np.cumsum([len(r) for r in rows])
+        rs, ri = oracle.search(index.offsets, index.docs, data, index.num_docs, o,
+                               np.concatenate(rows).astype(np.int32), int(k), threads=os.cpu_count() or 1)
+        for j, i in enumerate(sel):
+            ok &= bool(np.array_equal(gi[koff[i]:koff[i + 1]], ri[j]) and
+                       np.array_equal(gs[koff[i]:koff[i + 1]].view(np.uint32), rs[j].view(np.uint32)))
+    return ok
+
+
+def blockmax_leg(pkg, args, local, world, flush, stream, rank):
+    """The block-max workload: 4.2M docs (V 1M, mean length 80), a threshold model trained on
+    200k queries, then 10k held-out queries of 2-10 terms drawn by df with K drawn from {10, 100}
+    per query, answered 250 to a Search (40 Searches, one pass over the set per timed pass), plain
+    and learned-pruned.  Besides queries/s: the postings each Search touches either way."""
+    import torch
+    spec = pkg.CONFIG_SHAPES[BLOCKMAX_WORKLOAD]
+    t = time.perf_counter()
+    index = pkg.synthetic_index(spec)
+    log(f'block-max corpus: N={index.num_docs} V={index.vocab} M={index.postings} in {time.perf_counter() - t:.1f}s')
+    lo, hi = BLOCKMAX_TERMS
+    n_batches = BLOCKMAX_EVAL // BLOCKMAX_Q
+    qo_all, w_all = pkg.synthetic_queries(index.offsets, BLOCKMAX_EVAL, lo, hi, 440000 + 1000 * rank)
+    ks_all = np.random.default_rng(550 + 1000 * rank).choice(BLOCKMAX_KS, BLOCKMAX_EVAL).astype(np.int32)
+    batches = []
+    for b in range(n_batches):
+        a0, a1 = b * BLOCKMAX_Q, (b + 1) * BLOCKMAX_Q
+        qo = (qo_all[a0:a1 + 1] - qo_all[a0]).astype(np.int64)
+        batches.append((qo, w_all[qo_all[a0]:qo_all[a1]].copy(), ks_all[a0:a1].copy()))
+    kmax = max(BLOCKMAX_KS)
+    session = pkg.Bm25Session.from_lazy(index.offsets, index.docs, index.tf, index.norm, index.idf, k1=spec.k1,
+                                        query_capacity=BLOCKMAX_Q, word_capacity=BLOCKMAX_Q * hi, max_k=kmax,
+                                        device_id=local, prune=True)
+    parity = None
+    if rank == 0:
+        ok = parity_by_k(pkg, index, spec.k1, session, *batches[0], BLOCKMAX_KS)
+        parity = {'batch': 0, 'bit_exact': ok, 'against': 'oracle (C restatement), per K group'}
+        log(f'block-max parity vs oracle: {parity}')
+    t = time.perf_counter()
+    cap = 1024
+    trainer = pkg.Bm25Session.from_lazy(index.offsets, index.docs, index.tf, index.norm, index.idf, k1=spec.k1,
+                                        query_capacity=cap, word_capacity=cap * hi, max_k=kmax, device_id=local,
+                                        prune=True)
+    model = pkg.learned.fit(trainer, index.offsets, queries=args.blockmax_train_queries, ks=BLOCKMAX_KS, lo=lo,
+                            hi=hi, seed=args.train_seed, steps=args.train_steps, batch=4096, gen_batch=cap,
+                            target_fallback=args.target_fallback, device=f'cuda:{local}')
+    trainer.close()
+    train_s = time.perf_counter() - t
+    log(f'block-max threshold model trained in {train_s:.1f}s: {model.report}')
+    dev = []
+    for qo, w, ks in batches:
+        koff = np.zeros(BLOCKMAX_Q + 1, np.int64)
+        np.cumsum(ks, out=koff[1:])
+        dev.append(tuple(torch.from_numpy(x).cuda() for x in (qo, w, ks, koff[:-1].copy())))
+    d_s = torch.empty(BLOCKMAX_Q * kmax, dtype=torch.float32, device='cuda')
+    d_i = torch.empty(BLOCKMAX_Q * kmax, dtype=torch.int32, device='cuda')
+    d_x = torch.empty(BLOCKMAX_Q, dtype=torch.int32, device='cuda')
+    out = {'workload': BLOCKMAX_WORKLOAD, 'docs': spec.docs, 'vocab': spec.vocab, 'len_mean': spec.len_mean,
+           'postings': index.postings, 'eval_queries': BLOCKMAX_EVAL, 'queries_per_search': BLOCKMAX_Q,
+           'terms': f'U{{{lo}..{hi}}} drawn by df', 'k': 'per query from {10, 100}', 'parity': parity,
+           'model': {'train_queries': model.report['train_queries'], 'train_s': train_s, 'margin': model.margin,
+                     'val_fallback': model.report['val_fallback']}}
+    steps = n_batches  # one pass over the held-out set
+    for label, learned in (('plain', False), ('learned', True)):
+        session.set_threshold_model(model if learned else None)
+
+        def step(i):
+            o, w, k, ko = dev[i % n_batches]
+            session.search_batch_device(o.data_ptr(), w.data_ptr(), k.data_ptr(), ko.data_ptr(), BLOCKMAX_Q, kmax,
+                                        d_s.data_ptr(), d_i.data_ptr(), d_x.data_ptr(), learned,
+                                        stream.cuda_stream)
+
+        step_ms, kernel_ms, _ = timed_device(session, step, steps, args.warmup, flush, stream, world)
+        stats = session.search_stats(reset=True)
+        total = max_over_ranks(sum(step_ms), world)
+        host_ms, fallbacks = [], 0
+        for i in range(args.warmup):
+            session.search_batch(batches[i % n_batches][:2], batches[i % n_batches][2], learned=learned)
+        for i in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = session.search_batch(batches[i][:2], batches[i][2], learned=learned)
+            host_ms.append((time.perf_counter() - t0) * 1e3)
+            if learned:
+                fallbacks += int(np.sum(r[3] == 0))
+        e2e_total = max_over_ranks(sum(host_ms), world)
+        per = {key: v / steps for key, v in stats.items()}
+        out[label] = {'value': world * BLOCKMAX_Q * steps / (total / 1e3), 'unit': UNIT,
+                      'p50_ms': percentile(step_ms, 50), 'p95_ms': percentile(step_ms, 95),
+                      'main_kernel_ms_avg': sum(kernel_ms) / len(kernel_ms),
+                      'e2e': {'value': world * BLOCKMAX_Q * steps / (e2e_total / 1e3), 'unit': UNIT,
+                              'p50_ms': percentile(host_ms, 50), 'p95_ms': percentile(host_ms, 95)},
+                      'per_search': per, 'steps': steps,
+                      # postings read block by block plus postings streamed whole (8 B each)
+                      'posting_bytes_per_search': 8.0 * (per['postings_read'] + per['postings_copied'])}
+        if learned:
+            out[label]['fallback_share'] = fallbacks / BLOCKMAX_EVAL
+    out['speedup_learned_vs_plain'] = out['learned']['value'] / out['plain']['value']
+    out['e2e_speedup_learned_vs_plain'] = out['learned']['e2e']['value'] / out['plain']['e2e']['value']
+    out['posting_bytes_learned_vs_plain'] = (out['learned']['posting_bytes_per_search'] /
+                                             max(out['plain']['posting_bytes_per_search'], 1.0))
+    session.close()
+    return out
+
+
 SERVE_RATES = (5000, 10000, 20000, 50000)
 SERVE_TERMS, SERVE_KS, SERVE_POOL = (1, 16), (10, 100, 1000), 4096
 
@@ -531,6 +652,8 @@ def main():
     ap.add_argument('--target-fallback', type=float, default=0.02)
     ap.add_argument('--no-mix', action='store_true', help='skip the batched 256-query mix')
     ap.add_argument('--mix-train-queries', type=int, default=120_000)
+    ap.add_argument('--no-blockmax', action='store_true', help='skip the 4.2M-doc block-max workload')
+    ap.add_argument('--blockmax-train-queries', type=int, default=200_000)
     ap.add_argument('--serve', action='store_true', help='also run the serving loop (Poisson arrivals)')
     ap.add_argument('--serve-seconds', type=float, default=1.0)
     args = ap.parse_args()
@@ -644,10 +767,16 @@ def main():
     if info['kernel'] == 4 and args.serve and world == 1:
         serving = serve_leg(pkg, args, spec, index, local)
 
-    mix = None
-    if info['kernel'] == 4 and not args.no_mix and not (args.docs or args.vocab):
-        session.close()  # frees the 10M index before the mix corpus is resident
+    mix = blockmax = None
+    full_size = info['kernel'] == 4 and not (args.docs or args.vocab)
+    session_open = True
+    if full_size and not (args.no_mix and args.no_blockmax):
+        session.close()  # frees the 10M index before the next corpus is resident
+        session_open = False
+    if full_size and not args.no_mix:
         mix = mix_leg(pkg, args, local, world, flush, stream, rank)
+    if full_size and not args.no_blockmax:
+        blockmax = blockmax_leg(pkg, args, local, world, flush, stream, rank)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -688,12 +817,14 @@ def main():
             line['learned_pruned'] = learned
         if mix is not None:
             line['batched_mix'] = mix
+        if blockmax is not None:
+            line['blockmax_c4'] = blockmax
         if serving is not None:
             line['serving'] = serving
         if cpu is not None:
             line['cpu_baseline'] = cpu
         print(json.dumps(line), flush=True)
-    if mix is None:
+    if session_open:
         session.close()
     if world > 1:
         dist.barrier()
