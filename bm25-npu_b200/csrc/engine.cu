@@ -789,9 +789,6 @@ class Engine {
                                                "cudaMalloc word rows"));
             d_item_count_ = static_cast<unsigned *>(Alloc(4 * sizeof(unsigned), "cudaMalloc block work count"));
             d_safe_ = static_cast<float *>(Alloc(opts_.query_capacity * sizeof(float), "cudaMalloc safe bounds"));
-            Cuda(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "cudaStreamCreate");
-            Cuda(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "cudaEventCreate");
-            Cuda(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "cudaEventCreate");
             d_term_top_ = static_cast<float *>(Alloc(vocab_ * bm25k::kTermTop * sizeof(float), "cudaMalloc term top"));
             d_term_mean_ = static_cast<float *>(Alloc(vocab_ * sizeof(float), "cudaMalloc term mean"));
             d_model_ = static_cast<float *>(Alloc(bm25mlp::kParams * sizeof(float), "cudaMalloc model"));
@@ -1004,17 +1001,14 @@ class Engine {
                 Cuda(cudaMemsetAsync(d_qkept_, 0, (size_t)q * sizeof(unsigned), s), "kept count reset");
             }
             if (learned) {
-                // tau is this session's bound array, written here on a side stream so that the
-                // bounds and the plan are built at once (a fork and a join in a captured graph)
-                Cuda(cudaEventRecord(fork_, s), "cudaEventRecord");
-                Cuda(cudaStreamWaitEvent(side_, fork_, 0), "cudaStreamWaitEvent");
+                // tau is this session's bound array, written here; the plan kernel, launched
+                // overlapped, is built meanwhile and waits for these bounds before it completes
                 bm25k::LearnedArgs la = LearnedArgsFor(q, k, qoffsets, words);
                 la.kq = kq;
                 la.safe = d_safe_;
                 bm25k::LearnedBoundKernel<<<(q + bm25k::kLearnedQueries - 1) / bm25k::kLearnedQueries,
-                                            bm25k::kLearnedThreads, 0, side_>>>(la);
+                                            bm25k::kLearnedThreads, 0, s>>>(la);
                 Cuda(cudaGetLastError(), "learned bound kernel launch");
-                Cuda(cudaEventRecord(join_, side_), "cudaEventRecord");
             }
             if (tau) {
                 sa.boff = d_boff_;
@@ -1026,10 +1020,13 @@ class Engine {
                 sa.item_count = d_item_count_;
                 sa.item_cap = item_cap_;
             }
-            bm25k::PlanKernel<<<bm25k::PlanGrid(opts_.word_capacity, plan_.tiles, sms_), bm25k::kPlanThreads, 0, s>>>(sa);
-            Cuda(cudaGetLastError(), "plan kernel launch");
             if (learned)
-                Cuda(cudaStreamWaitEvent(s, join_, 0), "cudaStreamWaitEvent");
+                LaunchOverlapped(bm25k::PlanKernel, bm25k::PlanGrid(opts_.word_capacity, plan_.tiles, sms_),
+                                 bm25k::kPlanThreads, 0, s, sa);
+            else
+                bm25k::PlanKernel<<<bm25k::PlanGrid(opts_.word_capacity, plan_.tiles, sms_), bm25k::kPlanThreads, 0,
+                                    s>>>(sa);
+            Cuda(cudaGetLastError(), "plan kernel launch");
             const long long claims = (long long)q * ((plan_.tiles + bm25k::kWgWarps - 1) / bm25k::kWgWarps);
             const int wg_grid = (int)std::max<long long>(1, std::min<long long>(plan_.grid, claims));
             auto tile_group = [&](const bm25k::StreamArgs &args) {
@@ -1272,14 +1269,6 @@ class Engine {
             cudaFreeHost(h_out_);
         h_in_ = h_out_ = nullptr;
         DestroyTiming();
-        if (fork_)
-            cudaEventDestroy(fork_);
-        if (join_)
-            cudaEventDestroy(join_);
-        if (side_)
-            cudaStreamDestroy(side_);
-        fork_ = join_ = nullptr;
-        side_ = nullptr;
         if (done_)
             cudaEventDestroy(done_);
         done_ = nullptr;
@@ -1311,8 +1300,6 @@ class Engine {
     uint4 *d_items_ = nullptr;
     int *d_wrow_ = nullptr;
     float *d_safe_ = nullptr;
-    cudaStream_t side_ = nullptr;  // the learned bounds run beside the plan
-    cudaEvent_t fork_ = nullptr, join_ = nullptr;
     unsigned *d_item_count_ = nullptr;
     long long item_cap_ = 0;
     size_t bs_smem_ = 0;

@@ -227,6 +227,7 @@ __global__ void __launch_bounds__(kLearnedThreads) LearnedBoundKernel(const Lear
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = tid / kH, i = tid % kH;  // query slot in the CTA, hidden unit
     const int q0 = blockIdx.x * kLearnedQueries;
+    AllowDependents();  // the plan kernel is built meanwhile (it reads none of this kernel's output)
     if (a.params) {
         const float *p = a.params;
         for (int x = tid; x < kH * kIn; x += kLearnedThreads)

@@ -184,14 +184,6 @@ struct StreamShared {
 
 __device__ __forceinline__ unsigned SmemAddr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
-// Programmatic dependent launch.  A kernel launched with programmatic stream serialization may
-// start while the kernel before it in the stream still runs: it waits in WaitPrerequisites
-// (until that kernel has completed and its writes are visible) before reading anything that
-// kernel wrote.  AllowDependents lets the next such kernel start early.  Both are no-ops when
-// no launch in the stream uses the attribute.
-__device__ __forceinline__ void WaitPrerequisites() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void AllowDependents() { asm volatile("griddepcontrol.launch_dependents;" :::); }
-
 __device__ __forceinline__ void MbarInit(unsigned long long *bar, unsigned count)
 {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(SmemAddr(bar)), "r"(count) : "memory");
@@ -513,8 +505,10 @@ __global__ void __launch_bounds__(kPlanThreads) PlanKernel(const StreamArgs a)
     }
     const int t0 = (int)blockIdx.y * kPlanTileChunk;
     const int t1 = min(a.tiles, t0 + kPlanTileChunk);
-    if (t0 >= t1)
+    if (t0 >= t1) {
+        WaitPrerequisites();  // completes only after the kernel before it (the learned bounds)
         return;
+    }
     const int tid = threadIdx.x;
     for (long long w = blockIdx.x; w < total; w += gridDim.x) {
         const int term = a.words[w];
@@ -604,6 +598,9 @@ __global__ void __launch_bounds__(kPlanThreads) PlanKernel(const StreamArgs a)
         }
         __syncthreads();  // range[] is rewritten for the next word
     }
+    // launched overlapped after the learned bounds: complete only after them, so that every
+    // kernel waiting for this one sees the bounds too
+    WaitPrerequisites();
 }
 
 // Grid of PlanKernel for a batch capacity of `words` query words.

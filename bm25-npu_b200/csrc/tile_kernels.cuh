@@ -87,6 +87,14 @@ struct TileShared {
     int last;
 };
 
+// Programmatic dependent launch.  A kernel launched with programmatic stream serialization may
+// start while the kernel before it in the stream still runs: it waits in WaitPrerequisites
+// (until that kernel has completed and its writes are visible) before reading anything that
+// kernel wrote.  AllowDependents lets the next such kernel start early.  Both are no-ops when
+// no launch in the stream uses the attribute.
+__device__ __forceinline__ void WaitPrerequisites() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void AllowDependents() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
 __device__ __forceinline__ bool Better(float as, int ai, float bs, int bi)
 {
     return as > bs || (as == bs && ai < bi);
