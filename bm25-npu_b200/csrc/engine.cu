@@ -862,7 +862,7 @@ class Engine {
             const size_t qc = (size_t)opts_.query_capacity, tiles_z = (size_t)plan_.tiles;
             // worst case for K <= 32: every selection of every tile appends max_k candidates.  For
             // K > 32 a tile appends every document at or above the running bound; the buffer holds
-            // 512 K (at least 2^19) and a query that overflows it is searched again from its final
+            // 512 K (at least 2^18) and a query that overflows it is searched again from its final
             // bound by the retry pass.
             cand_cap_ = (long long)tiles_z * per_tile;
             if (opts_.max_k > bm25k::kMaxSmallK) {
@@ -871,7 +871,7 @@ class Engine {
                       "candidate_capacity must be 0 or at least max_k");
                 cand_cap_ = std::min<long long>(cand_cap_, opts_.candidate_capacity
                                                                ? opts_.candidate_capacity
-                                                               : std::max<long long>(1 << 19, 512LL * opts_.max_k));
+                                                               : std::max<long long>(1 << 18, 512LL * opts_.max_k));
             }
             cand_cap_ = (cand_cap_ + 3) & ~3LL;  // rows start on 16-byte boundaries (128-bit reads)
             if (opts_.prune || opts_.max_k > bm25k::kMaxSmallK) {
