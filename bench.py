@@ -325,7 +325,9 @@ def learned_leg(pkg, args, spec, index, session, sets, want, flush, stream, dev_
                     'p50_ms': percentile(host_ms, 50), 'p95_ms': percentile(host_ms, 95),
                     'path': 'bm25_search_learned (C ABI, host buffers): one graph replay'},
             'fallback_share': fallbacks / (Q * args.steps),
-            'gpu_launches': args.steps * 7,  # bound, plan, seed, pruned pass, select, retry pass, retry select
+            # learned bounds, plan, block bound, block score, final select, then the retry pass's block
+            # bound, block score and final select (an empty list ends them at once)
+            'gpu_launches': args.steps * 8,
             'per_search': {key: v / args.steps for key, v in stats.items()},
             'bit_exact_vs_oracle': parity if want is not None else None,
         }
