@@ -469,6 +469,17 @@ def parity_by_k(pkg, index, k1, session, qo, w, ks, kset):
     return ok
 
 
+def split_queries(qoffsets, words, ks, per_search):
+    """Packed queries (offsets [Q+1], words) with a K each, cut into Searches of per_search queries
+    (the last one shorter when Q is not a multiple): a list of (offsets from 0, words, ks)."""
+    out = []
+    for a0 in range(0, qoffsets.size - 1, per_search):
+        a1 = min(a0 + per_search, qoffsets.size - 1)
+        out.append(((qoffsets[a0:a1 + 1] - qoffsets[a0]).astype(np.int64),
+                    words[qoffsets[a0]:qoffsets[a1]].copy(), ks[a0:a1].copy()))
+    return out
+
+
 def blockmax_leg(pkg, args, local, world, flush, stream, rank):
     """The block-max workload: 4.2M docs (V 1M, mean length 80), a threshold model trained on
     200k queries, then 10k held-out queries of 2-10 terms drawn by df with K drawn from {10, 100}
@@ -480,14 +491,10 @@ def blockmax_leg(pkg, args, local, world, flush, stream, rank):
     index = pkg.synthetic_index(spec)
     log(f'block-max corpus: N={index.num_docs} V={index.vocab} M={index.postings} in {time.perf_counter() - t:.1f}s')
     lo, hi = BLOCKMAX_TERMS
-    n_batches = BLOCKMAX_EVAL // BLOCKMAX_Q
     qo_all, w_all = pkg.synthetic_queries(index.offsets, BLOCKMAX_EVAL, lo, hi, 440000 + 1000 * rank)
     ks_all = np.random.default_rng(550 + 1000 * rank).choice(BLOCKMAX_KS, BLOCKMAX_EVAL).astype(np.int32)
-    batches = []
-    for b in range(n_batches):
-        a0, a1 = b * BLOCKMAX_Q, (b + 1) * BLOCKMAX_Q
-        qo = (qo_all[a0:a1 + 1] - qo_all[a0]).astype(np.int64)
-        batches.append((qo, w_all[qo_all[a0]:qo_all[a1]].copy(), ks_all[a0:a1].copy()))
+    batches = split_queries(qo_all, w_all, ks_all, BLOCKMAX_Q)
+    n_batches = len(batches)
     kmax = max(BLOCKMAX_KS)
     session = pkg.Bm25Session.from_lazy(index.offsets, index.docs, index.tf, index.norm, index.idf, k1=spec.k1,
                                         query_capacity=BLOCKMAX_Q, word_capacity=BLOCKMAX_Q * hi, max_k=kmax,
