@@ -649,7 +649,8 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--tile-docs', type=int, default=0)
     ap.add_argument('--fan-in', type=int, default=0)
-    ap.add_argument('--kernel', type=int, default=4, help='0 streaming, 1 one CTA per (query, tile), 4 tile groups')
+    ap.add_argument('--kernel', type=int, default=5,
+                    help='0 streaming, 1 one CTA per (query, tile), 4 tile groups, 5 warp tiles')
     ap.add_argument('--stages', type=int, default=0)
     ap.add_argument('--chunk', type=int, default=0, help='postings per ring stage of the tile-group kernel')
     ap.add_argument('--docs', type=int, default=0, help='reduced corpus for profiling captures (not a bench line)')
@@ -688,7 +689,7 @@ def main():
                                         query_capacity=Q, word_capacity=Q * TERMS, max_k=K, device_id=local,
                                         tile_docs=args.tile_docs, merge_fan_in=args.fan_in, kernel=args.kernel,
                                         ring_stages=args.stages, ring_chunk=args.chunk,
-                                        prune=args.kernel == 4 and not args.no_learned)
+                                        prune=args.kernel in (4, 5) and not args.no_learned)
     info = session.info()
     log(f'engine ready in {time.perf_counter() - t:.1f}s: {info}')
 
@@ -761,23 +762,24 @@ def main():
     launches_per_search = 1 if info['kernel'] == 1 else 3
     peak, peak_kind = hbm_peak()
     traffic = traffic_from_profile({0: 'stream_search_kernel_synthetic_10m.txt',
-                                    4: 'tile_group_kernel_synthetic_10m.txt'}.get(info['kernel'], '-'))
+                                    4: 'tile_group_kernel_synthetic_10m.txt',
+                                    5: 'warp_tile_kernel_synthetic_10m.txt'}.get(info['kernel'], '-'))
     if args.docs or args.vocab:
         traffic = None  # the profiles cover the full-size workload
 
     learned = None
-    if info['kernel'] == 4 and not args.no_learned:
+    if info['kernel'] in (4, 5) and not args.no_learned:
         learned = learned_leg(pkg, args, spec, index, session, sets, want, flush, stream, dev_sets, local, world)
         learned['speedup_vs_plain'] = learned['learned']['value'] / value
         learned['e2e_speedup_vs_plain'] = learned['learned']['e2e']['value'] / e2e_value
         learned['plain_per_search'] = {key: v / args.steps for key, v in plain_stats.items()}
 
     serving = None
-    if info['kernel'] == 4 and args.serve and world == 1:
+    if info['kernel'] in (4, 5) and args.serve and world == 1:
         serving = serve_leg(pkg, args, spec, index, local)
 
     mix = blockmax = None
-    full_size = info['kernel'] == 4 and not (args.docs or args.vocab)
+    full_size = info['kernel'] in (4, 5) and not (args.docs or args.vocab)
     session_open = True
     if full_size and not (args.no_mix and args.no_blockmax):
         session.close()  # frees the 10M index before the next corpus is resident
@@ -817,7 +819,7 @@ def main():
                          'kernel_share_of_step': sum(kernel_ms) / sum(step_ms),
                          'search_achieved_gbs': search_achieved,
                          'kernel': {0: 'bm25k::StreamSearchKernel', 1: 'bm25k::TileSearchKernel',
-                       4: 'bm25k::TileGroupKernel'}[info['kernel']]},
+                                    4: 'bm25k::TileGroupKernel', 5: 'bm25k::WarpTileKernel'}[info['kernel']]},
             'gpu_launches': args.steps * launches_per_search,
             'clocks': clock_info,
             'parity': parity,

@@ -20,7 +20,7 @@ NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
 ENGINE_SOURCES = ['engine.cu', 'mlp.cu', 'serve.cpp', 'builder.cu']
-ENGINE_HEADERS = ['tile_kernels.cuh', 'stream_kernel.cuh', 'tile_group_kernel.cuh', 'block_kernels.cuh',
+ENGINE_HEADERS = ['tile_kernels.cuh', 'stream_kernel.cuh', 'tile_group_kernel.cuh', 'warp_tile_kernel.cuh', 'block_kernels.cuh',
                   'learned_kernels.cuh', 'mlp.cuh', 'merge_kernel.cuh']
 
 

@@ -15,6 +15,7 @@
 #include "stream_kernel.cuh"
 #include "tile_group_kernel.cuh"
 #include "tile_kernels.cuh"
+#include "warp_tile_kernel.cuh"
 
 #include <cuda_runtime.h>
 #include <omp.h>
@@ -71,6 +72,14 @@ static void RaiseSmemCap(const void *kernel, size_t bytes)
 }
 
 static size_t Align32(size_t n) { return (n + 31) & ~size_t(31); }
+
+// The kernels with 1024-document tiles, a K per query, K up to 1024 and the pruned paths: the
+// warp-tile kernel (plain Searches; pruned Searches stream their routed and retried queries with
+// the tile-group kernel) and the tile-group kernel.
+static bool TileFamily(int kernel) { return kernel == BM25_KERNEL_TILE_GROUP || kernel == BM25_KERNEL_WARP_TILE; }
+
+// Tiles per claim of the warp-tile kernel.
+constexpr int kWtClaimTiles = 4;
 
 // Launch with programmatic stream serialization: the kernel may start while the kernel before it
 // in the stream runs (the kernel waits in WaitPrerequisites before reading that kernel's output).
@@ -177,12 +186,12 @@ class Engine {
         : opts_(o), vocab_(vocab), docs_(docs), postings_(postings)
     {
         Check(o.max_k >= 1 && o.max_k <= bm25k::kLargeMaxK, "max_k must be in [1, 1024]");
-        Check(o.max_k <= bm25k::kMaxSmallK || o.kernel == BM25_KERNEL_TILE_GROUP,
-              "max_k above 32 needs the tile-group kernel");
+        Check(o.max_k <= bm25k::kMaxSmallK || TileFamily(o.kernel),
+              "max_k above 32 needs the warp-tile or tile-group kernel");
         Check(o.max_k <= docs, "max_k exceeds the document count");
         Check(o.query_capacity >= 1 && o.query_capacity <= 65535, "query_capacity must be in [1, 65535]");
         Check(o.word_capacity >= 0 && o.word_capacity <= 16777216, "word_capacity must be in [0, 2^24]");
-        Check(!o.prune || o.kernel == BM25_KERNEL_TILE_GROUP, "prune needs the tile-group kernel");
+        Check(!o.prune || TileFamily(o.kernel), "prune needs the warp-tile or tile-group kernel");
         Cuda(cudaSetDevice(o.device_id), "cudaSetDevice");
         device_ = o.device_id;
         size_t total = 0;
@@ -372,7 +381,7 @@ class Engine {
         RequireUsable();
         if (learned)
             RequirePrune();
-        Check(plan_.kernel == BM25_KERNEL_TILE_GROUP, "A K per query needs the tile-group kernel");
+        Check(TileFamily(plan_.kernel), "A K per query needs the warp-tile or tile-group kernel");
         Check(ks && out_scores && out_ids && (!learned || out_exact), "Null buffer");
         Check(q >= 1 && q <= opts_.query_capacity, "Query batch exceeds declared capacity or is empty");
         int kmax = 1;
@@ -441,7 +450,7 @@ class Engine {
         RequireUsable();
         if (learned)
             RequirePrune();
-        Check(plan_.kernel == BM25_KERNEL_TILE_GROUP, "A K per query needs the tile-group kernel");
+        Check(TileFamily(plan_.kernel), "A K per query needs the warp-tile or tile-group kernel");
         Check(q >= 1 && q <= opts_.query_capacity, "Query batch exceeds declared capacity or is empty");
         Check(kmax >= 1 && kmax <= opts_.max_k && kmax <= docs_, "K outside [1, min(max_k, N)]");
         Check(qoffsets && words && ks && kout && out_scores && out_ids && (!learned || out_exact), "Null device buffer");
@@ -640,8 +649,9 @@ class Engine {
   private:
     void RequirePrune() const
     {
-        if (!opts_.prune || plan_.kernel != BM25_KERNEL_TILE_GROUP)
-            throw InvalidState("Pruned Search needs a session created with prune = 1 and the tile-group kernel");
+        if (!opts_.prune || !TileFamily(plan_.kernel))
+            throw InvalidState("Pruned Search needs a session created with prune = 1 and the warp-tile or tile-group "
+                               "kernel");
     }
 
     void RequireUsable() const
@@ -662,11 +672,15 @@ class Engine {
     void MakePlan()
     {
         Check(opts_.kernel == BM25_KERNEL_STREAM || opts_.kernel == BM25_KERNEL_PER_TILE ||
-                  opts_.kernel == BM25_KERNEL_TILE_GROUP,
-              "kernel must be 0 (streaming), 1 (per-tile) or 4 (tile groups)");
+                  TileFamily(opts_.kernel),
+              "kernel must be 0 (streaming), 1 (per-tile), 4 (tile groups) or 5 (warp tiles)");
         plan_.kernel = opts_.kernel;
         int t = opts_.tile_docs;
-        if (plan_.kernel == 4) {
+        if (plan_.kernel == BM25_KERNEL_WARP_TILE) {
+            Check(t == 0 || t == bm25k::kWtTile, "tile_docs of the warp-tile kernel must be 1024");
+            Check(postings_ + kPad < INT32_MAX, "Posting count exceeds the INT32 contract");
+            t = bm25k::kWtTile;
+        } else if (plan_.kernel == BM25_KERNEL_TILE_GROUP) {
             Check(t == 0 || t == 1024 || t == 2048, "tile_docs of the tile-group kernel must be 1024 or 2048");
             Check(postings_ + kPad < INT32_MAX, "Posting count exceeds the INT32 contract");
             t = t ? t : bm25k::kWgTileDocs;
@@ -676,7 +690,7 @@ class Engine {
             while (t < per_sm && t < (plan_.kernel == 0 ? 8192 : 16384))
                 t <<= 1;
         }
-        Check(plan_.kernel == 4 || (t >= 2048 && t <= 32768 && (t & (t - 1)) == 0),
+        Check(TileFamily(plan_.kernel) || (t >= 2048 && t <= 32768 && (t & (t - 1)) == 0),
               "tile_docs must be a power of two in [2048, 32768]");
         plan_.tile_docs = t;
         plan_.tiles = (int)((docs_ + t - 1) / t);
@@ -700,10 +714,11 @@ class Engine {
         plan_.levels = (int)plan_.lists.size();
         if (plan_.kernel != 1) {
             // tile-group kernel: 3 stages of 1536 postings keep 3 CTAs on an SM (measured best at 10M docs)
-            const int st = opts_.ring_stages ? opts_.ring_stages : (plan_.kernel == BM25_KERNEL_TILE_GROUP ? 3 : 4);
+            // (the warp-tile kernel has no ring; its pruned Searches stream with the tile-group kernel)
+            const int st = opts_.ring_stages ? opts_.ring_stages : (TileFamily(plan_.kernel) ? 3 : 4);
             Check(st >= 2 && st <= bm25k::kMaxStages, "ring_stages must be in [2, 8]");
             plan_.stages = st;
-            if (plan_.kernel == BM25_KERNEL_TILE_GROUP) {
+            if (TileFamily(plan_.kernel)) {
                 const int c = opts_.ring_chunk ? opts_.ring_chunk : 1536;
                 Check(c >= bm25k::kWgChunkMin && c <= bm25k::kWgChunkMax && c % 4 == 0,
                       "ring_chunk must be a multiple of 4 in [512, 4096]");
@@ -845,12 +860,28 @@ class Engine {
                 threads = bm25k::kStreamThreads;
                 per_tile = (long long)bm25k::kConsumerWarps * opts_.max_k;  // every warp region
             } else {
-                smem_bytes_ = bm25k::TileGroupSmem(plan_.stages, plan_.chunk, plan_.tile_docs);
+                // the tile-group kernel: the main kernel of kernel 4; with kernel 5 it streams the
+                // routed and retried queries of pruned Searches
+                tg_smem_ = bm25k::TileGroupSmem(plan_.stages, plan_.chunk, plan_.tile_docs);
                 kernel = bm25k::TileGroupKernelFor(plan_.tile_docs);
-                RaiseSmemCap(bm25k::TileGroupKernelFor(plan_.tile_docs, true),
-                             bm25k::TileGroupSmem(plan_.stages, plan_.chunk, plan_.tile_docs));
+                RaiseSmemCap(bm25k::TileGroupKernelFor(plan_.tile_docs, true), tg_smem_);
+                RaiseSmemCap(kernel, tg_smem_);
+                int tg_per_sm = 0, n_sms = 0;
+                Cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tg_per_sm, kernel, bm25k::kWgThreads, tg_smem_),
+                     "occupancy");
+                Check(tg_per_sm >= 1, "tile_docs / ring_stages exceed the shared memory of one SM");
+                Cuda(cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, device_), "SM count");
+                tg_grid_ = tg_per_sm * n_sms;
+                smem_bytes_ = tg_smem_;
                 threads = bm25k::kWgThreads;
                 per_tile = opts_.max_k;
+                if (plan_.kernel == BM25_KERNEL_WARP_TILE) {
+                    smem_bytes_ = bm25k::WarpTileSmem();
+                    for (const bool lean : {true, false})
+                        RaiseSmemCap(bm25k::WarpTileKernelFor<kWtClaimTiles>(lean), smem_bytes_);
+                    kernel = bm25k::WarpTileKernelFor<kWtClaimTiles>(false);
+                    threads = bm25k::kWtThreads;
+                }
             }
             RaiseSmemCap(kernel, smem_bytes_);
             int per_sm = 0, sms = 0;
@@ -898,8 +929,13 @@ class Engine {
             cand_count_ = static_cast<unsigned *>(Alloc(qc * sizeof(unsigned), "cudaMalloc cand count"));
             cand_scores_ = static_cast<float *>(Alloc(qc * cand_cap_ * sizeof(float), "cudaMalloc candidates"));
             cand_ids_ = static_cast<int *>(Alloc(qc * cand_cap_ * sizeof(int), "cudaMalloc candidates"));
-            plan_entries_ = static_cast<bm25k::PlanEntry *>(
-                Alloc(std::max<size_t>(1, opts_.word_capacity) * tiles_z * sizeof(bm25k::PlanEntry), "cudaMalloc plan"));
+            if (plan_.kernel != BM25_KERNEL_WARP_TILE || opts_.prune)
+                plan_entries_ = static_cast<bm25k::PlanEntry *>(Alloc(
+                    std::max<size_t>(1, opts_.word_capacity) * tiles_z * sizeof(bm25k::PlanEntry), "cudaMalloc plan"));
+            if (plan_.kernel == BM25_KERNEL_WARP_TILE)
+                plan_rows_ = static_cast<int *>(Alloc(std::max<size_t>(1, opts_.word_capacity) * (tiles_z + 1) *
+                                                          sizeof(int),
+                                                      "cudaMalloc plan rows"));
             Cuda(cudaMemset(ctrl_, 0, sizeof(bm25k::StreamCtrl)), "cudaMemset");
             d_stats_ = static_cast<unsigned long long *>(Alloc(bm25k::kStats * sizeof(unsigned long long), "cudaMalloc stats"));
             Cuda(cudaMemset(d_stats_, 0, bm25k::kStats * sizeof(unsigned long long)), "cudaMemset");
@@ -971,7 +1007,7 @@ class Engine {
             sa.out_scores = out_scores;
             sa.out_ids = out_ids;
             sa.status = status;
-            sa.stats = plan_.kernel == BM25_KERNEL_TILE_GROUP ? d_stats_ : nullptr;
+            sa.stats = TileFamily(plan_.kernel) ? d_stats_ : nullptr;
             // the retry pass answers the queries on the fail list: those whose starting bound proved
             // too high, and (K > 32) those whose candidate buffer overflowed
             // a batch with a K per query (kq): k is its largest K, each final select takes its queries
@@ -1020,7 +1056,15 @@ class Engine {
                 sa.item_count = d_item_count_;
                 sa.item_cap = item_cap_;
             }
-            if (learned)
+            // plain Searches of a warp-tile session: plan rows of the words without a directory row,
+            // then the warp-tile kernel; every other Search: the (query word, tile) plan
+            const bool warp_tile = plan_.kernel == BM25_KERNEL_WARP_TILE && !tau;
+            sa.plan_rows = plan_rows_;
+            sa.prefetch = 1;
+            if (warp_tile)
+                bm25k::PlanRowsKernel<<<bm25k::PlanRowsGrid(opts_.word_capacity, plan_.tiles, sms_),
+                                        bm25k::kPlanThreads, 0, s>>>(sa);
+            else if (learned)
                 LaunchOverlapped(bm25k::PlanKernel, bm25k::PlanGrid(opts_.word_capacity, plan_.tiles, sms_),
                                  bm25k::kPlanThreads, 0, s, sa);
             else
@@ -1028,20 +1072,31 @@ class Engine {
                                     s>>>(sa);
             Cuda(cudaGetLastError(), "plan kernel launch");
             const long long claims = (long long)q * ((plan_.tiles + bm25k::kWgWarps - 1) / bm25k::kWgWarps);
-            const int wg_grid = (int)std::max<long long>(1, std::min<long long>(plan_.grid, claims));
+            const int wg_grid = (int)std::max<long long>(1, std::min<long long>(tg_grid_, claims));
+            const long long wt_claims = (long long)q * ((plan_.tiles + kWtClaimTiles - 1) / kWtClaimTiles);
+            const int wt_grid = (int)std::max<long long>(
+                1, std::min<long long>(plan_.grid, (wt_claims + bm25k::kWtWarps - 1) / bm25k::kWtWarps));
             auto tile_group = [&](const bm25k::StreamArgs &args) {
                 const bool lean = !args.retry && !args.kq && k <= bm25k::kMaxSmallK;
-                if (plan_.tile_docs == 2048) {
-                    if (lean)
-                        bm25k::TileGroupKernel<2048, true><<<wg_grid, bm25k::kWgThreads, smem_bytes_, s>>>(args);
+                if (warp_tile) {
+                    if (!args.retry)  // right after the plan rows: set up while they are built
+                        LaunchOverlapped(lean ? bm25k::WarpTileKernel<kWtClaimTiles, true>
+                                              : bm25k::WarpTileKernel<kWtClaimTiles, false>,
+                                         wt_grid, bm25k::kWtThreads, smem_bytes_, s, args);
                     else
-                        bm25k::TileGroupKernel<2048><<<wg_grid, bm25k::kWgThreads, smem_bytes_, s>>>(args);
+                        bm25k::WarpTileKernel<kWtClaimTiles, false><<<wt_grid, bm25k::kWtThreads, smem_bytes_, s>>>(
+                            args);
+                } else if (plan_.tile_docs == 2048) {
+                    if (lean)
+                        bm25k::TileGroupKernel<2048, true><<<wg_grid, bm25k::kWgThreads, tg_smem_, s>>>(args);
+                    else
+                        bm25k::TileGroupKernel<2048><<<wg_grid, bm25k::kWgThreads, tg_smem_, s>>>(args);
                 } else {
                     if (lean)  // right after the plan kernel: set up while it runs
-                        LaunchOverlapped(bm25k::TileGroupKernel<1024, true>, wg_grid, bm25k::kWgThreads, smem_bytes_,
-                                         s, args);
+                        LaunchOverlapped(bm25k::TileGroupKernel<1024, true>, wg_grid, bm25k::kWgThreads, tg_smem_, s,
+                                         args);
                     else
-                        bm25k::TileGroupKernel<1024><<<wg_grid, bm25k::kWgThreads, smem_bytes_, s>>>(args);
+                        bm25k::TileGroupKernel<1024><<<wg_grid, bm25k::kWgThreads, tg_smem_, s>>>(args);
                 }
             };
             auto final_select = [&](const bm25k::StreamArgs &args) {
@@ -1313,6 +1368,9 @@ class Engine {
     int *cand_ids_ = nullptr;
     long long cand_cap_ = 0;
     bm25k::PlanEntry *plan_entries_ = nullptr;
+    int *plan_rows_ = nullptr;
+    size_t tg_smem_ = 0;  // tile-group kernel: dynamic shared memory and grid
+    int tg_grid_ = 0;
     int sms_ = 148;
     std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs_;
     float *d_term_top_ = nullptr, *d_term_mean_ = nullptr, *d_model_ = nullptr, *d_tau_ = nullptr;
@@ -1404,7 +1462,7 @@ void bm25_default_options(bm25_options *o)
     o->max_k = 10;
     o->query_capacity = 8;
     o->word_capacity = 24;
-    o->kernel = BM25_KERNEL_TILE_GROUP;
+    o->kernel = BM25_KERNEL_WARP_TILE;
 }
 
 int bm25_create(const int64_t *indptr, const int32_t *indices, const float *data, int64_t vocab, int64_t num_docs,
@@ -1766,6 +1824,20 @@ struct StaticDevice {
 };
 std::mutex g_static_mutex;
 StaticDevice g_static_devices[64];
+// Host word each device's status is copied into: page-locked once per device at set-up
+// (cudaHostRegister of this static array; nothing is allocated), so the copy is a plain DMA.
+alignas(4096) unsigned g_static_status[64][1024];
+
+// Puts the caller's current device back on every exit of the allocation-free Search.
+struct DeviceRestore {
+    int device = -1;
+    DeviceRestore() { (void)cudaGetDevice(&device); }
+    ~DeviceRestore()
+    {
+        if (device >= 0)
+            (void)cudaSetDevice(device);
+    }
+};
 
 size_t AlignUp(size_t n, size_t a) { return (n + a - 1) / a * a; }
 size_t StaticSmem(int tile_docs)
@@ -1797,8 +1869,47 @@ void StaticSetup(int device, StaticDevice &d)
                        "occupancy");
         d.grid[i] = std::max(1, per_sm) * d.sms;
     }
+    const cudaError_t reg = cudaHostRegister(g_static_status[device], sizeof(g_static_status[device]),
+                                             cudaHostRegisterDefault);
+    if (reg != cudaSuccess && reg != cudaErrorHostMemoryAlreadyRegistered)
+        bm25b200::Cuda(reg, "cudaHostRegister(static status word)");
     d.scratch = static_cast<unsigned char *>(ptr);
     d.ready = true;
+}
+
+// Scratch layout of one Search: head | threshold[q] | cand_count[q] | slots[q][32] |
+// cand_scores[q][cap] | cand_ids[q][cap] | plan[num_words][tiles]; everything before cand_scores
+// starts at zero.
+struct StaticLayout {
+    long long cand_cap;
+    size_t off_thr, off_cnt, off_slots, off_cs, off_ci, off_plan, need;
+};
+StaticLayout StaticLayoutFor(int64_t q, int k, int64_t num_words, int64_t tiles)
+{
+    StaticLayout l;
+    l.cand_cap = tiles * bm25k::kConsumerWarps * k;
+    l.off_thr = kStaticHeadBytes;
+    l.off_cnt = AlignUp(l.off_thr + (size_t)q * 4, 16);
+    l.off_slots = AlignUp(l.off_cnt + (size_t)q * 4, 16);
+    l.off_cs = AlignUp(l.off_slots + (size_t)q * 32 * 4, 16);
+    l.off_ci = AlignUp(l.off_cs + (size_t)q * l.cand_cap * 4, 16);
+    l.off_plan = AlignUp(l.off_ci + (size_t)q * l.cand_cap * 4, 16);
+    l.need = l.off_plan + (size_t)std::max<int64_t>(1, num_words) * tiles * sizeof(bm25k::PlanEntry);
+    return l;
+}
+
+// Tile of the streaming kernel for num_docs on `sms` SMs: the smallest power of two from 2048 that
+// gives each SM at most one tile, capped at 8192.
+int StaticTile(int64_t num_docs, int sms, int *index)
+{
+    int tile = 2048, ti = 0;
+    const int64_t per_sm = (num_docs + sms - 1) / sms;
+    while (tile < per_sm && tile < 8192) {
+        tile <<= 1;
+        ++ti;
+    }
+    *index = ti;
+    return tile;
 }
 } // namespace
 
@@ -1819,27 +1930,18 @@ extern "C" int bm25_search_csc_static(const int64_t *indptr, const int32_t *indi
             Check(q >= 1 && q <= 65535 && num_words >= 0 && num_words <= 16777216, "Query batch out of range");
             Check(k >= 1 && k <= bm25k::kMaxSmallK && k <= num_docs, "K outside [1, min(32, N)]");
             Check(device_id >= 0 && device_id < 64, "device_id out of range");
-            int tile = 2048, ti = 0;
-            const int64_t per_sm = (num_docs + 147) / 148;
-            while (tile < per_sm && tile < 8192) {
-                tile <<= 1;
-                ++ti;
-            }
-            const int64_t tiles = (num_docs + tile - 1) / tile;
-            const long long cand_cap = tiles * bm25k::kConsumerWarps * k;
-            // scratch layout: head | threshold[q] | cand_count[q] | slots[q][32] | cand_scores[q][cap] |
-            // cand_ids[q][cap] | plan; everything before cand_scores starts at zero
-            const size_t off_thr = kStaticHeadBytes;
-            const size_t off_cnt = AlignUp(off_thr + (size_t)q * 4, 16);
-            const size_t off_slots = AlignUp(off_cnt + (size_t)q * 4, 16);
-            const size_t off_cs = AlignUp(off_slots + (size_t)q * 32 * 4, 16);
-            const size_t off_ci = AlignUp(off_cs + (size_t)q * cand_cap * 4, 16);
-            const size_t off_plan = AlignUp(off_ci + (size_t)q * cand_cap * 4, 16);
-            const size_t need = off_plan + (size_t)std::max<int64_t>(1, num_words) * tiles * sizeof(bm25k::PlanEntry);
-            if (need > kStaticScratchBytes)
-                throw bm25b200::InvalidArgument("Search needs " + std::to_string(need) +
-                                                " bytes of scratch; the allocation-free path holds " +
-                                                std::to_string(kStaticScratchBytes));
+            // The need falls as the tile grows: with the largest tile first, so a Search that can never
+            // fit is rejected before any CUDA call, then with the device's own tile.
+            const auto check_need = [&](int64_t tiles) {
+                const StaticLayout l = StaticLayoutFor(q, k, num_words, tiles);
+                if (l.need > kStaticScratchBytes)
+                    throw bm25b200::InvalidArgument("Search needs " + std::to_string(l.need) +
+                                                    " bytes of scratch; the allocation-free path holds " +
+                                                    std::to_string(kStaticScratchBytes));
+                return l;
+            };
+            check_need((num_docs + 8191) / 8192);
+            const DeviceRestore restore;
             Cuda(cudaSetDevice(device_id), "cudaSetDevice");
             StaticDevice *dev;
             {
@@ -1847,6 +1949,13 @@ extern "C" int bm25_search_csc_static(const int64_t *indptr, const int32_t *indi
                 dev = &g_static_devices[device_id];
                 StaticSetup(device_id, *dev);
             }
+            int ti = 0;
+            const int tile = StaticTile(num_docs, dev->sms, &ti);
+            const int64_t tiles = (num_docs + tile - 1) / tile;
+            const StaticLayout layout = check_need(tiles);
+            const long long cand_cap = layout.cand_cap;
+            const size_t off_thr = layout.off_thr, off_cnt = layout.off_cnt, off_slots = layout.off_slots,
+                         off_cs = layout.off_cs, off_ci = layout.off_ci, off_plan = layout.off_plan;
             StaticRaiseSmem(StaticSmem(tile));
             unsigned char *base = dev->scratch;
             cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1886,9 +1995,11 @@ extern "C" int bm25_search_csc_static(const int64_t *indptr, const int32_t *indi
             Cuda(cudaGetLastError(), "stream kernel launch");
             bm25k::FinalSelectKernel<<<(int)q, bm25k::kFinalThreads, 0, s>>>(sa);
             Cuda(cudaGetLastError(), "final kernel launch");
-            unsigned status = 0;
-            Cuda(cudaMemcpyAsync(&status, sa.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "status D2H");
+            volatile unsigned *slot = g_static_status[device_id];
+            Cuda(cudaMemcpyAsync(g_static_status[device_id], sa.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s),
+                 "status D2H");
             Cuda(cudaStreamSynchronize(s), "complete static Search");
+            const unsigned status = *slot;
             if (status && !(status & ~(unsigned)(bm25k::kStatusBadWord | bm25k::kStatusBadQuery)))
                 throw bm25b200::InvalidArgument("Invalid word ID or query offsets in the device query packet, status=" +
                                                 std::to_string(status));

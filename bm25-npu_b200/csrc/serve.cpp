@@ -234,8 +234,8 @@ int bm25_server_create(bm25_handle *h, const bm25_server_options *options, bm25_
         o = *options;
     if (o.max_batch < 1 || o.max_batch > info.query_capacity)
         return Fail(BM25_ERR_INVALID_PARAM, "max_batch must be in [1, query_capacity]");
-    if (info.kernel != BM25_KERNEL_TILE_GROUP)
-        return Fail(BM25_ERR_INVALID_PARAM, "The server needs a tile-group session (a K per query)");
+    if (info.kernel != BM25_KERNEL_TILE_GROUP && info.kernel != BM25_KERNEL_WARP_TILE)
+        return Fail(BM25_ERR_INVALID_PARAM, "The server needs a warp-tile or tile-group session (a K per query)");
     if (o.learned && !info.prune)
         return Fail(BM25_ERR_INVALID_PARAM, "Learned serving needs a session created with prune = 1");
     if (o.candidate_budget < 0 || o.max_wait_us < 0)

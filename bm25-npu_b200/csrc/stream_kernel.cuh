@@ -147,6 +147,11 @@ struct StreamArgs {
     // a batch with a K per query (tile-group kernel): nullptr when every query takes a.k
     const int *kq;               // [Q] K of each query (a.k is their maximum)
     const long long *kout;       // [Q] first output slot of each query (packed rows)
+    // warp-tile kernel: [word][tiles + 1] first posting (relative to indptr[term]) of each tile for
+    // the query words without a directory row (PlanRowsKernel); prefetch != 0: each claim's posting
+    // runs are prefetched into L2 when the claim is taken
+    int *plan_rows;
+    int prefetch;
 };
 
 // K of query q, and the first output slot of its row.

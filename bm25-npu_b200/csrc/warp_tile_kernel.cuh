@@ -1,0 +1,401 @@
+// Warp-tile BM25 Search kernel for sm_100a (kernel 5, the default plain path).
+//
+// The reference scores one (query, 8192-document leaf) per task, streaming each
+// query term's postings through the unified buffer
+//   feature_retrieval/src/ascendfaiss/ops/ascendc/bm25/fused/op_kernel/bm25_fused_score_top_k.cpp:637-793
+// This kernel gives every warp its own work and its own data path:
+//   * a claim is one query and kC consecutive 1024-document tiles; warps take
+//     claims from one global counter (the atomic for the next claim is in
+//     flight while the current one runs), in tile-major order, so every query
+//     gets tiles early and its running bound rises at once;
+//   * the warp resolves the claim itself: lane s holds query word s's posting
+//     position at each of the claim's kC + 1 tile bounds, read from the word's
+//     directory row (long lists, built at create) or from its plan row (short
+//     lists, PlanRowsKernel), and issues one L2 prefetch per word for the
+//     postings of all kC tiles (cp.async.bulk.prefetch.L2: no shared memory, no
+//     registers held while the bytes are in flight);
+//   * per tile the warp loads its postings straight from global memory into
+//     registers, up to kWtSlots windows of 128 postings at once across the
+//     query's words (lane l takes postings l, l + 32, l + 64, l + 96 of a
+//     window, so consecutive lanes add consecutive documents of a dense list
+//     into distinct shared-memory banks), and adds them into its private 4 KB
+//     FP32 row in query-word order (a __syncwarp between words orders the
+//     lanes: each document's sum is ((0 + s_1) + s_2) + ... as in
+//     cpu_index_search.h:176-188);
+//   * then it selects the tile's top-K at or above the query's running bound
+//     (TileSelectAppend, shared with the tile-group kernel) and clears the row.
+// No producer warp, no mbarrier, no wait on another warp: the only latencies
+// are the warp's own loads.  FinalSelectKernel finishes every query.
+//
+// A retry pass (a.retry) covers only the queries of the fail list, as in the
+// tile-group kernel.
+#pragma once
+#include "tile_group_kernel.cuh"
+
+namespace bm25k {
+
+constexpr int kWtTile = 1024;        // documents per tile (one warp's row)
+constexpr int kWtWarps = 8;
+constexpr int kWtThreads = kWtWarps * 32;
+constexpr int kWtWindow = 128;       // postings per window (4 per lane)
+constexpr int kWtSlots = 4;          // windows loaded before their adds
+constexpr int kPlanRowChunk = 2048;  // plan row entries per PlanRowsKernel CTA (grid.y)
+
+struct WtShared {
+    WarpSel wsel[kWtWarps];
+};
+
+inline size_t WarpTileSmem() { return (size_t)kWtWarps * kWtTile * sizeof(float) + sizeof(WtShared); }
+
+// Streaming loads of postings: read once, so they do not displace the query and directory lines
+// in L1.
+__device__ __forceinline__ int LdStreamI32(const int *p)
+{
+    int v;
+    asm("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ float LdStreamF32(const float *p)
+{
+    float v;
+    asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+
+// Prefetch of [p, p + bytes) into L2 (p 16-byte aligned, bytes a multiple of 16).
+__device__ __forceinline__ void PrefetchL2(const void *p, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Posting positions of query word w at the bounds of tiles t0 .. t0 + kC (clamped at the last
+// bound): off[j] = first posting of the word's list in tile t0 + j.  Words outside the vocabulary
+// have no postings (a negative one is flagged).
+template <int kC>
+__device__ __forceinline__ void WtWordOffsets(const StreamArgs &a, long long w, int t0, int *off, unsigned &bad)
+{
+    const int term = __ldg(a.words + w);
+    if (term < 0 || term >= a.vocab) {
+        if (term < 0)
+            bad |= kStatusBadWord;
+#pragma unroll
+        for (int j = 0; j <= kC; ++j)
+            off[j] = 0;
+        return;
+    }
+    const int base = (int)__ldg(a.indptr + term);
+    const int r = a.dir_row ? __ldg(a.dir_row + term) : -1;
+    if (r >= 0) {
+        const int *row = a.dir + (long long)r * a.dir_stride;
+#pragma unroll
+        for (int j = 0; j <= kC; ++j)
+            off[j] = base + __ldg(row + min(t0 + j, a.tiles));
+    } else {
+        const int *row = a.plan_rows + w * a.dir_stride;  // written by the kernel before this one
+#pragma unroll
+        for (int j = 0; j <= kC; ++j)
+            off[j] = base + __ldcg(row + min(t0 + j, a.tiles));
+    }
+}
+
+// L2 prefetch of postings [lo, hi) of both arrays, widened to 16-byte boundaries (the arrays are
+// padded past their end).
+__device__ __forceinline__ void PrefetchRun(const StreamArgs &a, int lo, int hi)
+{
+    if (lo >= hi)
+        return;
+    const int p0 = lo & ~3, p1 = (hi + 3) & ~3;
+    const unsigned bytes = (unsigned)(p1 - p0) * 4u;
+    PrefetchL2(a.indices + p0, bytes);
+    PrefetchL2(a.data + p0, bytes);
+}
+
+// Inclusive prefix sum over the warp.
+__device__ __forceinline__ int WarpInclusiveSum(int v, int lane)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int x = __shfl_up_sync(kFull, v, o);
+        if (lane >= o)
+            v += x;
+    }
+    return v;
+}
+
+// kC: tiles per claim.  kLean: the plain first pass with one K <= 32 for every query.
+template <int kC, bool kLean>
+__global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs a)
+{
+    extern __shared__ __align__(128) unsigned char wt_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float *row = reinterpret_cast<float *>(wt_smem) + (size_t)warp * kWtTile;
+    float4 *row4 = reinterpret_cast<float4 *>(row);
+    WtShared &sh = *reinterpret_cast<WtShared *>(wt_smem + (size_t)kWtWarps * kWtTile * sizeof(float));
+    WarpSel &ws = sh.wsel[warp];
+#pragma unroll
+    for (int j = 0; j < kWtTile / 128; ++j)
+        row4[lane + 32 * j] = make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncwarp();
+    AllowDependents();    // the final select may be placed as this kernel's CTAs retire
+    WaitPrerequisites();  // plan rows (and a retry pass's fail list) of the kernels before this one
+    const unsigned nq = !kLean && a.retry ? __ldcg(a.fail_in_count) : (unsigned)a.q;
+    const unsigned claims = nq * (unsigned)((a.tiles + kC - 1) / kC);
+    unsigned bad = 0;
+    unsigned n_claims = 0, n_tiles = 0, n_post = 0;  // per warp
+
+    unsigned nxt = 0;
+    if (lane == 0)
+        nxt = atomicAdd(&a.ctrl->next, 1u);
+    for (;;) {
+        const unsigned c = __shfl_sync(kFull, nxt, 0);
+        if (c >= claims)
+            break;
+        if (lane == 0)
+            nxt = atomicAdd(&a.ctrl->next, 1u);  // the next claim, in flight meanwhile
+
+        // ---- the claim: query, tiles, and each word's posting positions at the tile bounds ----
+        const unsigned qi = c % nq;
+        const int q = !kLean && a.retry ? __ldcg(a.fail_in + qi) : (int)qi;
+        const int t0 = (int)(c / nq) * kC;
+        const int nt = min(kC, a.tiles - t0);
+        const long long qb = __ldg(a.qoffsets + q), qe = __ldg(a.qoffsets + q + 1);
+        int nw = (int)(qe - qb);
+        if (qe - qb < 0 || qe - qb > kMaxTerms || qb < 0 || qe > a.word_cap) {
+            bad |= kStatusBadQuery;
+            nw = 0;
+        }
+        const int k = kLean ? a.k : QueryK(a, q);
+        const unsigned thr_bits = __ldcg(a.threshold + q);
+        const unsigned slot_bits = lane < k ? __ldcg(a.tslots + (long long)q * 32 + lane) : 0xffffffffu;
+        int offA[kC + 1], offB[kC + 1];  // words lane and lane + 32
+#pragma unroll
+        for (int j = 0; j <= kC; ++j)
+            offA[j] = offB[j] = 0;
+        if (lane < nw)
+            WtWordOffsets<kC>(a, qb + lane, t0, offA, bad);
+        if (lane + 32 < nw)
+            WtWordOffsets<kC>(a, qb + lane + 32, t0, offB, bad);
+        if (a.prefetch) {
+            PrefetchRun(a, offA[0], offA[kC]);
+            PrefetchRun(a, offB[0], offB[kC]);
+        }
+        const float thr = fmaxf(__uint_as_float(thr_bits), __uint_as_float(__reduce_min_sync(kFull, slot_bits)));
+        ++n_claims;
+        n_tiles += (unsigned)nt;
+        n_post += (unsigned)(offA[kC] - offA[0]) + (unsigned)(offB[kC] - offB[0]);
+
+        // ---- the claim's tiles ----
+        for (int j = 0; j < nt; ++j) {
+            const int tile = t0 + j;
+            const int base_doc = tile * kWtTile;
+            // windows of 128 postings of every word in this tile, numbered in word order
+            const int bA = offA[0], eA = offA[1], bB = offB[0], eB = offB[1];
+            const int nA = (eA - bA + kWtWindow - 1) / kWtWindow;
+            const int nB = (eB - bB + kWtWindow - 1) / kWtWindow;
+            const int cumA = WarpInclusiveSum(nA, lane);
+            const int WA = __shfl_sync(kFull, cumA, 31);
+            int cumB = 0, W = WA;
+            if (nw > 32) {  // uniform
+                cumB = WarpInclusiveSum(nB, lane) + WA;
+                W = __shfl_sync(kFull, cumB, 31);
+            }
+            int prev_word = -1;
+            for (int i0 = 0; i0 < W; i0 += kWtSlots) {
+                int ids[kWtSlots][4];
+                float vals[kWtSlots][4];
+                int word[kWtSlots];
+#pragma unroll
+                for (int u = 0; u < kWtSlots; ++u) {
+                    const int i = i0 + u;
+                    int p0 = 0, p1 = 0;
+                    word[u] = -1;
+                    if (i < W) {  // uniform
+                        int s, first, b, e;
+                        if (i < WA) {
+                            s = __popc(__ballot_sync(kFull, cumA <= i));
+                            first = __shfl_sync(kFull, cumA - nA, s);
+                            b = __shfl_sync(kFull, bA, s);
+                            e = __shfl_sync(kFull, eA, s);
+                            word[u] = s;
+                        } else {
+                            s = __popc(__ballot_sync(kFull, cumB <= i));
+                            first = __shfl_sync(kFull, cumB - nB, s);
+                            b = __shfl_sync(kFull, bB, s);
+                            e = __shfl_sync(kFull, eB, s);
+                            word[u] = 32 + s;
+                        }
+                        p0 = b + (i - first) * kWtWindow;
+                        p1 = min(p0 + kWtWindow, e);
+                    }
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) {
+                        const int p = p0 + lane + 32 * v;
+                        ids[u][v] = -1;
+                        vals[u][v] = 0.0f;
+                        if (p < p1) {
+                            ids[u][v] = LdStreamI32(a.indices + p);
+                            vals[u][v] = LdStreamF32(a.data + p);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kWtSlots; ++u) {
+                    if (word[u] < 0)
+                        break;  // uniform: no more windows
+                    if (word[u] != prev_word) {
+                        __syncwarp();  // the previous word's adds are in the row before this word's
+                        prev_word = word[u];
+                    }
+                    int d[4];
+                    float r[4];
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) {
+                        d[v] = ids[u][v] - base_doc;
+                        if (ids[u][v] >= 0 && (unsigned)d[v] >= (unsigned)kWtTile)
+                            bad |= kStatusBadPosting;
+                    }
+#pragma unroll
+                    for (int v = 0; v < 4; ++v)
+                        if ((unsigned)d[v] < (unsigned)kWtTile)
+                            r[v] = row[d[v]];
+#pragma unroll
+                    for (int v = 0; v < 4; ++v)
+                        if ((unsigned)d[v] < (unsigned)kWtTile)
+                            row[d[v]] = r[v] + vals[u][v];
+                }
+            }
+            __syncwarp();
+            if (W > 0) {  // a tile without postings has an all-zero row: nothing to select
+                bad |= TileSelectAppend<kWtTile, kLean>(a, ws, row4, thr, q, tile, lane);
+                __syncwarp();
+            }
+#pragma unroll
+            for (int x = 0; x < kC; ++x) {
+                offA[x] = offA[x + 1];
+                offB[x] = offB[x + 1];
+            }
+        }
+    }
+
+    bad = __reduce_or_sync(kFull, bad);
+    n_post = __reduce_add_sync(kFull, n_post);
+    if (lane == 0) {
+        if (bad)
+            atomicOr(a.status, bad);
+        if (a.stats && n_claims) {
+            atomicAdd(a.stats + kStatClaims, (unsigned long long)n_claims);
+            atomicAdd(a.stats + kStatTilesScanned, (unsigned long long)n_tiles);
+            atomicAdd(a.stats + kStatPostingsCopied, (unsigned long long)n_post);
+        }
+        // the last warp to run dry resets the work counter for the next pass
+        const unsigned d = atomicAdd(&a.ctrl->done, 1u);
+        if (d == gridDim.x * kWtWarps - 1) {
+            a.ctrl->next = 0u;
+            a.ctrl->done = 0u;
+        }
+    }
+}
+
+template <int kC>
+inline const void *WarpTileKernelFor(bool lean)
+{
+    return lean ? reinterpret_cast<const void *>(&WarpTileKernel<kC, true>)
+                : reinterpret_cast<const void *>(&WarpTileKernel<kC, false>);
+}
+
+// ---- plan rows of the words without a directory row -------------------------------------------
+//
+// rows[w][t] = (first posting of word w's list with document >= t * tile_docs) - indptr[term], for
+// t in [0, tiles] (the same values a directory row holds).  CTA (x, y) covers row entries
+// [y * kPlanRowChunk, (y + 1) * kPlanRowChunk) of words x, x + gridDim.x, ...; a word with a
+// directory row or outside the vocabulary is skipped (the search kernel does not read its plan row).
+// Two warps find the chunk's first and last posting (32-way searches), the chunk's postings mark
+// the entry of their tile when they are the first there, and a suffix minimum fills the entries of
+// the tiles without postings with the next marked one: O(postings + tiles) per word.
+__global__ void __launch_bounds__(kPlanThreads) PlanRowsKernel(const StreamArgs a)
+{
+    __shared__ int ent[kPlanRowChunk];
+    __shared__ int lim[2];
+    __shared__ int wmin[kPlanThreads / 32];
+    constexpr int kPer = kPlanRowChunk / kPlanThreads;
+    static_assert(kPlanRowChunk % kPlanThreads == 0, "whole entries per thread");
+    AllowDependents();  // the search kernel sets up its shared memory meanwhile
+    long long total = __ldg(a.qoffsets + a.q);
+    if (total < 0 || total > a.word_cap) {
+        if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
+            atomicOr(a.status, kStatusBadQuery);
+        total = total < 0 ? 0 : a.word_cap;
+    }
+    const int n_ent = a.tiles + 1;
+    const int e0 = (int)blockIdx.y * kPlanRowChunk, e1 = min(n_ent, e0 + kPlanRowChunk);
+    if (e0 >= e1)
+        return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (long long w = blockIdx.x; w < total; w += gridDim.x) {
+        const int term = __ldg(a.words + w);
+        if (term < 0 || term >= a.vocab)
+            continue;  // flagged by the search kernel; it reads no row for it
+        if (a.dir_row && __ldg(a.dir_row + term) >= 0)
+            continue;  // read from the directory
+        const long long s = __ldg(a.indptr + term), e = __ldg(a.indptr + term + 1);
+        if (warp < 2) {
+            const long long target = (long long)(warp == 0 ? e0 : e1) * a.tile_docs;
+            const long long p = WarpLowerBoundGlobal(a.indices, s, e, target, lane);
+            if (lane == 0)
+                lim[warp] = (int)(p - s);
+        }
+        for (int i = tid; i < kPlanRowChunk; i += kPlanThreads)
+            ent[i] = INT_MAX;
+        __syncthreads();
+        const int b = lim[0], en = lim[1];
+        for (int i = b + tid; i < en; i += kPlanThreads) {
+            const int t = __ldg(a.indices + s + i) / a.tile_docs;
+            const int tp = i > 0 ? __ldg(a.indices + s + i - 1) / a.tile_docs : -1;
+            if (tp != t)
+                ent[t - e0] = i;  // the tile's first posting; t is in [e0, e1)
+        }
+        __syncthreads();
+        // suffix minimum over the chunk, ending in en
+        int v[kPer];
+        int m = INT_MAX;
+#pragma unroll
+        for (int u = kPer - 1; u >= 0; --u) {
+            m = min(m, ent[tid * kPer + u]);
+            v[u] = m;
+        }
+        int x = m;  // suffix minimum of the thread aggregates within the warp
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_down_sync(kFull, x, o);
+            if (lane + o < 32)
+                x = min(x, y);
+        }
+        if (lane == 0)
+            wmin[warp] = x;
+        __syncthreads();
+        int carry = en;
+        for (int j = warp + 1; j < kPlanThreads / 32; ++j)
+            carry = min(carry, wmin[j]);
+        const int after = __shfl_down_sync(kFull, x, 1);
+        if (lane < 31)
+            carry = min(carry, after);
+        int *out = a.plan_rows + w * a.dir_stride;
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int t = e0 + tid * kPer + u;
+            if (t < e1)
+                out[t] = min(v[u], carry);
+        }
+        __syncthreads();  // ent, lim and wmin are rewritten for the next word
+    }
+}
+
+// Grid of PlanRowsKernel for a batch capacity of `words` query words.
+inline dim3 PlanRowsGrid(long long words, int tiles, int sms)
+{
+    const int chunks = (tiles + 1 + kPlanRowChunk - 1) / kPlanRowChunk;
+    const long long x = std::max<long long>(1, std::min<long long>(words, std::max(1, sms * 4 / chunks)));
+    return dim3((unsigned)x, (unsigned)chunks);
+}
+
+} // namespace bm25k

@@ -70,7 +70,7 @@ def pack_queries(queries):
 
 
 def _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes, stream,
-             kernel=4, ring_stages=0, ring_chunk=0, prune=False, candidate_capacity=0, prune_route=0.0):
+             kernel=5, ring_stages=0, ring_chunk=0, prune=False, candidate_capacity=0, prune_route=0.0):
     o = n.Options()
     n.engine_library().bm25_default_options(ctypes.byref(o))
     o.device_id = device_id
@@ -101,7 +101,7 @@ class Bm25Session:
 
     @classmethod
     def from_csc(cls, indptr, indices, data, num_docs, *, query_capacity=8, word_capacity=24, max_k=10,
-                 device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0, stream=None, kernel=4, ring_stages=0,
+                 device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0, stream=None, kernel=5, ring_stages=0,
                  ring_chunk=0, prune=False, candidate_capacity=0, prune_route=0.0):
         """Eager CSC index (bm25s layout): indptr int64 [V+1], indices int32 [M], data float32 [M]."""
         lib = n.engine_library()
@@ -122,7 +122,7 @@ class Bm25Session:
     @classmethod
     def from_lazy(cls, term_offsets, posting_doc_ids, posting_tf, doc_norm, idf, *, k1=1.2, query_capacity=8,
                   word_capacity=24, max_k=10, device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0,
-                  stream=None, kernel=4, ring_stages=0, ring_chunk=0, prune=False, candidate_capacity=0,
+                  stream=None, kernel=5, ring_stages=0, ring_chunk=0, prune=False, candidate_capacity=0,
                   prune_route=0.0):
         """The reference's resident index (common/bm25/index_data.h:9-42); posting scores built on the GPU."""
         lib = n.engine_library()

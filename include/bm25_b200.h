@@ -40,14 +40,15 @@ typedef struct bm25_handle bm25_handle;
 /* Session configuration (replaces Bm25Config, AscendIndexBm25.h:17-25). */
 typedef struct bm25_options {
     int32_t device_id;       /* CUDA device ordinal (Bm25Config::deviceId) */
-    int32_t max_k;           /* largest K a Search may ask for (Bm25Config::topK); 1..32 */
+    int32_t max_k;           /* largest K a Search may ask for (Bm25Config::topK); 1..32, or up to 1024 with
+                                the warp-tile and tile-group kernels */
     int64_t query_capacity;  /* largest query batch (Bm25Config::queryCount) */
     int64_t word_capacity;   /* largest total word count per batch (Bm25Config::maxQueryWords) */
     int32_t tile_docs;       /* documents per scoring tile; 0 = automatic (power of two, 2048..32768) */
     int32_t merge_fan_in;    /* lists merged per tree node; 0 = automatic (2..32) */
     int64_t directory_bytes; /* byte budget of the per-tile posting directory; 0 = automatic */
     void *stream;            /* borrowed cudaStream_t, or NULL for an engine-owned stream */
-    int32_t kernel;          /* BM25_KERNEL_*: search kernel; bm25_default_options picks BM25_KERNEL_TILE_GROUP */
+    int32_t kernel;          /* BM25_KERNEL_*: search kernel; bm25_default_options picks BM25_KERNEL_WARP_TILE */
     int32_t ring_stages;     /* posting-ring depth of the ring kernels (0 and 4), 2..8; 0 = automatic */
     int32_t ring_chunk;      /* postings per ring stage of the tile-group kernel, 512..4096, a multiple of 4;
                                 0 = automatic */
@@ -64,13 +65,18 @@ typedef struct bm25_options {
  *   BM25_KERNEL_STREAM     persistent kernel, 2048-8192-document tiles, one posting ring per CTA
  *   BM25_KERNEL_PER_TILE   one CTA per (query, tile) and an in-launch merge tree
  *   BM25_KERNEL_TILE_GROUP persistent kernel, 1024-document tiles, one warp per tile of an
- *                          8-tile group fed by one bulk copy per query word (the default) */
+ *                          8-tile group fed by one bulk copy per query word
+ *   BM25_KERNEL_WARP_TILE  persistent kernel, 1024-document tiles, every warp takes its own claims
+ *                          (a query and 4 consecutive tiles) and loads its postings itself, the
+ *                          claim's posting runs prefetched into L2 (the default); pruned Searches
+ *                          stream their routed and retried queries with the tile-group kernel */
 #define BM25_KERNEL_STREAM 0
 #define BM25_KERNEL_PER_TILE 1
 #define BM25_KERNEL_TILE_GROUP 4
+#define BM25_KERNEL_WARP_TILE 5
 
 /* Fills defaults: device 0, max_k 10, 8 queries, 24 words (the reference's Bm25Config defaults),
- * the tile-group kernel. */
+ * the warp-tile kernel. */
 void bm25_default_options(bm25_options *options);
 
 /*
@@ -237,16 +243,21 @@ int bm25_last_error(const bm25_handle *handle, char *buffer, size_t length, int6
  *     multiple of 4 elements past indptr[vocab];
  *   - num_words = qoffsets[q] (at most 64 words per query); 1 <= k <= min(32, num_docs);
  *   - all scratch comes from one fixed 16 MiB device array inside this library
- *     (held by every GPU that loads it until exit); a Search needing more
- *     (roughly q * ceil(num_docs / 8192) * (256 * k + 16 * num_words / q) bytes)
- *     is rejected with BM25_ERR_INVALID_PARAM;
+ *     (held by every GPU that loads it until exit); a Search needing more is
+ *     rejected with BM25_ERR_INVALID_PARAM before any device work.  The need,
+ *     in bytes, with a16(x) = x rounded up to a multiple of 16:
+ *       tile  = the smallest of 2048, 4096, 8192 with tile * SMs >= num_docs
+ *               (8192 when none is), tiles = ceil(num_docs / tile),
+ *       need  = 256 + 2 a16(4 q) + 128 q + 64 q tiles k + 16 max(1, num_words) tiles;
  *   - work runs on `stream` (a cudaStream_t) on device `device_id`; the call
- *     waits for it and returns the device status;
- *   - the first call on a device looks up the array's device address and sets
- *     kernel attributes: make it before any stream capture;
+ *     waits for it and returns the device status; the caller's current device
+ *     is the same after the call as before it;
+ *   - the first call on a device looks up the array's device address, sets
+ *     kernel attributes and page-locks a static host word for the status
+ *     (nothing is allocated): make it before any stream capture;
  *   - every call shares the array, so calls that overlap on the GPU (other
  *     streams, other host threads) race: serialise them;
- *   - error details: bm25_last_error(NULL, ...).
+ *   - error details: bm25_last_error(NULL, ...) on the calling thread.
  */
 int bm25_search_csc_static(const int64_t *indptr, const int32_t *indices, const float *data, int64_t vocab,
                            int64_t num_docs, const int64_t *qoffsets, const int32_t *words, int64_t q,

@@ -29,7 +29,7 @@ def test_default_options_match_reference_config(pkg):
     o = pkg._native.Options()
     pkg._native.engine_library().bm25_default_options(ctypes.byref(o))
     assert (o.device_id, o.query_capacity, o.word_capacity, o.max_k) == (0, 8, 24, 10)
-    assert o.kernel == 4  # the tile-group kernel
+    assert o.kernel == 5  # the warp-tile kernel
 
 
 @pytest.mark.parametrize('case', ['unsorted', 'range', 'nan', 'negative', 'bounds'])

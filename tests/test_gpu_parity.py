@@ -20,12 +20,12 @@ def _oracle(oracle_mod, index, data, offsets, words, k):
     return oracle_mod.search(index.offsets, index.docs, data, index.num_docs, offsets, words, k)
 
 
-KERNELS = pytest.mark.parametrize('kernel', [0, 1, 4], ids=['stream', 'per_tile', 'tile_group'])
+KERNELS = pytest.mark.parametrize('kernel', [0, 1, 4, 5], ids=['stream', 'per_tile', 'tile_group', 'warp_tile'])
 
 
 def _tile(kernel, tile_docs):
-    """The tile-group kernel takes 1024- or 2048-document tiles (0 = automatic)."""
-    return 0 if kernel == 4 else tile_docs
+    """The tile-group kernel takes 1024- or 2048-document tiles, the warp-tile kernel 1024 (0 = automatic)."""
+    return 0 if kernel in (4, 5) else tile_docs
 
 
 @KERNELS
@@ -49,7 +49,7 @@ def test_config_8192_docs_q8x3_k10(pkg, oracle_mod, cuda_ok, kernel):
                                                      (32768, 8, 4)])
 def test_tiles_and_merge_tree(pkg, oracle_mod, corpus, cuda_ok, tile_docs, fan_in, stages, kernel):
     spec, index, data = corpus
-    if kernel == 4 and tile_docs not in (0, 1024, 2048):
+    if (kernel == 4 and tile_docs not in (0, 1024, 2048)) or (kernel == 5 and tile_docs not in (0, 1024)):
         with pytest.raises(pkg.InvalidParam):
             pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, tile_docs=tile_docs,
                                      kernel=kernel)

@@ -109,3 +109,52 @@ def test_static_matches_session_twice(pkg, oracle_mod, cuda_ok):
                        d_scores.data_ptr(), d_ids.data_ptr(), stream.cuda_stream)
         assert status == n.BM25_OK, _error(lib)
         assert_same_topk(d_scores.cpu().numpy(), d_ids.cpu().numpy(), *want, 'static after error')
+
+
+@pytest.mark.gpu
+def test_static_exact_scratch_boundary(pkg, oracle_mod, cuda_ok):
+    """A Search that needs exactly the 16 MiB of the array runs; one word more (16 bytes more) is
+    rejected before any device work.  2048 documents make one 2048-document tile on any SM count, so
+    the need is 256 + 2 a16(4 q) + 128 q + 64 q k + 16 num_words: q = 7680, k = 32 and 240 words
+    come to 16,777,216 bytes."""
+    import torch
+    from importlib import import_module
+    n = import_module('bm25-npu_b200._native')
+    lib = n.engine_library()
+    spec = pkg.CorpusSpec(docs=2048, vocab=3000, seed=31, k1=1.2)
+    index = pkg.synthetic_index(spec)
+    data = oracle_mod.contributions(index, spec.k1)
+    m = int(index.offsets[-1])
+    dev = torch.device('cuda:0')
+    d_indptr = torch.from_numpy(np.ascontiguousarray(index.offsets, dtype=np.int64)).to(dev)
+    d_indices = torch.zeros((m + 3) // 4 * 4, dtype=torch.int32, device=dev)
+    d_indices[:m] = torch.from_numpy(np.ascontiguousarray(index.docs, dtype=np.int32)).to(dev)
+    d_data = torch.zeros((m + 3) // 4 * 4, dtype=torch.float32, device=dev)
+    d_data[:m] = torch.from_numpy(data).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    q, k = 7680, 32
+    a16 = lambda x: (x + 15) // 16 * 16  # noqa: E731
+    need = lambda nw: 256 + 2 * a16(4 * q) + 128 * q + 64 * q * k + 16 * max(1, nw)  # noqa: E731
+    assert need(240) == STATIC_SCRATCH_BYTES
+    rng = np.random.default_rng(8)
+    for nw, ok in ((240, True), (241, False)):
+        rows = [[] for _ in range(q)]
+        for i in range(nw):  # 80 queries of 3 words, the 241st word on a query of its own
+            rows[i // 3 if i < 240 else 100].append(int(rng.integers(0, index.vocab)))
+        offsets, words = pack(rows)
+        assert int(offsets[-1]) == nw
+        d_off = torch.from_numpy(offsets).to(dev)
+        d_words = torch.from_numpy(words).to(dev)
+        d_scores = torch.full((q, k), -1.0, dtype=torch.float32, device=dev)
+        d_ids = torch.full((q, k), -1, dtype=torch.int32, device=dev)
+        status = _call(lib, d_indptr.data_ptr(), d_indices.data_ptr(), d_data.data_ptr(), index.vocab,
+                       index.num_docs, d_off.data_ptr(), d_words.data_ptr(), q, nw, k, d_scores.data_ptr(),
+                       d_ids.data_ptr(), stream.cuda_stream)
+        if ok:
+            assert status == n.BM25_OK, _error(lib)
+            want = oracle_mod.search(index.offsets, index.docs, data, index.num_docs, offsets, words, k)
+            assert_same_topk(d_scores.cpu().numpy(), d_ids.cpu().numpy(), *want, f'static at {need(nw)} bytes')
+        else:
+            assert status == n.BM25_ERR_INVALID_PARAM
+            assert str(need(nw)) in _error(lib) and str(STATIC_SCRATCH_BYTES) in _error(lib)
+            assert (d_ids == -1).all().item(), 'a rejected Search wrote its output'
