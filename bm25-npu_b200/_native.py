@@ -16,6 +16,8 @@ BM25_OK = 0
 BM25_ERR_INVALID_PARAM = 1
 BM25_ERR_ILLEGAL_OPERATION = 2
 BM25_ERR_INNER_ERROR = 3
+BM25_INJECT_HOST_FAILURE = 1
+BM25_INJECT_STALL = 2
 
 
 class ServerOptions(ctypes.Structure):
@@ -44,6 +46,7 @@ class Options(ctypes.Structure):
         ('prune', c_int32),
         ('candidate_capacity', c_int64),
         ('prune_route', c_float),
+        ('wait_budget_cycles', c_int64),
     ]
 
 
@@ -71,6 +74,8 @@ class Info(ctypes.Structure):
         ('word_capacity', c_int32),
         ('max_k', c_int32),
         ('prune', c_int32),
+        ('graph_instantiations', c_int64),
+        ('graphs_cached', c_int64),
     ]
 
 
@@ -90,6 +95,7 @@ SIGNATURES = {
     'bm25_last_error': (c_int, [c_void_p, c_char_p, c_size_t, POINTER(c_int64)]),
     'bm25_get_info': (c_int, [c_void_p, POINTER(Info)]),
     'bm25_kernel_timing': (c_int, [c_void_p, c_int32]),
+    'bm25_test_inject': (c_int, [c_void_p, c_int32]),
     'bm25_kernel_times': (c_int, [c_void_p, POINTER(c_float), c_int64, POINTER(c_int64)]),
     'bm25_search_pruned_device': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p,
                                           c_void_p, c_void_p, c_void_p]),

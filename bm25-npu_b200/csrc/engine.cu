@@ -21,6 +21,7 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -80,6 +81,10 @@ static bool TileFamily(int kernel) { return kernel == BM25_KERNEL_TILE_GROUP || 
 
 // Tiles per claim of the warp-tile kernel.
 constexpr int kWtClaimTiles = 4;
+
+// Test hook: the next host-buffer Search of any session fails as a device error (bm25_test_inject
+// with no handle).
+static std::atomic<int> g_fail_next{0};
 
 // Launch with programmatic stream serialization: the kernel may start while the kernel before it
 // in the stream runs (the kernel waits in WaitPrerequisites before reading that kernel's output).
@@ -190,6 +195,7 @@ class Engine {
               "max_k above 32 needs the warp-tile or tile-group kernel");
         Check(o.max_k <= docs, "max_k exceeds the document count");
         Check(o.query_capacity >= 1 && o.query_capacity <= 65535, "query_capacity must be in [1, 65535]");
+        Check(o.wait_budget_cycles >= 0, "wait_budget_cycles must be >= 0");
         Check(o.word_capacity >= 0 && o.word_capacity <= 16777216, "word_capacity must be in [0, 2^24]");
         Check(!o.prune || TileFamily(o.kernel), "prune needs the warp-tile or tile-group kernel");
         Cuda(cudaSetDevice(o.device_id), "cudaSetDevice");
@@ -275,11 +281,19 @@ class Engine {
             Cuda(cudaSetDevice(device_), "cudaSetDevice");
             cudaGraphExec_t exec = GraphFor((int)q, k);
             Cuda(cudaStreamWaitEvent(stream_, done_, 0), "cudaStreamWaitEvent");
+            const bool stall = stall_armed_, fail = fail_armed_ || g_fail_next.exchange(0) != 0;
+            stall_armed_ = fail_armed_ = false;
+            if (stall)
+                Cuda(cudaMemsetAsync(d_inject_, 0x01, sizeof(unsigned), stream_), "arm stall");
             ++searches_;
             Cuda(cudaGraphLaunch(exec, stream_), "cudaGraphLaunch");
             ++replays_;
+            if (stall)
+                Cuda(cudaMemsetAsync(d_inject_, 0, sizeof(unsigned), stream_), "disarm stall");
             Cuda(cudaEventRecord(done_, stream_), "cudaEventRecord");
             Cuda(cudaStreamSynchronize(stream_), "complete Search through result D2H");
+            if (fail)
+                throw DeviceError(0, "Injected device failure (bm25_test_inject)");
             Receive(q, k, out_scores, out_ids);
         } catch (...) {
             failed_ = true;
@@ -592,6 +606,17 @@ class Engine {
         return out;
     }
 
+    // Test hook (bm25_test_inject): one-shot failure of the next host-buffer Search.
+    void Inject(int what)
+    {
+        RequireUsable();
+        Check(what == BM25_INJECT_HOST_FAILURE || what == BM25_INJECT_STALL, "Unknown injection");
+        if (what == BM25_INJECT_HOST_FAILURE)
+            fail_armed_ = true;
+        else
+            stall_armed_ = true;
+    }
+
     uint32_t DeviceStatus()
     {
         RequireUsable();
@@ -644,6 +669,8 @@ class Engine {
         info->word_capacity = opts_.word_capacity;
         info->max_k = opts_.max_k;
         info->prune = opts_.prune ? 1 : 0;
+        info->graph_instantiations = instantiations_;
+        info->graphs_cached = (int64_t)graphs_.size();
     }
 
   private:
@@ -829,6 +856,8 @@ class Engine {
         d_out_ = static_cast<unsigned char *>(Alloc(out_bytes_, "cudaMalloc output arena"));
         d_dev_status_ = static_cast<unsigned *>(Alloc(sizeof(unsigned), "cudaMalloc status"));
         Cuda(cudaMemset(d_dev_status_, 0, sizeof(unsigned)), "cudaMemset");
+        d_inject_ = static_cast<unsigned *>(Alloc(sizeof(unsigned), "cudaMalloc inject word"));
+        Cuda(cudaMemset(d_inject_, 0, sizeof(unsigned)), "cudaMemset");
         // Merge tree of the per-tile kernel: level 0 holds tile lists, the root level is the output.
         for (int l = 0; l < plan_.levels && plan_.kernel == 1; ++l) {
             bm25k::Level lv{};
@@ -1061,6 +1090,8 @@ class Engine {
             const bool warp_tile = plan_.kernel == BM25_KERNEL_WARP_TILE && !tau;
             sa.plan_rows = plan_rows_;
             sa.prefetch = 1;
+            sa.wait_budget = opts_.wait_budget_cycles;
+            sa.inject = d_inject_;
             if (warp_tile)
                 bm25k::PlanRowsKernel<<<bm25k::PlanRowsGrid(opts_.word_capacity, plan_.tiles, sms_),
                                         bm25k::kPlanThreads, 0, s>>>(sa);
@@ -1263,6 +1294,7 @@ class Engine {
         const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
         Cuda(e, "cudaGraphInstantiate");
+        ++instantiations_;
         graphs_[key] = exec;
         return exec;
     }
@@ -1362,6 +1394,9 @@ class Engine {
     void *h_in_ = nullptr, *h_out_ = nullptr;
     unsigned char *d_in_ = nullptr, *d_out_ = nullptr;
     unsigned *d_dev_status_ = nullptr;
+    unsigned *d_inject_ = nullptr;  // test hook word read by the tile-group kernel's producer
+    bool stall_armed_ = false, fail_armed_ = false;
+    int64_t instantiations_ = 0;
     bm25k::StreamCtrl *ctrl_ = nullptr;
     unsigned *threshold_ = nullptr, *cand_count_ = nullptr, *tslots_ = nullptr;
     float *cand_scores_ = nullptr;
@@ -1775,6 +1810,24 @@ void bm25_destroy(bm25_handle *h)
         return;
     bm25_close(h);
     delete h;
+}
+
+int bm25_test_inject(bm25_handle *h, int32_t what)
+{
+    if (!h) {
+        if (what != BM25_INJECT_HOST_FAILURE)
+            return BM25_ERR_INVALID_PARAM;
+        bm25b200::g_fail_next.store(1);
+        return BM25_OK;
+    }
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 session is closed");
+            h->engine->Inject(what);
+        },
+        h->error, h->code);
 }
 
 int bm25_last_error(const bm25_handle *h, char *buffer, size_t length, int64_t *code)

@@ -152,7 +152,18 @@ struct StreamArgs {
     // runs are prefetched into L2 when the claim is taken
     int *plan_rows;
     int prefetch;
+    // cycles a bounded wait spends before it gives up (0: kWaitBudget)
+    long long wait_budget;
+    // test hook: a nonzero word makes the tile-group kernel's producer issue no ring stage, so its
+    // consumers' bounded waits run out (nullptr: none)
+    const unsigned *inject;
 };
+
+// The wait budget of a launch.
+__device__ __forceinline__ long long WaitBudget(const StreamArgs &a)
+{
+    return a.wait_budget > 0 ? a.wait_budget : kWaitBudget;
+}
 
 // K of query q, and the first output slot of its row.
 __device__ __forceinline__ int QueryK(const StreamArgs &a, int q)
@@ -239,7 +250,8 @@ __device__ __forceinline__ bool MbarTryWaitSuspend(unsigned long long *bar, unsi
 }
 
 // Bounded wait; false when the budget ran out or another role aborted.
-__device__ __forceinline__ bool MbarWait(unsigned long long *bar, unsigned parity, volatile int *abort)
+__device__ __forceinline__ bool MbarWait(unsigned long long *bar, unsigned parity, volatile int *abort,
+                                         long long budget = kWaitBudget)
 {
     if (MbarTryWait(bar, parity))
         return true;
@@ -249,7 +261,7 @@ __device__ __forceinline__ bool MbarWait(unsigned long long *bar, unsigned parit
             return true;
         if (*abort)
             return false;
-        if (clock64() - t0 > kWaitBudget) {
+        if (clock64() - t0 > budget) {
             *abort = 1;
             return false;
         }
@@ -257,11 +269,12 @@ __device__ __forceinline__ bool MbarWait(unsigned long long *bar, unsigned parit
 }
 
 // Whole-warp bounded wait: lane 0 waits, then every lane acquires the completed phase.
-__device__ __forceinline__ bool WarpWait(unsigned long long *bar, unsigned parity, volatile int *abort, int lane)
+__device__ __forceinline__ bool WarpWait(unsigned long long *bar, unsigned parity, volatile int *abort, int lane,
+                                         long long budget = kWaitBudget)
 {
     int ok = 1;
     if (lane == 0)
-        ok = MbarWait(bar, parity, abort) ? 1 : 0;
+        ok = MbarWait(bar, parity, abort, budget) ? 1 : 0;
     ok = __shfl_sync(kFull, ok, 0);
     if (ok)
         (void)MbarTryWait(bar, parity);  // complete already: returns at once, acquiring for this lane
@@ -270,14 +283,15 @@ __device__ __forceinline__ bool WarpWait(unsigned long long *bar, unsigned parit
 
 // Whole-warp bounded wait with every lane on the barrier (no divergent branch);
 // the outcome is agreed by vote, so all lanes return the same.
-__device__ __forceinline__ bool WarpWaitAll(unsigned long long *bar, unsigned parity, volatile int *abort)
+__device__ __forceinline__ bool WarpWaitAll(unsigned long long *bar, unsigned parity, volatile int *abort,
+                                            long long budget = kWaitBudget)
 {
     bool ok = MbarTryWait(bar, parity);
     if (!__all_sync(kFull, ok)) {
         const long long t0 = clock64();
         while (!ok) {
             ok = MbarTryWaitSuspend(bar, parity);
-            if (!ok && (*abort || clock64() - t0 > kWaitBudget)) {
+            if (!ok && (*abort || clock64() - t0 > budget)) {
                 *abort = 1;
                 break;
             }
@@ -675,7 +689,7 @@ __global__ void __launch_bounds__(kStreamThreads, 1) StreamSearchKernel(const St
             const unsigned long long k = g / (unsigned long long)a.stages;
             int ok = 1;
             if (k > 0 && lane == 0)
-                ok = MbarWait(&sh.empty[st], (unsigned)((k - 1) & 1), abort) ? 1 : 0;
+                ok = MbarWait(&sh.empty[st], (unsigned)((k - 1) & 1), abort, WaitBudget(a)) ? 1 : 0;
             return __shfl_sync(kFull, ok, 0) != 0;
         };
 
@@ -814,7 +828,7 @@ __global__ void __launch_bounds__(kStreamThreads, 1) StreamSearchKernel(const St
             for (unsigned long long h = (g > (unsigned long long)a.stages ? g - a.stages : 0); h < g; ++h) {
                 const int st = (int)(h % (unsigned long long)a.stages);
                 const long long t0 = clock64();
-                while (!MbarTryWait(&sh.full[st], (unsigned)((h / a.stages) & 1)) && clock64() - t0 < kWaitBudget) {
+                while (!MbarTryWait(&sh.full[st], (unsigned)((h / a.stages) & 1)) && clock64() - t0 < WaitBudget(a)) {
                 }
             }
         }
@@ -831,7 +845,7 @@ __global__ void __launch_bounds__(kStreamThreads, 1) StreamSearchKernel(const St
     for (;;) {
         const int st = (int)(g % (unsigned long long)a.stages);
         const unsigned parity = (unsigned)((g / (unsigned long long)a.stages) & 1);
-        if (!WarpWait(&sh.full[st], parity, abort, lane))
+        if (!WarpWait(&sh.full[st], parity, abort, lane, WaitBudget(a)))
             break;
         const StageMeta m = sh.meta[st];
         if (m.flags & kStop)

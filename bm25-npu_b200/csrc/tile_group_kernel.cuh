@@ -378,7 +378,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
         auto claim_stage = [&]() -> bool {
             int ok = 1;
             if (wraps > 0 && lane == 0)
-                ok = MbarWait(&sh.empty[pst], (wraps - 1) & 1u, abort) ? 1 : 0;
+                ok = MbarWait(&sh.empty[pst], (wraps - 1) & 1u, abort, WaitBudget(a)) ? 1 : 0;
             return __shfl_sync(kFull, ok, 0) != 0;
         };
         auto advance_stage = [&]() {
@@ -442,6 +442,10 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
             return c;  // lane 0's value; broadcast when decoded
         };
 
+        // test hook: a stalled producer issues no stage (not even the stop), so every consumer's
+        // bounded wait runs out and the launch reports kStatusTimeout
+        if (a.inject && __ldcg(a.inject) != 0u)
+            dead = true;
         WgClaim cur, nx1, nx2;
         decode(__shfl_sync(kFull, take_claim(), 0), nx1);
         fetch_offsets(nx1);
@@ -580,7 +584,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
             for (unsigned long long h = (g > (unsigned long long)a.stages ? g - a.stages : 0); h < g; ++h) {
                 const int st = (int)(h % (unsigned long long)a.stages);
                 const long long t0 = clock64();
-                while (!MbarTryWait(&sh.full[st], (unsigned)((h / a.stages) & 1)) && clock64() - t0 < kWaitBudget) {
+                while (!MbarTryWait(&sh.full[st], (unsigned)((h / a.stages) & 1)) && clock64() - t0 < WaitBudget(a)) {
                 }
             }
         }
@@ -596,7 +600,7 @@ __global__ void __launch_bounds__(kWgThreads, kTile == 1024 ? 3 : 2) TileGroupKe
     unsigned bad = 0;
     bool touched = false;
     for (;;) {
-        if (!WarpWaitAll(&sh.full[st], parity, abort))
+        if (!WarpWaitAll(&sh.full[st], parity, abort, WaitBudget(a)))
             break;
         const WgMeta &m = sh.meta[st];
         const int flags = m.flags;

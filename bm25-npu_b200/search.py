@@ -70,7 +70,8 @@ def pack_queries(queries):
 
 
 def _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes, stream,
-             kernel=5, ring_stages=0, ring_chunk=0, prune=False, candidate_capacity=0, prune_route=0.0):
+             kernel=5, ring_stages=0, ring_chunk=0, prune=False, candidate_capacity=0, prune_route=0.0,
+             wait_budget_cycles=0):
     o = n.Options()
     n.engine_library().bm25_default_options(ctypes.byref(o))
     o.device_id = device_id
@@ -87,6 +88,7 @@ def _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_f
     o.prune = int(bool(prune))
     o.candidate_capacity = candidate_capacity
     o.prune_route = prune_route
+    o.wait_budget_cycles = wait_budget_cycles
     return o
 
 
@@ -102,7 +104,7 @@ class Bm25Session:
     @classmethod
     def from_csc(cls, indptr, indices, data, num_docs, *, query_capacity=8, word_capacity=24, max_k=10,
                  device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0, stream=None, kernel=5, ring_stages=0,
-                 ring_chunk=0, prune=False, candidate_capacity=0, prune_route=0.0):
+                 ring_chunk=0, prune=False, candidate_capacity=0, prune_route=0.0, wait_budget_cycles=0):
         """Eager CSC index (bm25s layout): indptr int64 [V+1], indices int32 [M], data float32 [M]."""
         lib = n.engine_library()
         indptr = np.ascontiguousarray(indptr, dtype=np.int64)
@@ -112,7 +114,8 @@ class Bm25Session:
         if vocab < 1 or indices.size != indptr[-1] or data.size != indices.size:
             raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'Index dimensions/endpoints differ')
         o = _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes,
-                     stream, kernel, ring_stages, ring_chunk, prune, candidate_capacity, prune_route)
+                     stream, kernel, ring_stages, ring_chunk, prune, candidate_capacity, prune_route,
+                     wait_budget_cycles)
         h = c_void_p()
         status = lib.bm25_create(n.ptr(indptr, c_int64), n.ptr(indices, c_int32), n.ptr(data, c_float), vocab,
                                  int(num_docs), ctypes.byref(o), ctypes.byref(h))
@@ -123,7 +126,7 @@ class Bm25Session:
     def from_lazy(cls, term_offsets, posting_doc_ids, posting_tf, doc_norm, idf, *, k1=1.2, query_capacity=8,
                   word_capacity=24, max_k=10, device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0,
                   stream=None, kernel=5, ring_stages=0, ring_chunk=0, prune=False, candidate_capacity=0,
-                  prune_route=0.0):
+                  prune_route=0.0, wait_budget_cycles=0):
         """The reference's resident index (common/bm25/index_data.h:9-42); posting scores built on the GPU."""
         lib = n.engine_library()
         offsets = np.ascontiguousarray(term_offsets, dtype=np.int64)
@@ -135,7 +138,8 @@ class Bm25Session:
         if offsets.size != vocab + 1 or docs.size != tf.size or offsets[-1] != docs.size:
             raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'Index dimensions/endpoints differ')
         o = _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes,
-                     stream, kernel, ring_stages, ring_chunk, prune, candidate_capacity, prune_route)
+                     stream, kernel, ring_stages, ring_chunk, prune, candidate_capacity, prune_route,
+                     wait_budget_cycles)
         h = c_void_p()
         status = lib.bm25_create_lazy(n.ptr(offsets, c_int64), n.ptr(docs, c_int32), n.ptr(tf, c_float),
                                       n.ptr(norm, c_float), n.ptr(idf, c_float), vocab, norm.size, float(k1),
@@ -292,6 +296,12 @@ class Bm25Session:
         status = self._lib.bm25_search_device(self._handle, c_void_p(qoffsets_ptr), c_void_p(words_ptr), q, k,
                                               c_void_p(scores_ptr), c_void_p(ids_ptr), c_void_p(stream_ptr))
         _raise(self._lib, status, self._handle)
+
+    def inject(self, what):
+        """Test hook (bm25_test_inject): the next ``search`` fails as a device error, either on the host
+        (BM25_INJECT_HOST_FAILURE) or by a stalled ring producer whose consumers' bounded waits run out
+        (BM25_INJECT_STALL)."""
+        _raise(self._lib, self._lib.bm25_test_inject(self._handle, int(what)), self._handle)
 
     def kernel_timing(self, enable=True):
         """Record CUDA events around the main search kernel of each ``search_device`` call."""

@@ -59,6 +59,9 @@ typedef struct bm25_options {
     float prune_route;       /* pruned Searches of 32 queries or more: a query keeping more than this share of
                                 its 128-document blocks is streamed by the tile-group kernel instead
                                 (0 = 0.3; negative = never) */
+    int64_t wait_budget_cycles; /* SM clock cycles a bounded wait of the ring kernels (0 and 4) spends
+                                   before it gives up and the Search reports a device error
+                                   (0 = 4e9, about 2 s) */
 } bm25_options;
 
 /* Search kernels (bm25_options.kernel):
@@ -229,6 +232,23 @@ int bm25_close(bm25_handle *handle);
 /* Closes (if needed) and frees the handle itself. */
 void bm25_destroy(bm25_handle *handle);
 
+/*
+ * Test hook, no counterpart in the reference: arms a one-shot failure of the next
+ * bm25_search on `handle` so the error contract can be tested without faulting a GPU
+ * (the reference tests it with a mocked session whose Search throws,
+ * ut/cases/bm25/sdk_facade_tests.cpp:47-56).
+ *   BM25_INJECT_HOST_FAILURE: the Search runs, then is reported as a device failure
+ *     (BM25_ERR_INNER_ERROR, the session poisoned); handle NULL arms it for the next
+ *     bm25_search of any handle in the process.
+ *   BM25_INJECT_STALL: the tile-group kernel's producer issues no ring stage, so its
+ *     consumers' bounded waits run out (options.wait_budget_cycles) and the kernel
+ *     reports a timeout in the device status: BM25_ERR_INNER_ERROR, session poisoned.
+ *     Needs a handle; other kernels have no wait to stall and ignore it.
+ */
+#define BM25_INJECT_HOST_FAILURE 1
+#define BM25_INJECT_STALL 2
+int bm25_test_inject(bm25_handle *handle, int32_t what);
+
 /* Last error message of the handle (ErrorInfo, common/bm25/error_info.h:8-20); code = CUDA error or 0. */
 int bm25_last_error(const bm25_handle *handle, char *buffer, size_t length, int64_t *code);
 
@@ -365,6 +385,8 @@ typedef struct bm25_info {
     int64_t graph_replays, searches;
     int32_t kernel, ring_stages, grid, smem_bytes, ring_chunk;
     int32_t query_capacity, word_capacity, max_k, prune;
+    int64_t graph_instantiations; /* CUDA graphs instantiated since create */
+    int64_t graphs_cached;        /* instantiated graphs held now */
 } bm25_info;
 int bm25_get_info(const bm25_handle *handle, bm25_info *info);
 

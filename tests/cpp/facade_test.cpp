@@ -5,6 +5,7 @@
 //                                     packed queries in Q, write scores + labels to OUT,
 //                                     checking the error behaviour around it
 #include "AscendIndexBm25.h"
+#include "bm25_b200.h"
 
 #include <cstdio>
 #include <cstdlib>
@@ -136,6 +137,22 @@ static int DeviceRun(const std::string &dir, const std::string &qfile, const std
     EXPECT(index.Close() == ascend::APP_ERR_OK);
     EXPECT(index.Search(queries, result) == ascend::APP_ERR_ILLEGAL_OPERATION);
     EXPECT(index.Close() == ascend::APP_ERR_OK);
+
+    // a device failure (injected on the host through the engine's test hook, as the reference's
+    // facade test mocks a failing session): INNER_ERROR, the output untouched, the session poisoned
+    // (later calls ILLEGAL_OPERATION), and Close still succeeds (sdk_facade_tests.cpp:47-56)
+    AscendIndexBm25 failing;
+    EXPECT(failing.Init(idx, config) == ascend::APP_ERR_OK);
+    Bm25SearchResult kept;
+    EXPECT(failing.Search(queries, kept) == ascend::APP_ERR_OK);
+    const Bm25SearchResult before = kept;
+    EXPECT(bm25_test_inject(nullptr, BM25_INJECT_HOST_FAILURE) == BM25_OK);
+    EXPECT(failing.Search(queries, kept) == ascend::APP_ERR_INNER_ERROR);
+    EXPECT(std::string(failing.GetLastError().message.data()).find("Injected device failure") != std::string::npos);
+    EXPECT(kept.scores == before.scores && kept.labels == before.labels);
+    EXPECT(failing.Search(queries, kept) == ascend::APP_ERR_ILLEGAL_OPERATION);
+    EXPECT(failing.Close() == ascend::APP_ERR_OK);
+    EXPECT(failing.Close() == ascend::APP_ERR_OK);
 
     std::ofstream f(out, std::ios::binary);
     f.write(reinterpret_cast<const char *>(first.scores.data()),

@@ -39,12 +39,12 @@ def _queries(index, seed, count):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize('tile_docs', [1024, 2048])
-def test_large_k_plain_matches_oracle(pkg, oracle_mod, corpus, cuda_ok, tile_docs):
+@pytest.mark.parametrize('kernel,tile_docs', [(5, 1024), (4, 1024), (4, 2048)])
+def test_large_k_plain_matches_oracle(pkg, oracle_mod, corpus, cuda_ok, kernel, tile_docs):
     index, data = corpus
     offsets, words = _queries(index, tile_docs, 29)
     with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, query_capacity=64,
-                                  word_capacity=1024, max_k=1024, tile_docs=tile_docs) as s:
+                                  word_capacity=1024, max_k=1024, tile_docs=tile_docs, kernel=kernel) as s:
         for k in (33, 100, 1000, 1024, 10):
             want = oracle_mod.search(index.offsets, index.docs, data, index.num_docs, offsets, words, k)
             assert_same_topk(*s.search((offsets, words), k), *want, f'k={k}')

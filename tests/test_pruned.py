@@ -61,8 +61,8 @@ def corpus(pkg, oracle_mod):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize('tile_docs', [1024, 2048])
-def test_pruned_matches_oracle(pkg, oracle_mod, corpus, cuda_ok, tile_docs):
+@pytest.mark.parametrize('kernel,tile_docs', [(5, 1024), (4, 1024), (4, 2048)])
+def test_pruned_matches_oracle(pkg, oracle_mod, corpus, cuda_ok, kernel, tile_docs):
     index, data = corpus
     rng = np.random.default_rng(tile_docs)
     # besides random rows: a duplicated word, an empty query, and 40 words (the block scorer
@@ -72,7 +72,8 @@ def test_pruned_matches_oracle(pkg, oracle_mod, corpus, cuda_ok, tile_docs):
     offsets, words = pack(rows)
     q = len(rows)
     with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, query_capacity=64,
-                                  word_capacity=1024, max_k=32, tile_docs=tile_docs, prune=True) as s:
+                                  word_capacity=1024, max_k=32, tile_docs=tile_docs, prune=True,
+                                  kernel=kernel) as s:
         for k in (10, 32):
             want_s, want_i, full = oracle_mod.search(index.offsets, index.docs, data, index.num_docs, offsets, words,
                                                      k, full=True)
