@@ -79,6 +79,8 @@ static size_t Align32(size_t n) { return (n + 31) & ~size_t(31); }
 // the tile-group kernel) and the tile-group kernel.
 static bool TileFamily(int kernel) { return kernel == BM25_KERNEL_TILE_GROUP || kernel == BM25_KERNEL_WARP_TILE; }
 
+static_assert(bm25k::kTermTop == bm25k::kTermTopK, "one layout of the per-term top scores");
+
 // Tiles per claim of the warp-tile kernel.
 constexpr int kWtClaimTiles = 4;
 
@@ -824,6 +826,17 @@ class Engine {
             }
             Cuda(cudaStreamSynchronize(stream_), "directory kernel");
         }
+        if (opts_.prune || plan_.kernel == BM25_KERNEL_WARP_TILE) {
+            // per-term statistics: the 32 largest posting scores (the warp-tile kernel's starting
+            // bounds; the learned bounds' features) and the mean posting score
+            d_term_top_ = static_cast<float *>(Alloc(vocab_ * bm25k::kTermTop * sizeof(float), "cudaMalloc term top"));
+            d_term_mean_ = static_cast<float *>(Alloc(vocab_ * sizeof(float), "cudaMalloc term mean"));
+            const int grid = (int)std::min<long long>((vocab_ + 7) / 8, 148 * 16);
+            bm25k::TermStatsKernel<<<grid, 256, 0, stream_>>>((const long long *)d_indptr_, d_data_, vocab_,
+                                                               d_term_top_, d_term_mean_);
+            Cuda(cudaGetLastError(), "term statistics kernel launch");
+            Cuda(cudaStreamSynchronize(stream_), "term statistics kernel");
+        }
         if (opts_.prune) {
             item_cap_ = (long long)opts_.query_capacity * tiles;
             d_items_ = static_cast<uint4 *>(Alloc(item_cap_ * sizeof(uint4), "cudaMalloc block work list"));
@@ -831,15 +844,8 @@ class Engine {
                                                "cudaMalloc word rows"));
             d_item_count_ = static_cast<unsigned *>(Alloc(4 * sizeof(unsigned), "cudaMalloc block work count"));
             d_safe_ = static_cast<float *>(Alloc(opts_.query_capacity * sizeof(float), "cudaMalloc safe bounds"));
-            d_term_top_ = static_cast<float *>(Alloc(vocab_ * bm25k::kTermTop * sizeof(float), "cudaMalloc term top"));
-            d_term_mean_ = static_cast<float *>(Alloc(vocab_ * sizeof(float), "cudaMalloc term mean"));
             d_model_ = static_cast<float *>(Alloc(bm25mlp::kParams * sizeof(float), "cudaMalloc model"));
             d_tau_ = static_cast<float *>(Alloc(opts_.query_capacity * sizeof(float), "cudaMalloc tau"));
-            const int grid = (int)std::min<long long>((vocab_ + 7) / 8, 148 * 16);
-            bm25k::TermStatsKernel<<<grid, 256, 0, stream_>>>((const long long *)d_indptr_, d_data_, vocab_,
-                                                               d_term_top_, d_term_mean_);
-            Cuda(cudaGetLastError(), "term statistics kernel launch");
-            Cuda(cudaStreamSynchronize(stream_), "term statistics kernel");
         }
         // Query packet / result arenas (fixed_query_packet.h:15-25 layout).
         word_offset_ = Align32((opts_.query_capacity + 1) * sizeof(int64_t));
@@ -1091,6 +1097,7 @@ class Engine {
             sa.plan_rows = plan_rows_;
             sa.prefetch = 1;
             sa.wait_budget = opts_.wait_budget_cycles;
+            sa.term_top = plan_.kernel == BM25_KERNEL_WARP_TILE ? d_term_top_ : nullptr;
             sa.inject = d_inject_;
             if (warp_tile)
                 bm25k::PlanRowsKernel<<<bm25k::PlanRowsGrid(opts_.word_capacity, plan_.tiles, sms_),

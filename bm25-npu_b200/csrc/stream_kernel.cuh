@@ -152,6 +152,10 @@ struct StreamArgs {
     // runs are prefetched into L2 when the claim is taken
     int *plan_rows;
     int prefetch;
+    // [vocab][32] each term's 32 largest posting scores (descending, 0 past its document
+    // frequency): the warp-tile kernel starts a K <= 32 query's running bound at the largest K-th
+    // score of its words, which K documents reach (nullptr: start at 0)
+    const float *term_top;
     // cycles a bounded wait spends before it gives up (0: kWaitBudget)
     long long wait_budget;
     // test hook: a nonzero word makes the tile-group kernel's producer issue no ring stage, so its

@@ -24,6 +24,16 @@
 //     cpu_index_search.h:176-188);
 //   * then it selects the tile's top-K at or above the query's running bound
 //     (TileSelectAppend, shared with the tile-group kernel) and clears the row.
+//     The lanes keep the largest sum they wrote, which is the tile's largest
+//     score (contributions are non-negative, so a document's final sum is the
+//     largest it takes); a tile whose largest score is below the bound only
+//     clears its row.
+// A K <= 32 query's running bound starts at the largest, over its words, of the
+// word's K-th largest posting score (term statistics kept at create): K
+// documents hold that word with at least that score, and a non-negative FP32
+// sum is at least each of its terms, so K documents reach it.  Without it the
+// first wave of claims (every warp's first tiles) would run with no bound and
+// select and append in full.
 // No producer warp, no mbarrier, no wait on another warp: the only latencies
 // are the warp's own loads.  FinalSelectKernel finishes every query.
 //
@@ -40,6 +50,7 @@ constexpr int kWtThreads = kWtWarps * 32;
 constexpr int kWtWindow = 128;       // postings per window (4 per lane)
 constexpr int kWtSlots = 4;          // windows loaded before their adds
 constexpr int kPlanRowChunk = 2048;  // plan row entries per PlanRowsKernel CTA (grid.y)
+constexpr int kTermTopK = 32;        // largest posting scores kept per term
 
 struct WtShared {
     WarpSel wsel[kWtWarps];
@@ -71,8 +82,10 @@ __device__ __forceinline__ void PrefetchL2(const void *p, unsigned bytes)
 // Posting positions of query word w at the bounds of tiles t0 .. t0 + kC (clamped at the last
 // bound): off[j] = first posting of the word's list in tile t0 + j.  Words outside the vocabulary
 // have no postings (a negative one is flagged).
+// seed: raised to the word's k-th largest posting score (k <= 32 and term statistics present).
 template <int kC>
-__device__ __forceinline__ void WtWordOffsets(const StreamArgs &a, long long w, int t0, int *off, unsigned &bad)
+__device__ __forceinline__ void WtWordOffsets(const StreamArgs &a, long long w, int t0, int *off, unsigned &bad,
+                                              int k, float &seed)
 {
     const int term = __ldg(a.words + w);
     if (term < 0 || term >= a.vocab) {
@@ -83,6 +96,8 @@ __device__ __forceinline__ void WtWordOffsets(const StreamArgs &a, long long w, 
             off[j] = 0;
         return;
     }
+    if (a.term_top && k <= kTermTopK)
+        seed = fmaxf(seed, __ldg(a.term_top + (long long)term * kTermTopK + (k - 1)));
     const int base = (int)__ldg(a.indptr + term);
     const int r = a.dir_row ? __ldg(a.dir_row + term) : -1;
     if (r >= 0) {
@@ -165,21 +180,21 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
             nw = 0;
         }
         const int k = kLean ? a.k : QueryK(a, q);
-        const unsigned thr_bits = __ldcg(a.threshold + q);
-        const unsigned slot_bits = lane < k ? __ldcg(a.tslots + (long long)q * 32 + lane) : 0xffffffffu;
         int offA[kC + 1], offB[kC + 1];  // words lane and lane + 32
 #pragma unroll
         for (int j = 0; j <= kC; ++j)
             offA[j] = offB[j] = 0;
+        float seed = 0.0f;
         if (lane < nw)
-            WtWordOffsets<kC>(a, qb + lane, t0, offA, bad);
+            WtWordOffsets<kC>(a, qb + lane, t0, offA, bad, k, seed);
         if (lane + 32 < nw)
-            WtWordOffsets<kC>(a, qb + lane + 32, t0, offB, bad);
+            WtWordOffsets<kC>(a, qb + lane + 32, t0, offB, bad, k, seed);
         if (a.prefetch) {
             PrefetchRun(a, offA[0], offA[kC]);
             PrefetchRun(a, offB[0], offB[kC]);
         }
-        const float thr = fmaxf(__uint_as_float(thr_bits), __uint_as_float(__reduce_min_sync(kFull, slot_bits)));
+        // the largest K-th posting score of the query's words (0 for K > 32)
+        seed = __uint_as_float(__reduce_max_sync(kFull, __float_as_uint(seed)));  // non-negative: bit order
         ++n_claims;
         n_tiles += (unsigned)nt;
         n_post += (unsigned)(offA[kC] - offA[0]) + (unsigned)(offB[kC] - offB[0]);
@@ -188,6 +203,10 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
         for (int j = 0; j < nt; ++j) {
             const int tile = t0 + j;
             const int base_doc = tile * kWtTile;
+            // the query's running bound, read now and used after the adds (other warps raise it)
+            const unsigned thr_bits = lane == 0 ? __ldcg(a.threshold + q) : 0u;
+            const unsigned slot_bits = lane < k ? __ldcg(a.tslots + (long long)q * 32 + lane) : 0xffffffffu;
+            float rmax = 0.0f;  // the largest sum this lane wrote
             // windows of 128 postings of every word in this tile, numbered in word order
             const int bA = offA[0], eA = offA[1], bB = offB[0], eB = offB[1];
             const int nA = (eA - bA + kWtWindow - 1) / kWtWindow;
@@ -260,13 +279,23 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
                             r[v] = row[d[v]];
 #pragma unroll
                     for (int v = 0; v < 4; ++v)
-                        if ((unsigned)d[v] < (unsigned)kWtTile)
-                            row[d[v]] = r[v] + vals[u][v];
+                        if ((unsigned)d[v] < (unsigned)kWtTile) {
+                            const float x = r[v] + vals[u][v];
+                            row[d[v]] = x;
+                            rmax = fmaxf(rmax, x);
+                        }
                 }
             }
             __syncwarp();
-            if (W > 0) {  // a tile without postings has an all-zero row: nothing to select
+            const float thr = fmaxf(fmaxf(seed, __uint_as_float(__shfl_sync(kFull, thr_bits, 0))),
+                                    __uint_as_float(__reduce_min_sync(kFull, slot_bits)));
+            if (__any_sync(kFull, rmax >= fmaxf(thr, kLeastPositive))) {
                 bad |= TileSelectAppend<kWtTile, kLean>(a, ws, row4, thr, q, tile, lane);
+                __syncwarp();
+            } else if (W > 0) {  // nothing reaches the bound: clear the row (a tile without postings is clear)
+#pragma unroll
+                for (int z = 0; z < kWtTile / 128; ++z)
+                    row4[lane + 32 * z] = make_float4(0.f, 0.f, 0.f, 0.f);
                 __syncwarp();
             }
 #pragma unroll
