@@ -47,6 +47,7 @@ class Options(ctypes.Structure):
         ('candidate_capacity', c_int64),
         ('prune_route', c_float),
         ('wait_budget_cycles', c_int64),
+        ('dense_density', c_float),
     ]
 
 
@@ -76,6 +77,7 @@ class Info(ctypes.Structure):
         ('prune', c_int32),
         ('graph_instantiations', c_int64),
         ('graphs_cached', c_int64),
+        ('dense_rows', c_int64),
     ]
 
 

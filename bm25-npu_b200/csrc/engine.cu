@@ -198,6 +198,7 @@ class Engine {
         Check(o.max_k <= docs, "max_k exceeds the document count");
         Check(o.query_capacity >= 1 && o.query_capacity <= 65535, "query_capacity must be in [1, 65535]");
         Check(o.wait_budget_cycles >= 0, "wait_budget_cycles must be >= 0");
+        Check(std::isfinite(o.dense_density) && o.dense_density <= 1.0f, "dense_density must be at most 1");
         Check(o.word_capacity >= 0 && o.word_capacity <= 16777216, "word_capacity must be in [0, 2^24]");
         Check(!o.prune || TileFamily(o.kernel), "prune needs the warp-tile or tile-group kernel");
         Cuda(cudaSetDevice(o.device_id), "cudaSetDevice");
@@ -673,6 +674,7 @@ class Engine {
         info->prune = opts_.prune ? 1 : 0;
         info->graph_instantiations = instantiations_;
         info->graphs_cached = (int64_t)graphs_.size();
+        info->dense_rows = dense_rows_;
     }
 
   private:
@@ -826,6 +828,8 @@ class Engine {
             }
             Cuda(cudaStreamSynchronize(stream_), "directory kernel");
         }
+        if (plan_.kernel == BM25_KERNEL_WARP_TILE && opts_.dense_density >= 0.0f)
+            BuildDense(dfs);
         if (opts_.prune || plan_.kernel == BM25_KERNEL_WARP_TILE) {
             // per-term statistics: the 32 largest posting scores (the warp-tile kernel's starting
             // bounds; the learned bounds' features) and the mean posting score
@@ -980,6 +984,40 @@ class Engine {
         Cuda(cudaDeviceSynchronize(), "index preparation");
     }
 
+    // Dense rows of the warp-tile kernel: the terms with df >= density * N, largest first, within a
+    // byte budget (the index's own size, at most 16 GiB); each row holds tiles * 1024 scores.
+    void BuildDense(const std::vector<int64_t> &dfs)
+    {
+        const double density = opts_.dense_density > 0.0f ? opts_.dense_density : 0.5;
+        const int64_t min_df = std::max<int64_t>(1, (int64_t)std::ceil(density * (double)docs_));
+        dense_stride_ = (int64_t)plan_.tiles * plan_.tile_docs;
+        const int64_t budget = std::min<int64_t>(int64_t(16) << 30, std::max<int64_t>(index_bytes_, 1));
+        std::vector<int32_t> terms;
+        for (int64_t t = 0; t < vocab_; ++t)
+            if (dfs[t] >= min_df)
+                terms.push_back((int32_t)t);
+        std::sort(terms.begin(), terms.end(), [&](int32_t x, int32_t y) { return dfs[x] > dfs[y] || (dfs[x] == dfs[y] && x < y); });
+        const int64_t fit = budget / (dense_stride_ * (int64_t)sizeof(float));
+        if ((int64_t)terms.size() > fit)
+            terms.resize((size_t)std::max<int64_t>(0, fit));
+        dense_rows_ = (int64_t)terms.size();
+        std::vector<int32_t> row_of(vocab_, -1);
+        for (size_t r = 0; r < terms.size(); ++r)
+            row_of[terms[r]] = (int32_t)r;
+        d_dense_row_ = static_cast<int32_t *>(Alloc(vocab_ * sizeof(int32_t), "cudaMalloc dense row"));
+        Cuda(cudaMemcpy(d_dense_row_, row_of.data(), vocab_ * sizeof(int32_t), cudaMemcpyHostToDevice), "dense upload");
+        if (terms.empty())
+            return;
+        d_dense_ = static_cast<float *>(Alloc((size_t)dense_rows_ * dense_stride_ * sizeof(float), "cudaMalloc dense rows"));
+        Cuda(cudaMemset(d_dense_, 0, (size_t)dense_rows_ * dense_stride_ * sizeof(float)), "cudaMemset dense rows");
+        int32_t *d_terms = static_cast<int32_t *>(Alloc(terms.size() * sizeof(int32_t), "cudaMalloc dense terms"));
+        Cuda(cudaMemcpy(d_terms, terms.data(), terms.size() * sizeof(int32_t), cudaMemcpyHostToDevice), "dense upload");
+        bm25k::BuildDenseKernel<<<dim3(256, (unsigned)dense_rows_), 256, 0, stream_>>>(
+            (const long long *)d_indptr_, d_indices_, d_data_, d_terms, d_dense_, dense_stride_);
+        Cuda(cudaGetLastError(), "dense row kernel launch");
+        Cuda(cudaStreamSynchronize(stream_), "dense row kernel");
+    }
+
     // tau / exact: the pruned Search's starting bounds and exactness flags (nullptr: plain Search).
     void Launch(int q, int k, const int64_t *qoffsets, const int32_t *words, float *out_scores, int32_t *out_ids,
                 unsigned *status, cudaStream_t s, const float *tau = nullptr, int32_t *exact = nullptr,
@@ -1098,6 +1136,9 @@ class Engine {
             sa.prefetch = 1;
             sa.wait_budget = opts_.wait_budget_cycles;
             sa.term_top = plan_.kernel == BM25_KERNEL_WARP_TILE ? d_term_top_ : nullptr;
+            sa.dense = d_dense_;
+            sa.dense_row = d_dense_row_;
+            sa.dense_stride = dense_stride_;
             sa.inject = d_inject_;
             if (warp_tile)
                 bm25k::PlanRowsKernel<<<bm25k::PlanRowsGrid(opts_.word_capacity, plan_.tiles, sms_),
@@ -1411,6 +1452,9 @@ class Engine {
     long long cand_cap_ = 0;
     bm25k::PlanEntry *plan_entries_ = nullptr;
     int *plan_rows_ = nullptr;
+    float *d_dense_ = nullptr;  // dense rows of the most frequent terms (warp-tile kernel)
+    int32_t *d_dense_row_ = nullptr;
+    int64_t dense_rows_ = 0, dense_stride_ = 0;
     size_t tg_smem_ = 0;  // tile-group kernel: dynamic shared memory and grid
     int tg_grid_ = 0;
     int sms_ = 148;

@@ -156,6 +156,11 @@ struct StreamArgs {
     // frequency): the warp-tile kernel starts a K <= 32 query's running bound at the largest K-th
     // score of its words, which K documents reach (nullptr: start at 0)
     const float *term_top;
+    // [dense row][dense_stride] per-document scores of the terms kept dense (0 where absent);
+    // dense_row [vocab]: a term's dense row or -1
+    const float *dense;
+    const int *dense_row;
+    long long dense_stride;
     // cycles a bounded wait spends before it gives up (0: kWaitBudget)
     long long wait_budget;
     // test hook: a nonzero word makes the tile-group kernel's producer issue no ring stage, so its

@@ -504,6 +504,19 @@ __global__ void BuildContributionsKernel(const long long *offsets, int vocab, lo
 // Per-tile posting directory for long lists:
 // dir[row][j] = (first posting of the term with doc >= j * tile_docs) - indptr[t],
 // one thread per entry, lower_bound over the term's sorted doc ids.
+// Dense rows: dense[r][doc] = the posting score of term dense_terms[r] in doc (the rows are
+// zeroed before).  Grid y: rows; grid x strides over the term's postings.
+__global__ void BuildDenseKernel(const long long *indptr, const int *indices, const float *data,
+                                 const int *dense_terms, float *dense, long long stride)
+{
+    const int t = dense_terms[blockIdx.y];
+    const long long s = indptr[t], e = indptr[t + 1];
+    float *row = dense + (long long)blockIdx.y * stride;
+    for (long long p = s + (long long)blockIdx.x * blockDim.x + threadIdx.x; p < e;
+         p += (long long)gridDim.x * blockDim.x)
+        row[indices[p]] = data[p];
+}
+
 __global__ void BuildDirectoryKernel(const long long *indptr, const int *indices, const int *dir_terms, long long rows,
                                      int tile_docs, int tiles, int *dir, long long stride)
 {

@@ -72,6 +72,14 @@ __device__ __forceinline__ float LdStreamF32(const float *p)
     asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
     return v;
 }
+__device__ __forceinline__ float4 LdStreamF32x4(const float4 *p)
+{
+    float4 v;
+    asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+        : "l"(p));
+    return v;
+}
 
 // Prefetch of [p, p + bytes) into L2 (p 16-byte aligned, bytes a multiple of 16).
 __device__ __forceinline__ void PrefetchL2(const void *p, unsigned bytes)
@@ -83,11 +91,13 @@ __device__ __forceinline__ void PrefetchL2(const void *p, unsigned bytes)
 // bound): off[j] = first posting of the word's list in tile t0 + j.  Words outside the vocabulary
 // have no postings (a negative one is flagged).
 // seed: raised to the word's k-th largest posting score (k <= 32 and term statistics present).
+// drow: the term's dense row, or -1.
 template <int kC>
 __device__ __forceinline__ void WtWordOffsets(const StreamArgs &a, long long w, int t0, int *off, unsigned &bad,
-                                              int k, float &seed)
+                                              int k, float &seed, int &drow)
 {
     const int term = __ldg(a.words + w);
+    drow = -1;
     if (term < 0 || term >= a.vocab) {
         if (term < 0)
             bad |= kStatusBadWord;
@@ -98,6 +108,8 @@ __device__ __forceinline__ void WtWordOffsets(const StreamArgs &a, long long w, 
     }
     if (a.term_top && k <= kTermTopK)
         seed = fmaxf(seed, __ldg(a.term_top + (long long)term * kTermTopK + (k - 1)));
+    if (a.dense_row)
+        drow = __ldg(a.dense_row + term);
     const int base = (int)__ldg(a.indptr + term);
     const int r = a.dir_row ? __ldg(a.dir_row + term) : -1;
     if (r >= 0) {
@@ -115,10 +127,15 @@ __device__ __forceinline__ void WtWordOffsets(const StreamArgs &a, long long w, 
 
 // L2 prefetch of postings [lo, hi) of both arrays, widened to 16-byte boundaries (the arrays are
 // padded past their end).
-__device__ __forceinline__ void PrefetchRun(const StreamArgs &a, int lo, int hi)
+__device__ __forceinline__ void PrefetchRun(const StreamArgs &a, int lo, int hi, int drow, int t0, int nt)
 {
     if (lo >= hi)
         return;
+    if (drow >= 0) {  // the dense row's scores of the claim's tiles
+        PrefetchL2(a.dense + (long long)drow * a.dense_stride + (long long)t0 * kWtTile,
+                   (unsigned)nt * kWtTile * (unsigned)sizeof(float));
+        return;
+    }
     const int p0 = lo & ~3, p1 = (hi + 3) & ~3;
     const unsigned bytes = (unsigned)(p1 - p0) * 4u;
     PrefetchL2(a.indices + p0, bytes);
@@ -185,14 +202,16 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
         for (int j = 0; j <= kC; ++j)
             offA[j] = offB[j] = 0;
         float seed = 0.0f;
+        int drowA = -1, drowB = -1;
         if (lane < nw)
-            WtWordOffsets<kC>(a, qb + lane, t0, offA, bad, k, seed);
+            WtWordOffsets<kC>(a, qb + lane, t0, offA, bad, k, seed, drowA);
         if (lane + 32 < nw)
-            WtWordOffsets<kC>(a, qb + lane + 32, t0, offB, bad, k, seed);
+            WtWordOffsets<kC>(a, qb + lane + 32, t0, offB, bad, k, seed, drowB);
         if (a.prefetch) {
-            PrefetchRun(a, offA[0], offA[kC]);
-            PrefetchRun(a, offB[0], offB[kC]);
+            PrefetchRun(a, offA[0], offA[kC], drowA, t0, nt);
+            PrefetchRun(a, offB[0], offB[kC], drowB, t0, nt);
         }
+        const unsigned denseA = __ballot_sync(kFull, drowA >= 0), denseB = __ballot_sync(kFull, drowB >= 0);
         // the largest K-th posting score of the query's words (0 for K > 32)
         seed = __uint_as_float(__reduce_max_sync(kFull, __float_as_uint(seed)));  // non-negative: bit order
         ++n_claims;
@@ -209,8 +228,9 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
             float rmax = 0.0f;  // the largest sum this lane wrote
             // windows of 128 postings of every word in this tile, numbered in word order
             const int bA = offA[0], eA = offA[1], bB = offB[0], eB = offB[1];
-            const int nA = (eA - bA + kWtWindow - 1) / kWtWindow;
-            const int nB = (eB - bB + kWtWindow - 1) / kWtWindow;
+            // a dense word with postings in the tile is one window, added from its dense row
+            const int nA = drowA >= 0 ? (eA > bA ? 1 : 0) : (eA - bA + kWtWindow - 1) / kWtWindow;
+            const int nB = drowB >= 0 ? (eB > bB ? 1 : 0) : (eB - bB + kWtWindow - 1) / kWtWindow;
             const int cumA = WarpInclusiveSum(nA, lane);
             const int WA = __shfl_sync(kFull, cumA, 31);
             int cumB = 0, W = WA;
@@ -219,32 +239,69 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
                 W = __shfl_sync(kFull, cumB, 31);
             }
             int prev_word = -1;
-            for (int i0 = 0; i0 < W; i0 += kWtSlots) {
+            // word of window i (uniform): lane index among the first 32 words, or 32 + among the rest
+            auto word_of = [&](int i) {
+                return i < WA ? __popc(__ballot_sync(kFull, cumA <= i))
+                              : 32 + __popc(__ballot_sync(kFull, cumB <= i));
+            };
+            auto is_dense = [&](int s) { return s < 32 ? ((denseA >> s) & 1u) != 0 : ((denseB >> (s - 32)) & 1u) != 0; };
+            for (int i0 = 0; i0 < W;) {
+                const int s0 = word_of(i0);
+                if (is_dense(s0)) {
+                    // dense word: the tile's 1024 scores, 8 x 128 bits per lane, added in place
+                    const int drow = s0 < 32 ? __shfl_sync(kFull, drowA, s0) : __shfl_sync(kFull, drowB, s0 - 32);
+                    const float4 *src = reinterpret_cast<const float4 *>(a.dense + (long long)drow * a.dense_stride +
+                                                                         base_doc);
+                    float4 v[kWtTile / 128];
+#pragma unroll
+                    for (int z = 0; z < kWtTile / 128; ++z)
+                        v[z] = LdStreamF32x4(src + lane + 32 * z);
+                    __syncwarp();  // the previous word's adds are in the row before this word's
+                    prev_word = s0;
+#pragma unroll
+                    for (int z = 0; z < kWtTile / 128; ++z) {
+                        float4 r = row4[lane + 32 * z];
+                        r.x += v[z].x;
+                        r.y += v[z].y;
+                        r.z += v[z].z;
+                        r.w += v[z].w;
+                        row4[lane + 32 * z] = r;
+                        rmax = fmaxf(rmax, fmaxf(fmaxf(r.x, r.y), fmaxf(r.z, r.w)));
+                    }
+                    ++i0;
+                    continue;
+                }
+                // up to kWtSlots windows of postings, ending before the next dense word
                 int ids[kWtSlots][4];
                 float vals[kWtSlots][4];
                 int word[kWtSlots];
+                bool more = true;
+                int taken = 0;
 #pragma unroll
                 for (int u = 0; u < kWtSlots; ++u) {
                     const int i = i0 + u;
                     int p0 = 0, p1 = 0;
                     word[u] = -1;
-                    if (i < W) {  // uniform
-                        int s, first, b, e;
-                        if (i < WA) {
-                            s = __popc(__ballot_sync(kFull, cumA <= i));
-                            first = __shfl_sync(kFull, cumA - nA, s);
-                            b = __shfl_sync(kFull, bA, s);
-                            e = __shfl_sync(kFull, eA, s);
-                            word[u] = s;
+                    if (more && i < W) {  // uniform
+                        const int s = u == 0 ? s0 : word_of(i);
+                        if (is_dense(s)) {
+                            more = false;
                         } else {
-                            s = __popc(__ballot_sync(kFull, cumB <= i));
-                            first = __shfl_sync(kFull, cumB - nB, s);
-                            b = __shfl_sync(kFull, bB, s);
-                            e = __shfl_sync(kFull, eB, s);
-                            word[u] = 32 + s;
+                            int first, b, e;
+                            if (s < 32) {
+                                first = __shfl_sync(kFull, cumA - nA, s);
+                                b = __shfl_sync(kFull, bA, s);
+                                e = __shfl_sync(kFull, eA, s);
+                            } else {
+                                first = __shfl_sync(kFull, cumB - nB, s - 32);
+                                b = __shfl_sync(kFull, bB, s - 32);
+                                e = __shfl_sync(kFull, eB, s - 32);
+                            }
+                            word[u] = s;
+                            p0 = b + (i - first) * kWtWindow;
+                            p1 = min(p0 + kWtWindow, e);
+                            taken = u + 1;
                         }
-                        p0 = b + (i - first) * kWtWindow;
-                        p1 = min(p0 + kWtWindow, e);
                     }
 #pragma unroll
                     for (int v = 0; v < 4; ++v) {
@@ -260,7 +317,7 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
 #pragma unroll
                 for (int u = 0; u < kWtSlots; ++u) {
                     if (word[u] < 0)
-                        break;  // uniform: no more windows
+                        break;  // uniform: no more windows in this batch
                     if (word[u] != prev_word) {
                         __syncwarp();  // the previous word's adds are in the row before this word's
                         prev_word = word[u];
@@ -285,6 +342,7 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
                             rmax = fmaxf(rmax, x);
                         }
                 }
+                i0 += taken;
             }
             __syncwarp();
             const float thr = fmaxf(fmaxf(seed, __uint_as_float(__shfl_sync(kFull, thr_bits, 0))),

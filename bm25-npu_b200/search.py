@@ -71,7 +71,7 @@ def pack_queries(queries):
 
 def _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes, stream,
              kernel=5, ring_stages=0, ring_chunk=0, prune=False, candidate_capacity=0, prune_route=0.0,
-             wait_budget_cycles=0):
+             wait_budget_cycles=0, dense_density=0.0):
     o = n.Options()
     n.engine_library().bm25_default_options(ctypes.byref(o))
     o.device_id = device_id
@@ -89,6 +89,7 @@ def _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_f
     o.candidate_capacity = candidate_capacity
     o.prune_route = prune_route
     o.wait_budget_cycles = wait_budget_cycles
+    o.dense_density = dense_density
     return o
 
 
@@ -104,7 +105,8 @@ class Bm25Session:
     @classmethod
     def from_csc(cls, indptr, indices, data, num_docs, *, query_capacity=8, word_capacity=24, max_k=10,
                  device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0, stream=None, kernel=5, ring_stages=0,
-                 ring_chunk=0, prune=False, candidate_capacity=0, prune_route=0.0, wait_budget_cycles=0):
+                 ring_chunk=0, prune=False, candidate_capacity=0, prune_route=0.0, wait_budget_cycles=0,
+                 dense_density=0.0):
         """Eager CSC index (bm25s layout): indptr int64 [V+1], indices int32 [M], data float32 [M]."""
         lib = n.engine_library()
         indptr = np.ascontiguousarray(indptr, dtype=np.int64)
@@ -115,7 +117,7 @@ class Bm25Session:
             raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'Index dimensions/endpoints differ')
         o = _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes,
                      stream, kernel, ring_stages, ring_chunk, prune, candidate_capacity, prune_route,
-                     wait_budget_cycles)
+                     wait_budget_cycles, dense_density)
         h = c_void_p()
         status = lib.bm25_create(n.ptr(indptr, c_int64), n.ptr(indices, c_int32), n.ptr(data, c_float), vocab,
                                  int(num_docs), ctypes.byref(o), ctypes.byref(h))
@@ -126,7 +128,7 @@ class Bm25Session:
     def from_lazy(cls, term_offsets, posting_doc_ids, posting_tf, doc_norm, idf, *, k1=1.2, query_capacity=8,
                   word_capacity=24, max_k=10, device_id=0, tile_docs=0, merge_fan_in=0, directory_bytes=0,
                   stream=None, kernel=5, ring_stages=0, ring_chunk=0, prune=False, candidate_capacity=0,
-                  prune_route=0.0, wait_budget_cycles=0):
+                  prune_route=0.0, wait_budget_cycles=0, dense_density=0.0):
         """The reference's resident index (common/bm25/index_data.h:9-42); posting scores built on the GPU."""
         lib = n.engine_library()
         offsets = np.ascontiguousarray(term_offsets, dtype=np.int64)
@@ -139,7 +141,7 @@ class Bm25Session:
             raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'Index dimensions/endpoints differ')
         o = _options(query_capacity, word_capacity, max_k, device_id, tile_docs, merge_fan_in, directory_bytes,
                      stream, kernel, ring_stages, ring_chunk, prune, candidate_capacity, prune_route,
-                     wait_budget_cycles)
+                     wait_budget_cycles, dense_density)
         h = c_void_p()
         status = lib.bm25_create_lazy(n.ptr(offsets, c_int64), n.ptr(docs, c_int32), n.ptr(tf, c_float),
                                       n.ptr(norm, c_float), n.ptr(idf, c_float), vocab, norm.size, float(k1),

@@ -62,6 +62,11 @@ typedef struct bm25_options {
     int64_t wait_budget_cycles; /* SM clock cycles a bounded wait of the ring kernels (0 and 4) spends
                                    before it gives up and the Search reports a device error
                                    (0 = 4e9, about 2 s) */
+    float dense_density;     /* warp-tile kernel: a term whose postings cover at least this share of the
+                                documents is also kept as a dense FP32 row of per-document scores (zero
+                                where absent), read with 128-bit loads instead of scattered
+                                (0 = 0.5, where the row is no more bytes than the postings; negative =
+                                none) */
 } bm25_options;
 
 /* Search kernels (bm25_options.kernel):
@@ -387,6 +392,7 @@ typedef struct bm25_info {
     int32_t query_capacity, word_capacity, max_k, prune;
     int64_t graph_instantiations; /* CUDA graphs instantiated since create */
     int64_t graphs_cached;        /* instantiated graphs held now */
+    int64_t dense_rows;           /* terms kept as dense rows (dense_density) */
 } bm25_info;
 int bm25_get_info(const bm25_handle *handle, bm25_info *info);
 

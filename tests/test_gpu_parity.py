@@ -212,3 +212,32 @@ def test_kernel_timing_hook(pkg, corpus, cuda_ok, kernel):
         assert s.kernel_times().size == 0
         s.kernel_timing(False)
         assert s.device_status() == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('density', [-1.0, 0.0, 0.02, 1.0])
+def test_warp_tile_dense_rows(pkg, oracle_mod, corpus, cuda_ok, density):
+    """The warp-tile kernel adds the terms kept as dense rows (df >= density * N) from those rows and
+    the others from their postings, in query-word order: same bits as the oracle with no dense rows
+    (-1), the default (0: half the documents), nearly every term dense (0.02), and only terms in every
+    document (1.0).  Queries mix dense and sparse words in every order, repeats and unknown words."""
+    spec, index, data = corpus
+    df = np.diff(index.offsets)
+    order = np.argsort(-df)
+    dense_words = [int(x) for x in order[:6]]
+    rng = np.random.default_rng(11)
+    rows = mixed_queries(index.vocab, rng, 20, 0, 10)
+    rows += [dense_words[:3], [dense_words[0], 5, dense_words[1], 7], [9, dense_words[2], dense_words[2], 9],
+             dense_words + [index.vocab + 3], [int(order[-1]), dense_words[4]]]
+    offsets, words = pack(rows)
+    with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, query_capacity=32,
+                                  word_capacity=512, max_k=32, kernel=5, dense_density=density) as s:
+        info = s.info()
+        if density < 0:
+            assert info['dense_rows'] == 0
+        else:
+            d = 0.5 if density == 0 else density
+            assert info['dense_rows'] == int(np.sum(df >= np.ceil(d * index.num_docs)))
+        for k in (1, 10, 32):
+            assert_same_topk(*s.search((offsets, words), k), *_oracle(oracle_mod, index, data, offsets, words, k),
+                             f'density={density} k={k}')
