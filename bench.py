@@ -208,7 +208,48 @@ def cpu_search_leg(index, sets, k, budget_s, max_steps, warmup=1):
             'p50_ms': percentile(times, 50) * 1e3, 'p95_ms': percentile(times, 95) * 1e3}
 
 
-def timed_device(session, step, steps, warmup, flush, stream, world, with_clocks=None):
+class StepCheck:
+    """Bit-checks every timed Search of a leg, as the reference's Measure compares every timed result
+    with its checkpoint (FR/test/ascendhost/bm25/benchmark_common.h:70-95).  After each timed step,
+    outside its timed interval, the step's device outputs are copied into a slot of their own; after
+    the timed loop every slot is compared bit for bit with the expected outputs of that step's batch
+    (the oracle's on rank 0, where they were computed).  `outputs`: the device tensors a step writes;
+    `expected(i)`: the list of host arrays step i must equal (None: not checked); `length`: how many
+    leading elements of each output a step writes (packed batches)."""
+
+    def __init__(self, outputs, expected, steps, length=None):
+        import torch
+        self.outputs = outputs
+        self.expected = expected
+        self.length = length
+        self.slots = [[torch.empty_like(t) for t in outputs] for _ in range(steps)]
+        self.checked = 0
+        self.mismatched = 0
+
+    def capture(self, i):
+        for dst, src in zip(self.slots[i], self.outputs):
+            dst.copy_(src)
+
+    def verify(self, n):
+        for i in range(n):
+            want = self.expected(i)
+            if want is None:
+                continue
+            m = self.length(i) if self.length else None
+            ok = True
+            for got, w in zip(self.slots[i], want):
+                g = got.reshape(-1)[:m].cpu().numpy() if m is not None else got.cpu().numpy()
+                w = np.asarray(w).reshape(-1)[:g.size] if m is not None else np.asarray(w)
+                ok &= bool(np.array_equal(g.reshape(-1).view(np.uint32), w.reshape(-1).view(np.uint32)))
+            self.checked += 1
+            self.mismatched += 0 if ok else 1
+
+    def report(self):
+        return {'checked_searches': self.checked, 'mismatched': self.mismatched,
+                'bit_exact': self.checked > 0 and self.mismatched == 0}
+
+
+def timed_device(session, step, steps, warmup, flush, stream, world, with_clocks=None, check=None):
     """Device-resident steps timed with CUDA events on the launching stream, L2 flushed between
     steps; returns (step ms, main-kernel ms, clocks).
 
@@ -235,7 +276,11 @@ def timed_device(session, step, steps, warmup, flush, stream, world, with_clocks
             starts[i].record(stream)
             step(i)
             ends[i].record(stream)
+            if check is not None:
+                check.capture(i)  # after the step's end event: not in its timed interval
         torch.cuda.synchronize()
+        if check is not None:
+            check.verify(steps)
         clocks = with_clocks.stop() if with_clocks and not marks else None
         status = session.device_status()
         if status != 0:
@@ -303,19 +348,23 @@ def learned_leg(pkg, args, spec, index, session, sets, want, flush, stream, dev_
             for qs, (rs, ri) in zip(sets, want):
                 gs, gi, _ = session.search_learned(qs, K)
                 parity &= bool(np.array_equal(gi, ri) and np.array_equal(gs.view(np.uint32), rs.view(np.uint32)))
-        step_ms, kernel_ms, _ = timed_device(session, step, args.steps, args.warmup, flush, stream, world)
+        check = StepCheck([d_scores, d_ids], lambda i: want[i % 2] if want is not None else None, args.steps)
+        step_ms, kernel_ms, _ = timed_device(session, step, args.steps, args.warmup, flush, stream, world, check=check)
         stats = session.search_stats(reset=True)
         total = max_over_ranks(sum(step_ms), world)
-        host_ms, fallbacks = [], 0
+        host_ms, fallbacks, e2e_checked, e2e_bad = [], 0, 0, 0
         for i in range(args.warmup):
             session.search_learned(sets[i % 2], K)
         for i in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            _, _, exact = session.search_learned(sets[i % 2], K)
+            gs, gi, exact = session.search_learned(sets[i % 2], K)
             host_ms.append((time.perf_counter() - t0) * 1e3)
             fallbacks += int(np.sum(exact == 0))
+            if want is not None:
+                e2e_checked += 1
+                e2e_bad += 0 if same_bits((gs, gi), want[i % 2]) else 1
         e2e_total = max_over_ranks(sum(host_ms), world)
         out[label] = {
             'value': world * Q * args.steps / (total / 1e3), 'unit': UNIT,
@@ -330,6 +379,7 @@ def learned_leg(pkg, args, spec, index, session, sets, want, flush, stream, dev_
             'gpu_launches': args.steps * 8,
             'per_search': {key: v / args.steps for key, v in stats.items()},
             'bit_exact_vs_oracle': parity if want is not None else None,
+            'timed_parity': dict(check.report(), e2e_checked=e2e_checked, e2e_mismatched=e2e_bad),
         }
     out['learned']['model'] = {'train_queries': model.report['train_queries'], 'train_s': train_s,
                                'margin': model.margin, 'val_fallback': model.report['val_fallback'],
@@ -362,24 +412,16 @@ def mix_leg(pkg, args, local, world, flush, stream, rank):
                                         query_capacity=MIX_Q, word_capacity=MIX_Q * hi, max_k=kmax,
                                         device_id=local, prune=True)
     parity = None
+    expected = None
     if rank == 0:
         from oracle import oracle
         data = oracle.contributions(index, spec.k1)
-        ok = True
-        qo, w, ks = batches[0]
-        gs, gi, koff = session.search_batch((qo, w), ks)
-        for k in MIX_KS:
-            sel = np.nonzero(ks == k)[0]
-            rows = [w[qo[i]:qo[i + 1]] for i in sel]
-            o = np.zeros(len(rows) + 1, np.int64)
-            o[1:] = np.cumsum([len(r) for r in rows])
-            rs, ri = oracle.search(index.offsets, index.docs, data, index.num_docs, o,
-                                   np.concatenate(rows).astype(np.int32), int(k), threads=os.cpu_count() or 1)
-            for j, i in enumerate(sel):
-                ok &= bool(np.array_equal(gi[koff[i]:koff[i + 1]], ri[j]) and
-                           np.array_equal(gs[koff[i]:koff[i + 1]].view(np.uint32), rs[j].view(np.uint32)))
+        expected = [oracle_packed(index, data, qo, w, ks, MIX_KS) for qo, w, ks in batches]
         del data
-        parity = {'batch': 0, 'bit_exact': ok, 'against': 'oracle (C restatement), per K group'}
+        ok = all(same_bits(session.search_batch((qo, w), ks)[:2], want)
+                 for (qo, w, ks), want in zip(batches, expected))
+        parity = {'batches': len(batches), 'queries_checked': MIX_Q * len(batches), 'bit_exact': ok,
+                  'against': 'oracle (C restatement), per K group'}
         log(f'mix parity vs oracle: {parity}')
     t = time.perf_counter()
     cap = 1024
@@ -406,6 +448,7 @@ def mix_leg(pkg, args, local, world, flush, stream, rank):
            'model': {'train_queries': model.report['train_queries'], 'train_s': train_s, 'margin': model.margin,
                      'val_fallback': model.report['val_fallback']}}
     steps = max(3, args.steps // 4)
+    totals = [int(ks.sum()) for _, _, ks in batches]
     for label, learned in (('plain', False), ('learned', True)):
         session.set_threshold_model(model if learned else None)
 
@@ -415,10 +458,12 @@ def mix_leg(pkg, args, local, world, flush, stream, rank):
                                         d_s.data_ptr(), d_i.data_ptr(), d_x.data_ptr(), learned,
                                         stream.cuda_stream)
 
-        step_ms, kernel_ms, _ = timed_device(session, step, steps, args.warmup, flush, stream, world)
+        check = StepCheck([d_s, d_i], lambda i: expected[i % 2] if expected else None, steps,
+                          length=lambda i: totals[i % 2])
+        step_ms, kernel_ms, _ = timed_device(session, step, steps, args.warmup, flush, stream, world, check=check)
         stats = session.search_stats(reset=True)
         total = max_over_ranks(sum(step_ms), world)
-        host_ms, fallbacks = [], 0
+        host_ms, fallbacks, e2e_checked, e2e_bad = [], 0, 0, 0
         for i in range(args.warmup):
             session.search_batch(batches[i % 2][:2], batches[i % 2][2], learned=learned)
         for i in range(steps):
@@ -429,13 +474,17 @@ def mix_leg(pkg, args, local, world, flush, stream, rank):
             host_ms.append((time.perf_counter() - t0) * 1e3)
             if learned:
                 fallbacks += int(np.sum(r[3] == 0))
+            if expected:
+                e2e_checked += 1
+                e2e_bad += 0 if same_bits(r[:2], expected[i % 2]) else 1
         e2e_total = max_over_ranks(sum(host_ms), world)
         out[label] = {'value': world * MIX_Q * steps / (total / 1e3), 'unit': UNIT,
                       'p50_ms': percentile(step_ms, 50), 'p95_ms': percentile(step_ms, 95),
                       'main_kernel_ms_avg': sum(kernel_ms) / len(kernel_ms),
                       'e2e': {'value': world * MIX_Q * steps / (e2e_total / 1e3), 'unit': UNIT,
                               'p50_ms': percentile(host_ms, 50), 'p95_ms': percentile(host_ms, 95)},
-                      'per_search': {key: v / steps for key, v in stats.items()}, 'steps': steps}
+                      'per_search': {key: v / steps for key, v in stats.items()}, 'steps': steps,
+                      'timed_parity': dict(check.report(), e2e_checked=e2e_checked, e2e_mismatched=e2e_bad)}
         if learned:
             out[label]['fallback_share'] = fallbacks / (MIX_Q * steps)
     out['speedup_learned_vs_plain'] = out['learned']['value'] / out['plain']['value']
@@ -448,12 +497,14 @@ BLOCKMAX_WORKLOAD = 'blockmax_4p2m'
 BLOCKMAX_Q, BLOCKMAX_TERMS, BLOCKMAX_KS, BLOCKMAX_EVAL = 250, (2, 10), (10, 100), 10_000
 
 
-def parity_by_k(pkg, index, k1, session, qo, w, ks, kset):
-    """One batch with a K per query against the oracle, one oracle call per K (rank 0 only)."""
+def oracle_packed(index, data, qo, w, ks, kset):
+    """The oracle's results of a batch with a K per query, packed by query as bm25_search_batch packs
+    them (query i's ks[i] entries start at ks[0] + ... + ks[i-1]); one oracle call per K."""
     from oracle import oracle
-    data = oracle.contributions(index, k1)
-    ok = True
-    gs, gi, koff = session.search_batch((qo, w), ks)
+    koff = np.zeros(ks.size + 1, np.int64)
+    np.cumsum(ks, out=koff[1:])
+    ps = np.empty(int(koff[-1]), np.float32)
+    pi = np.empty(int(koff[-1]), np.int32)
     for k in kset:
         sel = np.nonzero(ks == k)[0]
         if sel.size == 0:
@@ -464,9 +515,15 @@ def parity_by_k(pkg, index, k1, session, qo, w, ks, kset):
         rs, ri = oracle.search(index.offsets, index.docs, data, index.num_docs, o,
                                np.concatenate(rows).astype(np.int32), int(k), threads=os.cpu_count() or 1)
         for j, i in enumerate(sel):
-            ok &= bool(np.array_equal(gi[koff[i]:koff[i + 1]], ri[j]) and
-                       np.array_equal(gs[koff[i]:koff[i + 1]].view(np.uint32), rs[j].view(np.uint32)))
-    return ok
+            ps[koff[i]:koff[i + 1]] = rs[j]
+            pi[koff[i]:koff[i + 1]] = ri[j]
+    return ps, pi
+
+
+def same_bits(got, want):
+    """(scores, ids) pairs equal bit for bit."""
+    return all(np.array_equal(np.asarray(g).reshape(-1).view(np.uint32), np.asarray(x).reshape(-1).view(np.uint32))
+               for g, x in zip(got, want))
 
 
 def split_queries(qoffsets, words, ks, per_search):
@@ -500,9 +557,17 @@ def blockmax_leg(pkg, args, local, world, flush, stream, rank):
                                         query_capacity=BLOCKMAX_Q, word_capacity=BLOCKMAX_Q * hi, max_k=kmax,
                                         device_id=local, prune=True)
     parity = None
+    expected = None
     if rank == 0:
-        ok = parity_by_k(pkg, index, spec.k1, session, *batches[0], BLOCKMAX_KS)
-        parity = {'batch': 0, 'bit_exact': ok, 'against': 'oracle (C restatement), per K group'}
+        from oracle import oracle
+        t = time.perf_counter()
+        data = oracle.contributions(index, spec.k1)
+        expected = [oracle_packed(index, data, qo, w, ks, BLOCKMAX_KS) for qo, w, ks in batches]
+        del data
+        ok = all(same_bits(session.search_batch((qo, w), ks)[:2], want)
+                 for (qo, w, ks), want in zip(batches, expected))
+        parity = {'batches': n_batches, 'c4_queries_checked': BLOCKMAX_EVAL, 'bit_exact': ok,
+                  'against': 'oracle (C restatement), per K group', 'oracle_s': time.perf_counter() - t}
         log(f'block-max parity vs oracle: {parity}')
     t = time.perf_counter()
     cap = 1024
@@ -529,6 +594,7 @@ def blockmax_leg(pkg, args, local, world, flush, stream, rank):
            'model': {'train_queries': model.report['train_queries'], 'train_s': train_s, 'margin': model.margin,
                      'val_fallback': model.report['val_fallback']}}
     steps = n_batches  # one pass over the held-out set
+    totals = [int(ks.sum()) for _, _, ks in batches]
     for label, learned in (('plain', False), ('learned', True)):
         session.set_threshold_model(model if learned else None)
 
@@ -538,10 +604,12 @@ def blockmax_leg(pkg, args, local, world, flush, stream, rank):
                                         d_s.data_ptr(), d_i.data_ptr(), d_x.data_ptr(), learned,
                                         stream.cuda_stream)
 
-        step_ms, kernel_ms, _ = timed_device(session, step, steps, args.warmup, flush, stream, world)
+        check = StepCheck([d_s, d_i], lambda i: expected[i % n_batches] if expected else None, steps,
+                          length=lambda i: totals[i % n_batches])
+        step_ms, kernel_ms, _ = timed_device(session, step, steps, args.warmup, flush, stream, world, check=check)
         stats = session.search_stats(reset=True)
         total = max_over_ranks(sum(step_ms), world)
-        host_ms, fallbacks = [], 0
+        host_ms, fallbacks, e2e_checked, e2e_bad = [], 0, 0, 0
         for i in range(args.warmup):
             session.search_batch(batches[i % n_batches][:2], batches[i % n_batches][2], learned=learned)
         for i in range(steps):
@@ -552,6 +620,9 @@ def blockmax_leg(pkg, args, local, world, flush, stream, rank):
             host_ms.append((time.perf_counter() - t0) * 1e3)
             if learned:
                 fallbacks += int(np.sum(r[3] == 0))
+            if expected:
+                e2e_checked += 1
+                e2e_bad += 0 if same_bits(r[:2], expected[i]) else 1
         e2e_total = max_over_ranks(sum(host_ms), world)
         per = {key: v / steps for key, v in stats.items()}
         out[label] = {'value': world * BLOCKMAX_Q * steps / (total / 1e3), 'unit': UNIT,
@@ -560,6 +631,7 @@ def blockmax_leg(pkg, args, local, world, flush, stream, rank):
                       'e2e': {'value': world * BLOCKMAX_Q * steps / (e2e_total / 1e3), 'unit': UNIT,
                               'p50_ms': percentile(host_ms, 50), 'p95_ms': percentile(host_ms, 95)},
                       'per_search': per, 'steps': steps,
+                      'timed_parity': dict(check.report(), e2e_checked=e2e_checked, e2e_mismatched=e2e_bad),
                       # postings read block by block plus postings streamed whole (8 B each)
                       'posting_bytes_per_search': 8.0 * (per['postings_read'] + per['postings_copied'])}
         if learned:
@@ -723,8 +795,9 @@ def main():
         session.search_device(o.data_ptr(), w.data_ptr(), Q, K, d_scores.data_ptr(), d_ids.data_ptr(),
                               stream.cuda_stream)
 
+    check = StepCheck([d_scores, d_ids], lambda i: want[i % 2] if want is not None else None, args.steps)
     step_ms, kernel_ms, clock_info = timed_device(session, device_step, args.steps, args.warmup, flush, stream,
-                                                  world, Clocks(local))
+                                                  world, Clocks(local), check=check)
     plain_stats = session.search_stats(reset=True)
     total_ms = max_over_ranks(sum(step_ms), world)
     value = world * Q * args.steps / (total_ms / 1e3)
@@ -736,12 +809,19 @@ def main():
         session.search(sets[i % 2], K, out=out)
     if world > 1:
         dist.barrier()
+    e2e_checked = e2e_bad = 0
     for i in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         session.search(sets[i % 2], K, out=out)
         host_ms.append((time.perf_counter() - t0) * 1e3)
+        if want is not None:  # outside the timer: every e2e result against the oracle
+            e2e_checked += 1
+            e2e_bad += 0 if same_bits(out, want[i % 2]) else 1
+    if parity is not None:
+        parity['timed'] = dict(check.report(), e2e_checked=e2e_checked, e2e_mismatched=e2e_bad)
+        parity['bit_exact'] = bool(parity['bit_exact'] and check.mismatched == 0 and e2e_bad == 0)
     e2e_total = sum(host_ms)
     if world > 1:
         tt = torch.tensor([e2e_total], device='cuda', dtype=torch.float64)
