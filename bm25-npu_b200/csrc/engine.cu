@@ -1155,6 +1155,11 @@ class Engine {
             const long long wt_claims = (long long)q * ((plan_.tiles + kWtClaimTiles - 1) / kWtClaimTiles);
             const int wt_grid = (int)std::max<long long>(
                 1, std::min<long long>(plan_.grid, (wt_claims + bm25k::kWtWarps - 1) / bm25k::kWtWarps));
+            {
+                // single-tile claims for the last tiles: about two per warp of the launch
+                const long long tail = (2LL * wt_grid * bm25k::kWtWarps + q - 1) / q;
+                sa.wt_bulk = (int)std::max<long long>(0, (plan_.tiles - tail) / kWtClaimTiles);
+            }
             auto tile_group = [&](const bm25k::StreamArgs &args) {
                 const bool lean = !args.retry && !args.kq && k <= bm25k::kMaxSmallK;
                 if (warp_tile) {

@@ -161,6 +161,9 @@ struct StreamArgs {
     const float *dense;
     const int *dense_row;
     long long dense_stride;
+    // warp-tile kernel: claims of kC tiles cover tile blocks [0, wt_bulk); the tiles after them
+    // are claimed one at a time, so the last claims of the launch are short
+    int wt_bulk;
     // cycles a bounded wait spends before it gives up (0: kWaitBudget)
     long long wait_budget;
     // test hook: a nonzero word makes the tile-group kernel's producer issue no ring stage, so its

@@ -7,7 +7,9 @@
 //   * a claim is one query and kC consecutive 1024-document tiles; warps take
 //     claims from one global counter (the atomic for the next claim is in
 //     flight while the current one runs), in tile-major order, so every query
-//     gets tiles early and its running bound rises at once;
+//     gets tiles early and its running bound rises at once; the last tiles
+//     (about two claims per warp) are claimed one at a time, so the launch does
+//     not end waiting on a few warps with long claims of a dense query;
 //   * the warp resolves the claim itself: lane s holds query word s's posting
 //     position at each of the claim's kC + 1 tile bounds, read from the word's
 //     directory row (long lists, built at create) or from its plan row (short
@@ -87,14 +89,14 @@ __device__ __forceinline__ void PrefetchL2(const void *p, unsigned bytes)
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-// Posting positions of query word w at the bounds of tiles t0 .. t0 + kC (clamped at the last
-// bound): off[j] = first posting of the word's list in tile t0 + j.  Words outside the vocabulary
+// Posting positions of query word w at the bounds of the claim's tiles t0 .. t0 + nt (j > nt
+// repeats the last bound): off[j] = first posting of the word's list in tile t0 + j.  Words outside the vocabulary
 // have no postings (a negative one is flagged).
 // seed: raised to the word's k-th largest posting score (k <= 32 and term statistics present).
 // drow: the term's dense row, or -1.
 template <int kC>
-__device__ __forceinline__ void WtWordOffsets(const StreamArgs &a, long long w, int t0, int *off, unsigned &bad,
-                                              int k, float &seed, int &drow)
+__device__ __forceinline__ void WtWordOffsets(const StreamArgs &a, long long w, int t0, int nt, int *off,
+                                              unsigned &bad, int k, float &seed, int &drow)
 {
     const int term = __ldg(a.words + w);
     drow = -1;
@@ -116,12 +118,12 @@ __device__ __forceinline__ void WtWordOffsets(const StreamArgs &a, long long w, 
         const int *row = a.dir + (long long)r * a.dir_stride;
 #pragma unroll
         for (int j = 0; j <= kC; ++j)
-            off[j] = base + __ldg(row + min(t0 + j, a.tiles));
+            off[j] = base + __ldg(row + t0 + min(j, nt));
     } else {
         const int *row = a.plan_rows + w * a.dir_stride;  // written by the kernel before this one
 #pragma unroll
         for (int j = 0; j <= kC; ++j)
-            off[j] = base + __ldcg(row + min(t0 + j, a.tiles));
+            off[j] = base + __ldcg(row + t0 + min(j, nt));
     }
 }
 
@@ -171,7 +173,9 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
     AllowDependents();    // the final select may be placed as this kernel's CTAs retire
     WaitPrerequisites();  // plan rows (and a retry pass's fail list) of the kernels before this one
     const unsigned nq = !kLean && a.retry ? __ldcg(a.fail_in_count) : (unsigned)a.q;
-    const unsigned claims = nq * (unsigned)((a.tiles + kC - 1) / kC);
+    const unsigned bulk = (unsigned)min(a.wt_bulk, a.tiles / kC);
+    const unsigned claims_bulk = nq * bulk;
+    const unsigned claims = claims_bulk + nq * (unsigned)(a.tiles - (int)bulk * kC);
     unsigned bad = 0;
     unsigned n_claims = 0, n_tiles = 0, n_post = 0;  // per warp
 
@@ -186,10 +190,12 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
             nxt = atomicAdd(&a.ctrl->next, 1u);  // the next claim, in flight meanwhile
 
         // ---- the claim: query, tiles, and each word's posting positions at the tile bounds ----
-        const unsigned qi = c % nq;
+        const bool single = c >= claims_bulk;
+        const unsigned cc = single ? c - claims_bulk : c;
+        const unsigned qi = cc % nq;
         const int q = !kLean && a.retry ? __ldcg(a.fail_in + qi) : (int)qi;
-        const int t0 = (int)(c / nq) * kC;
-        const int nt = min(kC, a.tiles - t0);
+        const int t0 = single ? (int)(bulk * kC + cc / nq) : (int)(cc / nq) * kC;
+        const int nt = single ? 1 : kC;
         const long long qb = __ldg(a.qoffsets + q), qe = __ldg(a.qoffsets + q + 1);
         int nw = (int)(qe - qb);
         if (qe - qb < 0 || qe - qb > kMaxTerms || qb < 0 || qe > a.word_cap) {
@@ -204,9 +210,9 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
         float seed = 0.0f;
         int drowA = -1, drowB = -1;
         if (lane < nw)
-            WtWordOffsets<kC>(a, qb + lane, t0, offA, bad, k, seed, drowA);
+            WtWordOffsets<kC>(a, qb + lane, t0, nt, offA, bad, k, seed, drowA);
         if (lane + 32 < nw)
-            WtWordOffsets<kC>(a, qb + lane + 32, t0, offB, bad, k, seed, drowB);
+            WtWordOffsets<kC>(a, qb + lane + 32, t0, nt, offB, bad, k, seed, drowB);
         if (a.prefetch) {
             PrefetchRun(a, offA[0], offA[kC], drowA, t0, nt);
             PrefetchRun(a, offB[0], offB[kC], drowB, t0, nt);
