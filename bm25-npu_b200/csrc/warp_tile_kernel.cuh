@@ -17,13 +17,17 @@
 //     postings of all kC tiles (cp.async.bulk.prefetch.L2: no shared memory, no
 //     registers held while the bytes are in flight);
 //   * per tile the warp loads its postings straight from global memory into
-//     registers, up to kWtSlots windows of 128 postings at once across the
-//     query's words (lane l takes postings l, l + 32, l + 64, l + 96 of a
-//     window, so consecutive lanes add consecutive documents of a dense list
-//     into distinct shared-memory banks), and adds them into its private 4 KB
-//     FP32 row in query-word order (a __syncwarp between words orders the
-//     lanes: each document's sum is ((0 + s_1) + s_2) + ... as in
-//     cpu_index_search.h:176-188);
+//     registers -- the first window (128 postings) of each of the query's first
+//     kWtLead words at once, so a typical tile waits for memory once, the rest
+//     of a long word two windows at a time (lane l takes postings l, l + 32,
+//     l + 64, l + 96 of a window, so consecutive lanes add consecutive
+//     documents of a dense list into distinct shared-memory banks) -- and adds
+//     them into its private 4 KB FP32 row in query-word order (a __syncwarp
+//     between words orders the lanes: each document's sum is
+//     ((0 + s_1) + s_2) + ... as in cpu_index_search.h:176-188).  A word kept as
+//     a dense row (df >= dense_density * N) is added from that row instead:
+//     1024 scores with 128-bit loads, zero where the word is absent (adding +0
+//     leaves a sum unchanged);
 //   * then it selects the tile's top-K at or above the query's running bound
 //     (TileSelectAppend, shared with the tile-group kernel) and clears the row.
 //     The lanes keep the largest sum they wrote, which is the tile's largest
@@ -50,12 +54,19 @@ constexpr int kWtTile = 1024;        // documents per tile (one warp's row)
 constexpr int kWtWarps = 8;
 constexpr int kWtThreads = kWtWarps * 32;
 constexpr int kWtWindow = 128;       // postings per window (4 per lane)
-constexpr int kWtSlots = 4;          // windows loaded before their adds
+constexpr int kWtLead = 4;           // words whose first window is loaded before any add
 constexpr int kPlanRowChunk = 2048;  // plan row entries per PlanRowsKernel CTA (grid.y)
 constexpr int kTermTopK = 32;        // largest posting scores kept per term
 
+constexpr int kWtMaxC = 8;           // largest kC: claim bounds kept per word
+
 struct WtShared {
     WarpSel wsel[kWtWarps];
+    // words 32..63 of a claim's query (rare: at most 64 words per query): their posting positions at
+    // the claim's tile bounds and their dense rows, per warp; words 0..31 are held in registers
+    int offB[kWtWarps][32][kWtMaxC + 1];
+    int drowB[kWtWarps][32];
+    unsigned counters[kWtWarps][3];  // claims, tiles, postings of the warp
 };
 
 inline size_t WarpTileSmem() { return (size_t)kWtWarps * kWtTile * sizeof(float) + sizeof(WtShared); }
@@ -144,22 +155,82 @@ __device__ __forceinline__ void PrefetchRun(const StreamArgs &a, int lo, int hi,
     PrefetchL2(a.data + p0, bytes);
 }
 
-// Inclusive prefix sum over the warp.
-__device__ __forceinline__ int WarpInclusiveSum(int v, int lane)
+// Adds one window set of a word: lane l's postings l, l + 32, l + 64, l + 96 of the window (ids -1:
+// none) into the warp's row.  A word's postings are distinct documents, so the lanes never collide.
+__device__ __forceinline__ void WtScatter(const int (&id)[4], const float (&val)[4], int base_doc, float *row,
+                                          float &rmax, unsigned &bad)
 {
+    int d[4];
+    float r[4];
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int x = __shfl_up_sync(kFull, v, o);
-        if (lane >= o)
-            v += x;
+    for (int v = 0; v < 4; ++v) {
+        d[v] = id[v] - base_doc;
+        if (id[v] >= 0 && (unsigned)d[v] >= (unsigned)kWtTile)
+            bad |= kStatusBadPosting;
     }
-    return v;
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+        if ((unsigned)d[v] < (unsigned)kWtTile)
+            r[v] = row[d[v]];
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+        if ((unsigned)d[v] < (unsigned)kWtTile) {
+            const float x = r[v] + val[v];
+            row[d[v]] = x;
+            rmax = fmaxf(rmax, x);
+        }
+}
+
+// Postings [b, e) of one word in the tile, two windows (256 postings) per round.
+__device__ __forceinline__ void WtWordWindows(const StreamArgs &a, int b, int e, int base_doc, float *row, int lane,
+                                              float &rmax, unsigned &bad)
+{
+    for (int p0 = b; p0 < e; p0 += 2 * kWtWindow) {  // uniform
+        int id[2][4];
+        float val[2][4];
+#pragma unroll
+        for (int w = 0; w < 2; ++w)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int p = p0 + w * kWtWindow + lane + 32 * v;
+                id[w][v] = -1;
+                val[w][v] = 0.0f;
+                if (p < e) {
+                    id[w][v] = LdStreamI32(a.indices + p);
+                    val[w][v] = LdStreamF32(a.data + p);
+                }
+            }
+        WtScatter(id[0], val[0], base_doc, row, rmax, bad);
+        WtScatter(id[1], val[1], base_doc, row, rmax, bad);
+    }
+}
+
+// A word kept as a dense row: the tile's 1024 scores, 8 x 128 bits per lane, added in place.
+__device__ __forceinline__ void WtDenseAdd(const StreamArgs &a, int drow, int base_doc, float4 *row4, int lane,
+                                           float &rmax)
+{
+    const float4 *src = reinterpret_cast<const float4 *>(a.dense + (long long)drow * a.dense_stride + base_doc);
+    float4 v[kWtTile / 128];
+#pragma unroll
+    for (int z = 0; z < kWtTile / 128; ++z)
+        v[z] = LdStreamF32x4(src + lane + 32 * z);
+#pragma unroll
+    for (int z = 0; z < kWtTile / 128; ++z) {
+        float4 r = row4[lane + 32 * z];
+        r.x += v[z].x;
+        r.y += v[z].y;
+        r.z += v[z].z;
+        r.w += v[z].w;
+        row4[lane + 32 * z] = r;
+        rmax = fmaxf(rmax, fmaxf(fmaxf(r.x, r.y), fmaxf(r.z, r.w)));
+    }
 }
 
 // kC: tiles per claim.  kLean: the plain first pass with one K <= 32 for every query.
 template <int kC, bool kLean>
 __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs a)
 {
+    static_assert(kC <= kWtMaxC, "claim bounds of words 32..63 are kept for kWtMaxC tiles");
     extern __shared__ __align__(128) unsigned char wt_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float *row = reinterpret_cast<float *>(wt_smem) + (size_t)warp * kWtTile;
@@ -177,7 +248,8 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
     const unsigned claims_bulk = nq * bulk;
     const unsigned claims = claims_bulk + nq * (unsigned)(a.tiles - (int)bulk * kC);
     unsigned bad = 0;
-    unsigned n_claims = 0, n_tiles = 0, n_post = 0;  // per warp
+    if (lane == 0)
+        sh.counters[warp][0] = sh.counters[warp][1] = sh.counters[warp][2] = 0u;
 
     unsigned nxt = 0;
     if (lane == 0)
@@ -203,26 +275,48 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
             nw = 0;
         }
         const int k = kLean ? a.k : QueryK(a, q);
-        int offA[kC + 1], offB[kC + 1];  // words lane and lane + 32
+        int offA[kC + 1];  // word `lane`'s posting positions at the claim's tile bounds
 #pragma unroll
         for (int j = 0; j <= kC; ++j)
-            offA[j] = offB[j] = 0;
+            offA[j] = 0;
         float seed = 0.0f;
-        int drowA = -1, drowB = -1;
+        int drowA = -1;
         if (lane < nw)
             WtWordOffsets<kC>(a, qb + lane, t0, nt, offA, bad, k, seed, drowA);
-        if (lane + 32 < nw)
-            WtWordOffsets<kC>(a, qb + lane + 32, t0, nt, offB, bad, k, seed, drowB);
-        if (a.prefetch) {
+        if (a.prefetch)
             PrefetchRun(a, offA[0], offA[kC], drowA, t0, nt);
-            PrefetchRun(a, offB[0], offB[kC], drowB, t0, nt);
+        const unsigned denseA = __ballot_sync(kFull, drowA >= 0);
+        unsigned denseB = 0;
+        if (nw > 32) {  // uniform: words 32..63 go to shared memory
+            int offB[kC + 1];
+#pragma unroll
+            for (int j = 0; j <= kC; ++j)
+                offB[j] = 0;
+            int drowB = -1;
+            if (lane + 32 < nw)
+                WtWordOffsets<kC>(a, qb + lane + 32, t0, nt, offB, bad, k, seed, drowB);
+            if (a.prefetch)
+                PrefetchRun(a, offB[0], offB[kC], drowB, t0, nt);
+#pragma unroll
+            for (int j = 0; j <= kC; ++j)
+                sh.offB[warp][lane][j] = offB[j];
+            sh.drowB[warp][lane] = drowB;
+            denseB = __ballot_sync(kFull, drowB >= 0);
+            __syncwarp();
         }
-        const unsigned denseA = __ballot_sync(kFull, drowA >= 0), denseB = __ballot_sync(kFull, drowB >= 0);
         // the largest K-th posting score of the query's words (0 for K > 32)
         seed = __uint_as_float(__reduce_max_sync(kFull, __float_as_uint(seed)));  // non-negative: bit order
-        ++n_claims;
-        n_tiles += (unsigned)nt;
-        n_post += (unsigned)(offA[kC] - offA[0]) + (unsigned)(offB[kC] - offB[0]);
+        {
+            unsigned posts = (unsigned)(offA[kC] - offA[0]);
+            if (nw > 32)
+                posts += (unsigned)(sh.offB[warp][lane][kC] - sh.offB[warp][lane][0]);
+            posts = __reduce_add_sync(kFull, posts);
+            if (lane == 0) {
+                sh.counters[warp][0] += 1u;
+                sh.counters[warp][1] += (unsigned)nt;
+                sh.counters[warp][2] += posts;
+            }
+        }
 
         // ---- the claim's tiles ----
         for (int j = 0; j < nt; ++j) {
@@ -232,124 +326,67 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
             const unsigned thr_bits = lane == 0 ? __ldcg(a.threshold + q) : 0u;
             const unsigned slot_bits = lane < k ? __ldcg(a.tslots + (long long)q * 32 + lane) : 0xffffffffu;
             float rmax = 0.0f;  // the largest sum this lane wrote
-            // windows of 128 postings of every word in this tile, numbered in word order
-            const int bA = offA[0], eA = offA[1], bB = offB[0], eB = offB[1];
-            // a dense word with postings in the tile is one window, added from its dense row
-            const int nA = drowA >= 0 ? (eA > bA ? 1 : 0) : (eA - bA + kWtWindow - 1) / kWtWindow;
-            const int nB = drowB >= 0 ? (eB > bB ? 1 : 0) : (eB - bB + kWtWindow - 1) / kWtWindow;
-            const int cumA = WarpInclusiveSum(nA, lane);
-            const int WA = __shfl_sync(kFull, cumA, 31);
-            int cumB = 0, W = WA;
-            if (nw > 32) {  // uniform
-                cumB = WarpInclusiveSum(nB, lane) + WA;
-                W = __shfl_sync(kFull, cumB, 31);
-            }
-            int prev_word = -1;
-            // word of window i (uniform): lane index among the first 32 words, or 32 + among the rest
-            auto word_of = [&](int i) {
-                return i < WA ? __popc(__ballot_sync(kFull, cumA <= i))
-                              : 32 + __popc(__ballot_sync(kFull, cumB <= i));
-            };
-            auto is_dense = [&](int s) { return s < 32 ? ((denseA >> s) & 1u) != 0 : ((denseB >> (s - 32)) & 1u) != 0; };
-            for (int i0 = 0; i0 < W;) {
-                const int s0 = word_of(i0);
-                if (is_dense(s0)) {
-                    // dense word: the tile's 1024 scores, 8 x 128 bits per lane, added in place
-                    const int drow = s0 < 32 ? __shfl_sync(kFull, drowA, s0) : __shfl_sync(kFull, drowB, s0 - 32);
-                    const float4 *src = reinterpret_cast<const float4 *>(a.dense + (long long)drow * a.dense_stride +
-                                                                         base_doc);
-                    float4 v[kWtTile / 128];
+            // First window (128 postings) of each of the first kWtLead sparse words: loaded at once,
+            // so a typical tile waits for memory once.
+            int lid[kWtLead][4];
+            float lval[kWtLead][4];
 #pragma unroll
-                    for (int z = 0; z < kWtTile / 128; ++z)
-                        v[z] = LdStreamF32x4(src + lane + 32 * z);
+            for (int s = 0; s < kWtLead; ++s) {
+                const int b = __shfl_sync(kFull, offA[0], s), e = __shfl_sync(kFull, offA[1], s);
+                const bool sparse = s < nw && !((denseA >> s) & 1u);  // uniform
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int p = b + lane + 32 * v;
+                    lid[s][v] = -1;
+                    lval[s][v] = 0.0f;
+                    if (sparse && p < e) {
+                        lid[s][v] = LdStreamI32(a.indices + p);
+                        lval[s][v] = LdStreamF32(a.data + p);
+                    }
+                }
+            }
+            // the words in query order
+#pragma unroll
+            for (int s = 0; s < kWtLead; ++s) {
+                if (s >= nw)
+                    break;  // uniform
+                if (s > 0)
                     __syncwarp();  // the previous word's adds are in the row before this word's
-                    prev_word = s0;
-#pragma unroll
-                    for (int z = 0; z < kWtTile / 128; ++z) {
-                        float4 r = row4[lane + 32 * z];
-                        r.x += v[z].x;
-                        r.y += v[z].y;
-                        r.z += v[z].z;
-                        r.w += v[z].w;
-                        row4[lane + 32 * z] = r;
-                        rmax = fmaxf(rmax, fmaxf(fmaxf(r.x, r.y), fmaxf(r.z, r.w)));
-                    }
-                    ++i0;
-                    continue;
+                const int b = __shfl_sync(kFull, offA[0], s), e = __shfl_sync(kFull, offA[1], s);
+                if ((denseA >> s) & 1u) {
+                    if (e > b)
+                        WtDenseAdd(a, __shfl_sync(kFull, drowA, s), base_doc, row4, lane, rmax);
+                } else {
+                    WtScatter(lid[s], lval[s], base_doc, row, rmax, bad);
+                    WtWordWindows(a, b + kWtWindow, e, base_doc, row, lane, rmax, bad);
                 }
-                // up to kWtSlots windows of postings, ending before the next dense word
-                int ids[kWtSlots][4];
-                float vals[kWtSlots][4];
-                int word[kWtSlots];
-                bool more = true;
-                int taken = 0;
-#pragma unroll
-                for (int u = 0; u < kWtSlots; ++u) {
-                    const int i = i0 + u;
-                    int p0 = 0, p1 = 0;
-                    word[u] = -1;
-                    if (more && i < W) {  // uniform
-                        const int s = u == 0 ? s0 : word_of(i);
-                        if (is_dense(s)) {
-                            more = false;
-                        } else {
-                            int first, b, e;
-                            if (s < 32) {
-                                first = __shfl_sync(kFull, cumA - nA, s);
-                                b = __shfl_sync(kFull, bA, s);
-                                e = __shfl_sync(kFull, eA, s);
-                            } else {
-                                first = __shfl_sync(kFull, cumB - nB, s - 32);
-                                b = __shfl_sync(kFull, bB, s - 32);
-                                e = __shfl_sync(kFull, eB, s - 32);
-                            }
-                            word[u] = s;
-                            p0 = b + (i - first) * kWtWindow;
-                            p1 = min(p0 + kWtWindow, e);
-                            taken = u + 1;
-                        }
-                    }
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) {
-                        const int p = p0 + lane + 32 * v;
-                        ids[u][v] = -1;
-                        vals[u][v] = 0.0f;
-                        if (p < p1) {
-                            ids[u][v] = LdStreamI32(a.indices + p);
-                            vals[u][v] = LdStreamF32(a.data + p);
-                        }
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < kWtSlots; ++u) {
-                    if (word[u] < 0)
-                        break;  // uniform: no more windows in this batch
-                    if (word[u] != prev_word) {
-                        __syncwarp();  // the previous word's adds are in the row before this word's
-                        prev_word = word[u];
-                    }
-                    int d[4];
-                    float r[4];
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) {
-                        d[v] = ids[u][v] - base_doc;
-                        if (ids[u][v] >= 0 && (unsigned)d[v] >= (unsigned)kWtTile)
-                            bad |= kStatusBadPosting;
-                    }
-#pragma unroll
-                    for (int v = 0; v < 4; ++v)
-                        if ((unsigned)d[v] < (unsigned)kWtTile)
-                            r[v] = row[d[v]];
-#pragma unroll
-                    for (int v = 0; v < 4; ++v)
-                        if ((unsigned)d[v] < (unsigned)kWtTile) {
-                            const float x = r[v] + vals[u][v];
-                            row[d[v]] = x;
-                            rmax = fmaxf(rmax, x);
-                        }
-                }
-                i0 += taken;
             }
+            for (int s = kWtLead; s < nw; ++s) {
+                __syncwarp();
+                int b, e, drow;
+                bool dense;
+                if (s < 32) {
+                    b = __shfl_sync(kFull, offA[0], s);
+                    e = __shfl_sync(kFull, offA[1], s);
+                    drow = __shfl_sync(kFull, drowA, s);
+                    dense = (denseA >> s) & 1u;
+                } else {
+                    b = sh.offB[warp][s - 32][j];
+                    e = sh.offB[warp][s - 32][j + 1];
+                    drow = sh.drowB[warp][s - 32];
+                    dense = (denseB >> (s - 32)) & 1u;
+                }
+                if (dense) {
+                    if (e > b)
+                        WtDenseAdd(a, drow, base_doc, row4, lane, rmax);
+                } else {
+                    WtWordWindows(a, b, e, base_doc, row, lane, rmax, bad);
+                }
+            }
+            bool any = lane < nw && offA[1] > offA[0];
+            if (nw > 32)
+                any |= lane + 32 < nw && sh.offB[warp][lane][j + 1] > sh.offB[warp][lane][j];
+            const bool W = __any_sync(kFull, any);
             __syncwarp();
             const float thr = fmaxf(fmaxf(seed, __uint_as_float(__shfl_sync(kFull, thr_bits, 0))),
                                     __uint_as_float(__reduce_min_sync(kFull, slot_bits)));
@@ -363,22 +400,19 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
                 __syncwarp();
             }
 #pragma unroll
-            for (int x = 0; x < kC; ++x) {
+            for (int x = 0; x < kC; ++x)
                 offA[x] = offA[x + 1];
-                offB[x] = offB[x + 1];
-            }
         }
     }
 
     bad = __reduce_or_sync(kFull, bad);
-    n_post = __reduce_add_sync(kFull, n_post);
     if (lane == 0) {
         if (bad)
             atomicOr(a.status, bad);
-        if (a.stats && n_claims) {
-            atomicAdd(a.stats + kStatClaims, (unsigned long long)n_claims);
-            atomicAdd(a.stats + kStatTilesScanned, (unsigned long long)n_tiles);
-            atomicAdd(a.stats + kStatPostingsCopied, (unsigned long long)n_post);
+        if (a.stats && sh.counters[warp][0]) {
+            atomicAdd(a.stats + kStatClaims, (unsigned long long)sh.counters[warp][0]);
+            atomicAdd(a.stats + kStatTilesScanned, (unsigned long long)sh.counters[warp][1]);
+            atomicAdd(a.stats + kStatPostingsCopied, (unsigned long long)sh.counters[warp][2]);
         }
         // the last warp to run dry resets the work counter for the next pass
         const unsigned d = atomicAdd(&a.ctrl->done, 1u);
