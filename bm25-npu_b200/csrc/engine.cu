@@ -988,7 +988,7 @@ class Engine {
     // byte budget (the index's own size, at most 16 GiB); each row holds tiles * 1024 scores.
     void BuildDense(const std::vector<int64_t> &dfs)
     {
-        const double density = opts_.dense_density > 0.0f ? opts_.dense_density : 0.5;
+        const double density = opts_.dense_density > 0.0f ? opts_.dense_density : 0.25;
         const int64_t min_df = std::max<int64_t>(1, (int64_t)std::ceil(density * (double)docs_));
         dense_stride_ = (int64_t)plan_.tiles * plan_.tile_docs;
         const int64_t budget = std::min<int64_t>(int64_t(16) << 30, std::max<int64_t>(index_bytes_, 1));

@@ -65,8 +65,8 @@ typedef struct bm25_options {
     float dense_density;     /* warp-tile kernel: a term whose postings cover at least this share of the
                                 documents is also kept as a dense FP32 row of per-document scores (zero
                                 where absent), read with 128-bit loads instead of scattered
-                                (0 = 0.5, where the row is no more bytes than the postings; negative =
-                                none) */
+                                (0 = 0.25: such a row is at most twice the bytes of the postings it
+                                replaces and a quarter of the instructions; negative = none) */
 } bm25_options;
 
 /* Search kernels (bm25_options.kernel):

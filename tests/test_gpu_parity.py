@@ -219,7 +219,7 @@ def test_kernel_timing_hook(pkg, corpus, cuda_ok, kernel):
 def test_warp_tile_dense_rows(pkg, oracle_mod, corpus, cuda_ok, density):
     """The warp-tile kernel adds the terms kept as dense rows (df >= density * N) from those rows and
     the others from their postings, in query-word order: same bits as the oracle with no dense rows
-    (-1), the default (0: half the documents), nearly every term dense (0.02), and only terms in every
+    (-1), the default (0: a quarter of the documents), nearly every term dense (0.02), and only terms in every
     document (1.0).  Queries mix dense and sparse words in every order, repeats and unknown words."""
     spec, index, data = corpus
     df = np.diff(index.offsets)
@@ -236,7 +236,7 @@ def test_warp_tile_dense_rows(pkg, oracle_mod, corpus, cuda_ok, density):
         if density < 0:
             assert info['dense_rows'] == 0
         else:
-            d = 0.5 if density == 0 else density
+            d = 0.25 if density == 0 else density
             fit = min(16 << 30, info['index_bytes']) // (info['tiles'] * 1024 * 4)  # the rows' byte budget
             assert info['dense_rows'] == min(fit, int(np.sum(df >= np.ceil(d * index.num_docs))))
         for k in (1, 10, 32):
