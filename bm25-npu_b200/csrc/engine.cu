@@ -968,9 +968,10 @@ class Engine {
             cand_count_ = static_cast<unsigned *>(Alloc(qc * sizeof(unsigned), "cudaMalloc cand count"));
             cand_scores_ = static_cast<float *>(Alloc(qc * cand_cap_ * sizeof(float), "cudaMalloc candidates"));
             cand_ids_ = static_cast<int *>(Alloc(qc * cand_cap_ * sizeof(int), "cudaMalloc candidates"));
-            if (plan_.kernel != BM25_KERNEL_WARP_TILE || opts_.prune)
-                plan_entries_ = static_cast<bm25k::PlanEntry *>(Alloc(
-                    std::max<size_t>(1, opts_.word_capacity) * tiles_z * sizeof(bm25k::PlanEntry), "cudaMalloc plan"));
+            // the (query word, tile) plan of every kernel but the warp-tile one, which uses it for the
+            // Searches it hands to the tile-group kernel
+            plan_entries_ = static_cast<bm25k::PlanEntry *>(Alloc(
+                std::max<size_t>(1, opts_.word_capacity) * tiles_z * sizeof(bm25k::PlanEntry), "cudaMalloc plan"));
             if (plan_.kernel == BM25_KERNEL_WARP_TILE)
                 plan_rows_ = static_cast<int *>(Alloc(std::max<size_t>(1, opts_.word_capacity) * (tiles_z + 1) *
                                                           sizeof(int),
@@ -1129,9 +1130,12 @@ class Engine {
                 sa.item_count = d_item_count_;
                 sa.item_cap = item_cap_;
             }
-            // plain Searches of a warp-tile session: plan rows of the words without a directory row,
-            // then the warp-tile kernel; every other Search: the (query word, tile) plan
-            const bool warp_tile = plan_.kernel == BM25_KERNEL_WARP_TILE && !tau;
+            // plain Searches of one K <= 32 in a warp-tile session: plan rows of the words without a
+            // directory row, then the warp-tile kernel.  Every other Search -- pruned, a K per query or
+            // K > 32 (no starting bound from the term statistics: the warp-tile kernel's wider first
+            // wave of claims would append far more candidates) -- takes the (query word, tile) plan and
+            // the tile-group kernel.
+            const bool warp_tile = plan_.kernel == BM25_KERNEL_WARP_TILE && !tau && !kq && k <= bm25k::kMaxSmallK;
             sa.plan_rows = plan_rows_;
             sa.prefetch = 1;
             sa.wait_budget = opts_.wait_budget_cycles;

@@ -76,8 +76,9 @@ typedef struct bm25_options {
  *                          8-tile group fed by one bulk copy per query word
  *   BM25_KERNEL_WARP_TILE  persistent kernel, 1024-document tiles, every warp takes its own claims
  *                          (a query and 4 consecutive tiles) and loads its postings itself, the
- *                          claim's posting runs prefetched into L2 (the default); pruned Searches
- *                          stream their routed and retried queries with the tile-group kernel */
+ *                          claim's posting runs prefetched into L2 (the default) -- for plain
+ *                          Searches with one K <= 32; pruned Searches, batches with a K per query
+ *                          and K > 32 run the tile-group kernel */
 #define BM25_KERNEL_STREAM 0
 #define BM25_KERNEL_PER_TILE 1
 #define BM25_KERNEL_TILE_GROUP 4
