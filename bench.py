@@ -644,11 +644,12 @@ def blockmax_leg(pkg, args, local, world, flush, stream, rank):
     return out
 
 
-SERVE_RATES = (5000, 10000, 20000, 50000)
+SERVE_RATES = (5000, 10000, 20000, 50000)  # --serve-all
+SERVE_RATES_DEFAULT = (5000, 20000)
 SERVE_TERMS, SERVE_KS, SERVE_POOL = (1, 16), (10, 100, 1000), 4096
 
 
-def serve_leg(pkg, args, spec, index, local):
+def serve_leg(pkg, args, spec, index, local, rates=SERVE_RATES):
     """The serving loop on the 10M-doc index: open-loop Poisson arrivals at 5k-50k queries/s of
     1-16 terms (drawn by df) and K from {10, 100, 1000}; the continuous-batching server (learned
     pruning on, every result exact) against the plain engine serving one query per Search."""
@@ -675,15 +676,19 @@ def serve_leg(pkg, args, spec, index, local):
     configs = (('plain, one query per Search', dict(max_batch=1, learned=False)),
                ('continuous batching, plain', dict(max_batch=256, learned=False, candidate_budget=64_000)),
                ('continuous batching, learned pruning', dict(max_batch=256, learned=True, candidate_budget=64_000)))
-    for rate in SERVE_RATES:
+    for rate in rates:
         total = int(min(rate * args.serve_seconds, 40_000))
         for label, opts in configs:
             if opts['max_batch'] == 1 and rate > 10_000:
                 continue  # saturated far below these rates: its queue only grows
+            made = session.info()['graph_instantiations']
             lat, st = pkg.serving.serve_poisson(session, qo, w, ks, rate_qps=rate, total=total, seed=rate, **opts)
+            made = session.info()['graph_instantiations'] - made
             row = {'config': label, 'offered_qps': rate, 'queries': total, 'achieved_qps': st['achieved_qps'],
                    'p50_ms': st['p50_us'] / 1e3, 'p95_ms': st['p95_us'] / 1e3, 'p99_ms': st['p99_us'] / 1e3,
-                   'mean_batch': st['mean_batch']}
+                   'mean_batch': st['mean_batch'],
+                   # graphs instantiated during the run, server creation (which prepares them all) included
+                   'graphs_instantiated': made}
             out['runs'].append(row)
             log(f'serve {row}')
     session.close()
@@ -736,7 +741,8 @@ def main():
     ap.add_argument('--mix-train-queries', type=int, default=120_000)
     ap.add_argument('--no-blockmax', action='store_true', help='skip the 4.2M-doc block-max workload')
     ap.add_argument('--blockmax-train-queries', type=int, default=200_000)
-    ap.add_argument('--serve', action='store_true', help='also run the serving loop (Poisson arrivals)')
+    ap.add_argument('--no-serve', action='store_true', help='skip the serving loop (Poisson arrivals)')
+    ap.add_argument('--serve-all', action='store_true', help='serving loop at 5k, 10k, 20k and 50k queries/s')
     ap.add_argument('--serve-seconds', type=float, default=1.0)
     args = ap.parse_args()
     if args.impl == 'reference':
@@ -855,8 +861,8 @@ def main():
         learned['plain_per_search'] = {key: v / args.steps for key, v in plain_stats.items()}
 
     serving = None
-    if info['kernel'] in (4, 5) and args.serve and world == 1:
-        serving = serve_leg(pkg, args, spec, index, local)
+    if info['kernel'] in (4, 5) and not args.no_serve and world == 1 and not (args.docs or args.vocab):
+        serving = serve_leg(pkg, args, spec, index, local, SERVE_RATES if args.serve_all else SERVE_RATES_DEFAULT)
 
     mix = blockmax = None
     full_size = info['kernel'] in (4, 5) and not (args.docs or args.vocab)

@@ -98,6 +98,7 @@ SIGNATURES = {
     'bm25_get_info': (c_int, [c_void_p, POINTER(Info)]),
     'bm25_kernel_timing': (c_int, [c_void_p, c_int32]),
     'bm25_test_inject': (c_int, [c_void_p, c_int32]),
+    'bm25_prepare_batch_graphs': (c_int, [c_void_p, c_int32, c_int32]),
     'bm25_kernel_times': (c_int, [c_void_p, POINTER(c_float), c_int64, POINTER(c_int64)]),
     'bm25_search_pruned_device': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p,
                                           c_void_p, c_void_p, c_void_p]),

@@ -402,31 +402,44 @@ class Engine {
         Check(ks && out_scores && out_ids && (!learned || out_exact), "Null buffer");
         Check(q >= 1 && q <= opts_.query_capacity, "Query batch exceeds declared capacity or is empty");
         int kmax = 1;
-        std::vector<int64_t> kout(q);
-        int64_t total = 0;
         for (int64_t i = 0; i < q; ++i) {
             Check(ks[i] >= 1 && ks[i] <= opts_.max_k && ks[i] <= docs_, "K outside [1, min(max_k, N)]");
-            kout[i] = total;
-            total += ks[i];
             kmax = std::max(kmax, ks[i]);
         }
-        Pack(qoffsets, words, q, kmax);
+        Check(qoffsets != nullptr, "Null query offsets");
+        // The batch runs in the graph of its capacity bucket (queries rounded up to a power of two,
+        // the largest K up to 32, 128 or 1024): the extra queries are empty with K = 1 and their
+        // results come after the real ones, so a few graphs serve every batch a server forms.
+        const int qb = BatchBucket((int)q), kb = KBucket(kmax);
+        std::vector<int64_t> offsets(qoffsets, qoffsets + q + 1);
+        offsets.resize((size_t)qb + 1, qoffsets[q]);
+        std::vector<int32_t> kpad(ks, ks + q);
+        kpad.resize((size_t)qb, 1);
+        std::vector<int64_t> kout(qb);
+        int64_t total = 0;
+        for (int i = 0; i < qb; ++i) {
+            kout[i] = total;
+            total += kpad[i];
+        }
+        total = kout[q - 1] + ks[q - 1];  // the real queries' results
+        Pack(offsets.data(), words, qb, kb);
         unsigned char *in = static_cast<unsigned char *>(h_in_);
-        std::memcpy(in + ks_offset_, ks, q * sizeof(int32_t));
-        std::memcpy(in + kout_offset_, kout.data(), q * sizeof(int64_t));
+        std::memcpy(in + ks_offset_, kpad.data(), (size_t)qb * sizeof(int32_t));
+        std::memcpy(in + kout_offset_, kout.data(), (size_t)qb * sizeof(int64_t));
+        kmax = kb;
         try {
             Cuda(cudaSetDevice(device_), "cudaSetDevice");
-            cudaGraphExec_t exec = GraphFor((int)q, kmax, (learned ? kModeLearned : kModePlain) | kModeMixed);
+            cudaGraphExec_t exec = GraphFor(qb, kmax, (learned ? kModeLearned : kModePlain) | kModeMixed);
             Cuda(cudaStreamWaitEvent(stream_, done_, 0), "cudaStreamWaitEvent");
             ++searches_;
             Cuda(cudaGraphLaunch(exec, stream_), "cudaGraphLaunch");
             ++replays_;
             unsigned char *ho = static_cast<unsigned char *>(h_out_);
             Cuda(cudaMemcpyAsync(ho, d_out_, total * sizeof(float), cudaMemcpyDeviceToHost, stream_), "D2H");
-            const size_t ids = IdOffset((int)q, kmax);
+            const size_t ids = IdOffset(qb, kmax);
             Cuda(cudaMemcpyAsync(ho + ids, d_out_ + ids, total * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_),
                  "D2H");
-            const size_t st = StatusOffset((int)q, kmax);
+            const size_t st = StatusOffset(qb, kmax);
             Cuda(cudaMemcpyAsync(ho + st, d_out_ + st, 32 + (learned ? (size_t)q * 4 : 0), cudaMemcpyDeviceToHost,
                                  stream_),
                  "D2H");
@@ -448,7 +461,7 @@ class Engine {
             std::memcpy(out_scores, scores, total * sizeof(float));
             std::memcpy(out_ids, idv, total * sizeof(int32_t));
             if (learned) {
-                const int32_t *ex = reinterpret_cast<const int32_t *>(ho + ExactOffset((int)q, kmax));
+                const int32_t *ex = reinterpret_cast<const int32_t *>(ho + ExactOffset(qb, kmax));
                 for (int64_t i = 0; i < q; ++i)
                     out_exact[i] = ex[i] ? 1 : 0;
             }
@@ -489,6 +502,46 @@ class Engine {
         }
     }
 
+    // Capacity buckets of bm25_search_batch's graphs.
+    int BatchBucket(int q) const
+    {
+        int b = 1;
+        while (b < q)
+            b <<= 1;
+        return (int)std::min<int64_t>(b, opts_.query_capacity);
+    }
+    int KBucket(int kmax) const
+    {
+        const int cap = (int)std::min<int64_t>(opts_.max_k, docs_);
+        for (const int b : {32, 128, 1024})
+            if (kmax <= b && b <= cap)
+                return b;
+        return cap;
+    }
+
+    // Instantiates every graph bm25_search_batch (learned or plain) replays for batches of up to
+    // max_batch queries, so that none is instantiated on a serving loop's request path.
+    void PrepareBatchGraphs(int max_batch, bool learned)
+    {
+        RequireUsable();
+        if (learned)
+            RequirePrune();
+        Check(TileFamily(plan_.kernel), "A K per query needs the warp-tile or tile-group kernel");
+        Check(max_batch >= 1 && max_batch <= opts_.query_capacity, "max_batch must be in [1, query_capacity]");
+        Cuda(cudaSetDevice(device_), "cudaSetDevice");
+        std::vector<int> kbs;
+        for (const int k : {1, 33, 129})
+            if (k <= std::min<int64_t>(opts_.max_k, docs_) && (kbs.empty() || KBucket(k) != kbs.back()))
+                kbs.push_back(KBucket(k));
+        const int top = BatchBucket(max_batch);
+        for (int qb = 1;; qb = std::min(qb * 2, top)) {
+            for (const int kb : kbs)
+                (void)GraphFor(qb, kb, (learned ? kModeLearned : kModePlain) | kModeMixed);
+            if (qb == top)
+                break;
+        }
+    }
+
     // Threshold model of the learned bounds (host params, bm25mlp::kParams floats), or none.
     void SetThresholdModel(const float *params, float margin)
     {
@@ -509,7 +562,7 @@ class Engine {
         // graphs hold the model pointer and margin by value: rebuild the learned ones
         for (auto it = graphs_.begin(); it != graphs_.end();) {
             if (std::get<2>(it->first) & kModeLearned) {
-                cudaGraphExecDestroy(it->second);
+                cudaGraphExecDestroy(it->second.exec);
                 it = graphs_.erase(it);
             } else {
                 ++it;
@@ -1314,8 +1367,20 @@ class Engine {
         mode &= ~kModeMixed;
         const bool pruned = mode != kModePlain;
         auto it = graphs_.find(key);
-        if (it != graphs_.end())
-            return it->second;
+        if (it != graphs_.end()) {
+            it->second.last_use = ++graph_uses_;
+            return it->second.exec;
+        }
+        if (graphs_.size() >= kGraphCacheMax) {  // bounded: drop the least recently used graph
+            auto old = graphs_.begin();
+            for (auto g = graphs_.begin(); g != graphs_.end(); ++g)
+                if (g->second.last_use < old->second.last_use)
+                    old = g;
+            Cuda(cudaStreamWaitEvent(stream_, done_, 0), "cudaStreamWaitEvent");
+            Cuda(cudaStreamSynchronize(stream_), "graph eviction");
+            cudaGraphExecDestroy(old->second.exec);
+            graphs_.erase(old);
+        }
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         Cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin graph capture");
@@ -1352,7 +1417,7 @@ class Engine {
         cudaGraphDestroy(graph);
         Cuda(e, "cudaGraphInstantiate");
         ++instantiations_;
-        graphs_[key] = exec;
+        graphs_[key] = CachedGraph{exec, ++graph_uses_};
         return exec;
     }
 
@@ -1401,7 +1466,7 @@ class Engine {
     void Release()
     {
         for (auto &g : graphs_)
-            cudaGraphExecDestroy(g.second);
+            cudaGraphExecDestroy(g.second.exec);
         graphs_.clear();
         for (void *p : allocations_)
             cudaFree(p);
@@ -1467,7 +1532,13 @@ class Engine {
     size_t tg_smem_ = 0;  // tile-group kernel: dynamic shared memory and grid
     int tg_grid_ = 0;
     int sms_ = 148;
-    std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs_;
+    struct CachedGraph {
+        cudaGraphExec_t exec;
+        int64_t last_use;
+    };
+    static constexpr size_t kGraphCacheMax = 64;  // instantiated graphs kept; the least recently used goes
+    std::map<std::tuple<int, int, int>, CachedGraph> graphs_;
+    int64_t graph_uses_ = 0;
     float *d_term_top_ = nullptr, *d_term_mean_ = nullptr, *d_model_ = nullptr, *d_tau_ = nullptr;
     unsigned long long *d_stats_ = nullptr;
     int *d_fail_list_ = nullptr;
@@ -1870,6 +1941,20 @@ void bm25_destroy(bm25_handle *h)
         return;
     bm25_close(h);
     delete h;
+}
+
+int bm25_prepare_batch_graphs(bm25_handle *h, int32_t max_batch, int32_t learned)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            h->engine->PrepareBatchGraphs(max_batch, learned != 0);
+        },
+        h->error, h->code);
 }
 
 int bm25_test_inject(bm25_handle *h, int32_t what)

@@ -240,6 +240,13 @@ int bm25_server_create(bm25_handle *h, const bm25_server_options *options, bm25_
         return Fail(BM25_ERR_INVALID_PARAM, "Learned serving needs a session created with prune = 1");
     if (o.candidate_budget < 0 || o.max_wait_us < 0)
         return Fail(BM25_ERR_INVALID_PARAM, "Negative budget or wait");
+    // every batch the worker can form replays an instantiated graph: none is built on the request path
+    const int prep = bm25_prepare_batch_graphs(h, o.max_batch, o.learned);
+    if (prep != BM25_OK) {
+        char message[512] = {0};
+        bm25_last_error(h, message, sizeof(message), nullptr);
+        return Fail(prep, std::string("Preparing the batch graphs failed: ") + message);
+    }
     auto s = new bm25_server();
     s->handle = h;
     s->opts = o;

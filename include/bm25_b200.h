@@ -167,6 +167,17 @@ int bm25_search_pruned(bm25_handle *handle, const int64_t *qoffsets, const int32
 int bm25_search_batch(bm25_handle *handle, const int64_t *qoffsets, const int32_t *words, const int32_t *ks,
                       int64_t q, float *out_scores, int32_t *out_ids);
 
+/*
+ * A batch runs in the CUDA graph of its capacity bucket: the query count rounded up to
+ * a power of two (at most query_capacity) and the largest K rounded up to 32, 128 or
+ * 1024 (at most max_k); the extra queries are empty.  Graphs are instantiated on first
+ * use and at most 64 are kept (the least recently used is dropped).
+ * bm25_prepare_batch_graphs instantiates every bucket's graph for batches of up to
+ * max_batch queries (learned: the learned variant), so that a serving loop never
+ * instantiates one on its request path; bm25_server_create calls it.
+ */
+int bm25_prepare_batch_graphs(bm25_handle *handle, int32_t max_batch, int32_t learned);
+
 /* bm25_search_batch with the learned bounds; out_exact int32 [q] as bm25_search_pruned. */
 int bm25_search_batch_learned(bm25_handle *handle, const int64_t *qoffsets, const int32_t *words, const int32_t *ks,
                               int64_t q, float *out_scores, int32_t *out_ids, int32_t *out_exact);

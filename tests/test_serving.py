@@ -39,6 +39,8 @@ def test_server_matches_oracle(pkg, oracle_mod, corpus, cuda_ok, learned):
     with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, query_capacity=16,
                                   word_capacity=256, max_k=100, prune=True) as s:
         with pkg.serving.Server(s, max_batch=16, learned=learned, candidate_budget=300) as srv:
+            prepared = s.info()['graph_instantiations']
+            assert prepared >= 5  # batch buckets 1, 2, 4, 8, 16 at least (x K buckets)
             tickets = [None] * len(rows)
 
             def submit(part):
@@ -60,6 +62,8 @@ def test_server_matches_oracle(pkg, oracle_mod, corpus, cuda_ok, learned):
                 assert lat > 0
             st = srv.stats()
             assert st['served'] == len(rows) and 1 <= st['batches'] <= len(rows)
+            # every batch replayed a graph instantiated when the server was created
+            assert s.info()['graph_instantiations'] == prepared
             with pytest.raises(pkg.InvalidParam):
                 srv.wait(tickets[0])  # already waited for
 
@@ -74,3 +78,31 @@ def test_poisson_run_completes(pkg, corpus, cuda_ok):
         lat, st = pkg.serving.serve_poisson(s, qo, w, ks, rate_qps=5000, total=2000, max_batch=64)
         assert lat.shape == (2000,) and np.all(lat > 0)
         assert st['batches'] >= 1 and st['achieved_qps'] > 1000
+
+
+@pytest.mark.gpu
+def test_batch_buckets_pad_exactly(pkg, oracle_mod, corpus, cuda_ok):
+    """Batches of 1..13 queries with K up to 100 run in their bucket's graph (queries padded to a power
+    of two, K to 32 or 128): results equal the oracle, and one graph serves every batch of a bucket."""
+    index, data = corpus
+    rng = np.random.default_rng(21)
+    with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, query_capacity=16,
+                                  word_capacity=256, max_k=100) as s:
+        for q in (1, 2, 3, 5, 8, 13):
+            rows = mixed_queries(index.vocab, rng, q, 0, 6, oov=True)
+            ks = rng.choice([1, 7, 32, 33, 100], q).astype(np.int32)
+            qo = np.zeros(q + 1, np.int64)
+            qo[1:] = np.cumsum([len(r) for r in rows])
+            words = np.array([w for r in rows for w in r], np.int32)
+            gs, gi, koff = s.search_batch((qo, words), ks)
+            for i in range(q):
+                want = oracle_mod.search(index.offsets, index.docs, data, index.num_docs,
+                                         np.array([0, len(rows[i])], np.int64), np.array(rows[i], np.int32),
+                                         int(ks[i]))
+                assert np.array_equal(gi[koff[i]:koff[i + 1]], want[1][0]), (q, i)
+                assert np.array_equal(gs[koff[i]:koff[i + 1]].view(np.uint32), want[0][0].view(np.uint32)), (q, i)
+        made = s.info()['graph_instantiations']
+        for q in (5, 6, 7):  # bucket 8, K bucket 128: the graph made above
+            qo, w = pkg.synthetic_queries(index.offsets, q, 1, 4, q)
+            s.search_batch((qo, w), np.full(q, 100, np.int32))
+        assert s.info()['graph_instantiations'] == made
