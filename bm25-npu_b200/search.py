@@ -299,6 +299,12 @@ class Bm25Session:
                                               c_void_p(scores_ptr), c_void_p(ids_ptr), c_void_p(stream_ptr))
         _raise(self._lib, status, self._handle)
 
+    def prepare_batch_graphs(self, max_batch, learned=False):
+        """Instantiates the graphs search_batch replays for batches of up to max_batch queries
+        (bm25_prepare_batch_graphs); a server does this when it is created."""
+        _raise(self._lib, self._lib.bm25_prepare_batch_graphs(self._handle, int(max_batch), int(bool(learned))),
+               self._handle)
+
     def inject(self, what):
         """Test hook (bm25_test_inject): the next ``search`` fails as a device error, either on the host
         (BM25_INJECT_HOST_FAILURE) or by a stalled ring producer whose consumers' bounded waits run out
