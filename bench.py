@@ -697,6 +697,72 @@ def serve_leg(pkg, args, spec, index, local, rates=SERVE_RATES):
     return out
 
 
+def run_doc_sharded(args):
+    """--shard docs: the 10M-doc index split by document range over the N ranks (one GPU each); every
+    rank searches the same query batches over its range, the local top-K lists are all-gathered with
+    NCCL (Q*K*8 bytes per rank) and merged on every rank by the merge kernel (ShardedSession).  A step
+    is one Search of the batch; value = queries/s of the whole job (strong scaling: the corpus is fixed,
+    each rank holds 1/N of it); steps timed with CUDA events on the launching stream, max over ranks."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    rank, world, local = setup_dist(args.gpus)
+    torch.cuda.set_device(local)
+    dist.init_process_group('nccl', timeout=timedelta(seconds=300), device_id=torch.device('cuda', local))
+    pkg = importlib.import_module('bm25-npu_b200')
+    from oracle import oracle
+    spec, index = build_corpus(pkg, args.docs, args.vocab)
+    data = oracle.contributions(index, spec.k1)  # the eager scores each rank slices its shard from
+    sets = batches(pkg, index, 0)  # the same batches on every rank
+    session = pkg.sharded.ShardedSession(index.offsets, index.docs, data, index.num_docs, query_capacity=Q,
+                                         word_capacity=Q * TERMS, max_k=K)
+    want = [oracle.search(index.offsets, index.docs, data, index.num_docs, *qs, K) for qs in sets] \
+        if rank == 0 else None
+    del data
+    parity = True
+    for i, qs in enumerate(sets):
+        got = session.search(qs, K)
+        if want is not None:
+            parity &= same_bits(got, want[i])
+    stream = torch.cuda.current_stream()
+    dev_sets = [(torch.from_numpy(o).cuda(), torch.from_numpy(w).cuda()) for o, w in sets]
+    flush = torch.empty(64 << 20, dtype=torch.float32, device='cuda')
+    for i in range(args.warmup):
+        session.search_device(*dev_sets[i % 2], Q, K)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    checked = bad = 0
+    dist.barrier()
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        flush.zero_()
+        starts[i].record(stream)
+        gs, gi = session.search_device(*dev_sets[i % 2], Q, K)
+        ends[i].record(stream)
+        if want is not None:  # outside the step's events
+            checked += 1
+            bad += 0 if same_bits((gs.cpu().numpy(), gi.cpu().numpy()), want[i % 2]) else 1
+    torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    total = max_over_ranks(sum(step_ms), world)
+    dist.barrier()
+    if rank == 0:
+        print(json.dumps({
+            'metric': METRIC, 'value': Q * args.steps / (total / 1e3), 'unit': UNIT, 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': total / args.steps,
+            'higher_is_better': True, 'scaling': 'strong', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+            'config': {'workload': WORKLOAD, 'docs': spec.docs, 'queries': Q, 'terms': TERMS, 'k': K,
+                       'parallelism': f'doc-sharded x{world} (NCCL all-gather of the local top-K, merge kernel)',
+                       'l2': 'flushed between steps (256 MiB write)'},
+            'parity': {'bit_exact': bool(parity and bad == 0), 'checked_searches': checked + len(sets),
+                       'against': 'unsharded oracle'},
+        }), flush=True)
+    session.close()
+    dist.barrier()
+    dist.destroy_process_group()
+    return 0
+
+
 def run_reference(args):
     rank, world, _ = setup_dist(args.gpus)
     if rank != 0:
@@ -725,6 +791,8 @@ def main():
     ap.add_argument('--steps', type=int, default=60)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--shard', default='queries', choices=['queries', 'docs'],
+                    help='queries: a replica per GPU (the default); docs: the index split by document range')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--tile-docs', type=int, default=0)
     ap.add_argument('--fan-in', type=int, default=0)
@@ -749,6 +817,10 @@ def main():
     args = ap.parse_args()
     if args.impl == 'reference':
         return run_reference(args)
+    if args.shard == 'docs':
+        if args.warmup < 3:
+            args.warmup = 3
+        return run_doc_sharded(args)
     if args.warmup < 3:
         args.warmup = 3
 

@@ -1,9 +1,9 @@
 """Document-sharded Search: shard slicing, the gather step and the exact merge.
 
-CPU: shard_csc slices every list exactly; two gloo ranks each search their shard
-with the oracle and all-gather their local lists, and the restated rank merge of
-the gathered lists equals the unsharded oracle (the exchange and merge logic of
-ShardedSession without a GPU).  GPU: bm25_merge_topk over shards searched by
+CPU: shard_csc slices every list exactly; ShardedSession itself runs on two
+gloo ranks (each rank's local search is the oracle over its shard), all-gathers
+the local lists and merges them with the host rank merge, and equals the
+unsharded oracle; the host merge rejects a broken list as the kernel does.  GPU: bm25_merge_topk over shards searched by
 the engine equals the unsharded oracle, in both input layouts, and an invalid
 list makes its query's row -1 (the reference's merge contract).
 """
@@ -50,47 +50,82 @@ def test_shard_csc_slices_every_list(pkg, corpus):
     assert all(p[0][-1] == p[1].size == p[2].size for p in parts)
 
 
-def _gloo_rank(rank, world, port, index, data, offsets, words, k, out):
-    import torch
+def _oracle_local(indptr, indices, data, num_docs, offsets, words, k):
+    """The local search handed to ShardedSession on CPU ranks: the oracle over the rank's shard."""
+    from oracle import oracle
+    return oracle.search(indptr, indices, data, num_docs, offsets, words, k)
+
+
+def _gloo_rank(rank, world, port, index, data, queries, ks, out):
     import torch.distributed as dist
     from importlib import import_module
     os.environ['MASTER_ADDR'] = '127.0.0.1'
     os.environ['MASTER_PORT'] = str(port)
-    dist.init_process_group('gloo', rank=rank, world_size=world)
-    from oracle import oracle
+    from datetime import timedelta
+    dist.init_process_group('gloo', rank=rank, world_size=world, timeout=timedelta(seconds=60))
     sh = import_module('bm25-npu_b200.sharded')
-    lo, hi = sh.shard_range(index.num_docs, rank, world)
-    ip, ix, dt, nd = sh.shard_csc(index.offsets, index.docs, data, lo, hi)
-    ls, li = oracle.search(ip, ix, dt, nd, offsets, words, k)
-    gs = [torch.empty(ls.shape, dtype=torch.float32) for _ in range(world)]
-    gi = [torch.empty(li.shape, dtype=torch.int32) for _ in range(world)]
-    dist.all_gather(gs, torch.from_numpy(ls))
-    dist.all_gather(gi, torch.from_numpy(li))
-    bases = [sh.shard_range(index.num_docs, r, world)[0] for r in range(world)]
-    ms, mi = merge_restated(np.stack([g.numpy() for g in gs]), np.stack([g.numpy() for g in gi]), bases, k)
-    out[rank] = (ms, mi)
+    session = sh.ShardedSession(index.offsets, index.docs, data, index.num_docs, local_search=_oracle_local,
+                                device='cpu')
+    assert (session.lo, session.hi) == sh.shard_range(index.num_docs, rank, world)
+    out[rank] = [session.search(queries, k) for k in ks]
+    session.close()
     dist.barrier()
     dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_gather_and_merge_exactly(pkg, oracle_mod, corpus):
+def test_sharded_session_on_gloo_ranks_equals_unsharded(pkg, oracle_mod, corpus):
+    """ShardedSession itself on 2 gloo ranks (the CPU oracle as each rank's local search): shard slicing,
+    the all-gather and the host rank merge give the unsharded oracle's top-K on both ranks, K in {10, 100},
+    including queries with fewer than K positive documents (zero fill from the smallest global ids across
+    shards), empty queries and unknown words."""
     index, data = corpus
-    offsets, words = pack(mixed_queries(index.vocab, np.random.default_rng(2), 12, 0, 6, oov=True))
-    k = 10
-    want = oracle_mod.search(index.offsets, index.docs, data, index.num_docs, offsets, words, k)
+    df = np.diff(index.offsets)
+    rare = [int(t) for t in np.nonzero((df > 0) & (df < 4))[0][:3]]
+    rows = mixed_queries(index.vocab, np.random.default_rng(2), 12, 0, 6, oov=True) + [rare[:1], rare, []]
+    offsets, words = pack(rows)
+    ks = (10, 100)
     ctx = mp.get_context('spawn')
     with ctx.Manager() as m:
         out = m.dict()
         port = 29500 + os.getpid() % 1000
-        procs = [ctx.Process(target=_gloo_rank, args=(r, 2, port, index, data, offsets, words, k, out))
+        procs = [ctx.Process(target=_gloo_rank, args=(r, 2, port, index, data, (offsets, words), ks, out))
                  for r in range(2)]
         for p in procs:
             p.start()
         for p in procs:
-            p.join(120)
+            p.join(180)
         assert all(p.exitcode == 0 for p in procs)
-        for r in range(2):
-            assert_same_topk(*out[r], *want, f'rank {r}')
+        for j, k in enumerate(ks):
+            want = oracle_mod.search(index.offsets, index.docs, data, index.num_docs, offsets, words, k)
+            for r in range(2):
+                assert_same_topk(*out[r][j], *want, f'rank {r} k={k}')
+
+
+def test_host_merge_matches_restatement_and_rejects_bad_lists(pkg, oracle_mod, corpus):
+    """merge_topk_host (the host rank merge) equals a sort of all lists, and an out-of-order list turns its
+    query's row to -1 while the other queries stay exact (the merge operator's contract)."""
+    sh = pkg.sharded
+    index, data = corpus
+    offsets, words = pack(mixed_queries(index.vocab, np.random.default_rng(5), 8, 0, 6, oov=True) + [[]])
+    k, shards = 10, 3
+    loc_s, loc_i, bases = [], [], []
+    for r in range(shards):
+        lo, hi = sh.shard_range(index.num_docs, r, shards)
+        ls, li = oracle_mod.search(*sh.shard_csc(index.offsets, index.docs, data, lo, hi), offsets, words, k)
+        loc_s.append(ls)
+        loc_i.append(li)
+        bases.append(lo)
+    ss, ii = np.stack(loc_s), np.stack(loc_i)
+    got = sh.merge_topk_host(ss, ii, bases, index.num_docs)
+    assert_same_topk(*got, *merge_restated(ss, ii, bases, k), 'host merge vs restatement')
+    assert_same_topk(*got, *oracle_mod.search(index.offsets, index.docs, data, index.num_docs, offsets, words, k),
+                     'host merge vs unsharded')
+    bad = ss.copy()
+    bad[1, 2, 0], bad[1, 2, 1] = bad[1, 2, 1], bad[1, 2, 0] + 1.0  # order broken in shard 1, query 2
+    bs, bi = sh.merge_topk_host(bad, ii, bases, index.num_docs)
+    assert np.all(bs[2] == -1.0) and np.all(bi[2] == -1)
+    keep = [q for q in range(ss.shape[1]) if q != 2]
+    assert_same_topk(bs[keep], bi[keep], got[0][keep], got[1][keep], 'untouched rows')
 
 
 @pytest.mark.gpu
@@ -125,6 +160,9 @@ def test_device_merge_equals_unsharded(pkg, oracle_mod, corpus, cuda_ok, shards)
                                  o_s.data_ptr(), o_i.data_ptr(), shard_major=major)
             torch.cuda.synchronize()
             assert_same_topk(o_s.cpu().numpy(), o_i.cpu().numpy(), *want, f'k={k} shards={shards} major={major}')
+        # the host rank merge gives the kernel's result
+        assert_same_topk(*sh.merge_topk_host(np.stack(loc_s), np.stack(loc_i), bases, index.num_docs), *want,
+                         f'host merge k={k}')
         # an out-of-order list: that query's row becomes -1, the others stay exact
         bad = np.stack(loc_s).copy()
         bad[0, 1, [0, 1]] = bad[0, 1, [1, 0]] if bad[0, 1, 0] != bad[0, 1, 1] else [-1.0, bad[0, 1, 1]]
@@ -136,3 +174,47 @@ def test_device_merge_equals_unsharded(pkg, oracle_mod, corpus, cuda_ok, shards)
         got_s, got_i = o_s.cpu().numpy(), o_i.cpu().numpy()
         assert np.all(got_s[1] == -1.0) and np.all(got_i[1] == -1)
         assert_same_topk(got_s[[0, 2]], got_i[[0, 2]], want[0][[0, 2]], want[1][[0, 2]], 'untouched rows')
+
+
+def _nccl_single_rank(port, index, data, offsets, words, k, out):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    from importlib import import_module
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group('nccl', rank=0, world_size=1, timeout=timedelta(seconds=60),
+                            device_id=torch.device('cuda', 0))
+    sh = import_module('bm25-npu_b200.sharded')
+    session = sh.ShardedSession(index.offsets, index.docs, data, index.num_docs, query_capacity=32,
+                                word_capacity=256, max_k=100)
+    host = session.search((offsets, words), k)
+    d_o = torch.from_numpy(offsets).cuda()
+    d_w = torch.from_numpy(words).cuda()
+    gs, gi = session.search_device(d_o, d_w, offsets.size - 1, k)
+    torch.cuda.synchronize()
+    out['host'] = host
+    out['device'] = (gs.cpu().numpy(), gi.cpu().numpy())
+    session.close()
+    dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_sharded_session_on_the_gpu(pkg, oracle_mod, corpus, cuda_ok):
+    """ShardedSession with the engine as local search, NCCL and the merge kernel (one rank on the one GPU
+    here): search and search_device equal the unsharded oracle."""
+    index, data = corpus
+    offsets, words = pack(mixed_queries(index.vocab, np.random.default_rng(4), 10, 0, 6, oov=True) + [[]])
+    k = 10
+    want = oracle_mod.search(index.offsets, index.docs, data, index.num_docs, offsets, words, k)
+    ctx = mp.get_context('spawn')
+    with ctx.Manager() as m:
+        out = m.dict()
+        p = ctx.Process(target=_nccl_single_rank, args=(29700 + os.getpid() % 200, index, data, offsets, words, k,
+                                                        out))
+        p.start()
+        p.join(300)
+        assert p.exitcode == 0
+        assert_same_topk(*out['host'], *want, 'search')
+        assert_same_topk(*out['device'], *want, 'search_device')
