@@ -249,6 +249,39 @@ class StepCheck:
                 'bit_exact': self.checked > 0 and self.mismatched == 0}
 
 
+def cpu_bm25s_leg(index, k1, sets, want, budget_s=6.0, max_steps=20):
+    """bm25s's native retrieve (numba; oracle/bm25s_port.py restates its query step) on the same corpus
+    and batches, timed at n_threads in {1, 8, all host threads}: the reference's second CPU baseline
+    (standalone/bm25s_benchmark.py:76-95).  Its ranking keeps bm25s's non-strict ties, so its results
+    are checked against the oracle's as sorted score lists."""
+    from oracle import bm25s_port, oracle
+    if not bm25s_port.available():
+        return {'unavailable': 'numba is not installed'}
+    data = oracle.contributions(index, k1)
+    cores = os.cpu_count() or 1
+    out = {'kind': 'port', 'what': 'bm25s native retrieve (pinned 03eac5a8) restated with numba: zeros(N), '
+                                   'term-order scatter-add, size-K heap, sorted', 'cores': cores, 'threads': {}}
+    for n_threads in sorted({1, min(8, cores), cores}):
+        bm25s_port.retrieve(index.offsets, index.docs, data, index.num_docs, *sets[0], K, n_threads)  # compiles
+        times, ok = [], True
+        t_start = time.perf_counter()
+        i = 0
+        while i < max_steps and time.perf_counter() - t_start < budget_s:
+            t0 = time.perf_counter()
+            bs, _ = bm25s_port.retrieve(index.offsets, index.docs, data, index.num_docs, *sets[i % 2], K, n_threads)
+            times.append(time.perf_counter() - t0)
+            if want is not None:
+                ok &= bool(np.array_equal(np.sort(bs, axis=1), np.sort(want[i % 2][0], axis=1)))
+            i += 1
+        out['threads'][str(n_threads)] = {'value': Q * len(times) / sum(times), 'unit': UNIT,
+                                          'p50_ms': percentile(times, 50) * 1e3, 'searches': len(times),
+                                          'scores_match_oracle': ok}
+    best = max(out['threads'].values(), key=lambda r: r['value'])
+    out['value'] = best['value']
+    out['unit'] = UNIT
+    return out
+
+
 def timed_device(session, step, steps, warmup, flush, stream, world, with_clocks=None, check=None):
     """Device-resident steps timed with CUDA events on the launching stream, L2 flushed between
     steps; returns (step ms, main-kernel ms, clocks).
@@ -644,6 +677,87 @@ def blockmax_leg(pkg, args, local, world, flush, stream, rank):
     return out
 
 
+REFSHAPE_WORKLOAD = 'reference_10m'
+A5_PUBLISHED_MS = {'A': 1.759, 'B': 1.742}  # reference Search medians at 10M docs on its own corpus (docs/BM25S_PERFORMANCE.md:32)
+
+
+def refshape_leg(pkg, args, local, world, flush, stream, rank):
+    """The reference's own benchmark corpus shape at 10M documents (uniform over 1024 terms, lengths
+    16..48, seed 20261014, k1 1.2, b 0.75; generated by this repo's seeded generator, the same shape
+    as standalone/large_corpus.py:58-62) with the reference's query sets A and B (fixtures/A.txt,
+    B.txt, committed in tests/golden/large_corpus_n2048.npz): the plain Search timed device-resident
+    and end to end like the headline line, every timed result checked against the oracle, beside the
+    reference's published median on this shape and, on rank 0, its own C++ CPU search on this box."""
+    import torch
+    spec = pkg.CONFIG_SHAPES[REFSHAPE_WORKLOAD]
+    t = time.perf_counter()
+    index = pkg.synthetic_index(spec)
+    log(f'reference-shaped corpus: N={index.num_docs} V={index.vocab} M={index.postings} in '
+        f'{time.perf_counter() - t:.1f}s')
+    fx = np.load(ROOT / 'tests' / 'golden' / 'large_corpus_n2048.npz')
+    sets = [(fx['A_offsets'].astype(np.int64), fx['A_words'].astype(np.int32)),
+            (fx['B_offsets'].astype(np.int64), fx['B_words'].astype(np.int32))]
+    q = sets[0][0].size - 1
+    session = pkg.Bm25Session.from_lazy(index.offsets, index.docs, index.tf, index.norm, index.idf, k1=spec.k1,
+                                        query_capacity=q, word_capacity=int(sets[0][0][-1]), max_k=K,
+                                        device_id=local)
+    want = None
+    out = {'workload': REFSHAPE_WORKLOAD, 'docs': spec.docs, 'vocab': spec.vocab, 'postings': index.postings,
+           'lengths': 'uniform 16..48', 'queries': f'the reference\'s sets A and B ({q} x 3 words)', 'k': K,
+           'k1': spec.k1, 'b': spec.b, 'a5_published_median_ms': A5_PUBLISHED_MS}
+    if rank == 0:
+        from oracle import oracle
+        data = oracle.contributions(index, spec.k1)
+        want = [oracle.search(index.offsets, index.docs, data, index.num_docs, *qs, K) for qs in sets]
+        del data
+        out['parity'] = {'bit_exact': all(same_bits(session.search(qs, K), w) for qs, w in zip(sets, want)),
+                         'against': 'oracle (C restatement)'}
+        if oracle.reference_available():  # k1 = 1.2: the reference's own search gives the same bits
+            ref = oracle.ReferenceCpuSession(index, K, os.cpu_count() or 1, query_capacity=q,
+                                             word_capacity=int(sets[0][0][-1]))
+            ref_ms, ref_ok = [], True
+            for i in range(min(20, args.steps)):
+                t0 = time.perf_counter()
+                rs, ri, _ = ref.search(*sets[i % 2])
+                ref_ms.append((time.perf_counter() - t0) * 1e3)
+                ref_ok &= same_bits((rs, ri), want[i % 2])
+            out['reference_cpu'] = {'p50_ms': percentile(ref_ms, 50), 'queries_per_s': q * len(ref_ms) / (sum(ref_ms) / 1e3),
+                                    'threads': ref.threads, 'same_bits_as_oracle': bool(ref_ok),
+                                    'what': 'bm25cpu::CpuSearchSession compiled from the reference sources'}
+    dev = [(torch.from_numpy(o).cuda(), torch.from_numpy(w).cuda()) for o, w in sets]
+    d_s = torch.empty((q, K), dtype=torch.float32, device='cuda')
+    d_i = torch.empty((q, K), dtype=torch.int32, device='cuda')
+
+    def step(i):
+        o, w = dev[i % 2]
+        session.search_device(o.data_ptr(), w.data_ptr(), q, K, d_s.data_ptr(), d_i.data_ptr(), stream.cuda_stream)
+
+    check = StepCheck([d_s, d_i], lambda i: want[i % 2] if want is not None else None, args.steps)
+    step_ms, kernel_ms, _ = timed_device(session, step, args.steps, args.warmup, flush, stream, world, check=check)
+    host_ms, e2e_bad = [], 0
+    res = (np.empty((q, K), np.float32), np.empty((q, K), np.int32))
+    for i in range(args.warmup):
+        session.search(sets[i % 2], K, out=res)
+    for i in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        session.search(sets[i % 2], K, out=res)
+        host_ms.append((time.perf_counter() - t0) * 1e3)
+        if want is not None:
+            e2e_bad += 0 if same_bits(res, want[i % 2]) else 1
+    total = max_over_ranks(sum(step_ms), world)
+    out.update({'value': world * q * args.steps / (total / 1e3), 'unit': UNIT, 'p50_ms': percentile(step_ms, 50),
+                'p95_ms': percentile(step_ms, 95), 'main_kernel_ms_avg': sum(kernel_ms) / len(kernel_ms),
+                'e2e': {'p50_ms': percentile(host_ms, 50), 'p95_ms': percentile(host_ms, 95),
+                        'value': world * q * args.steps / (max_over_ranks(sum(host_ms), world) / 1e3)},
+                'timed_parity': dict(check.report(), e2e_checked=len(host_ms) if want is not None else 0,
+                                     e2e_mismatched=e2e_bad),
+                'a5_median_over_e2e_p50': (sum(A5_PUBLISHED_MS.values()) / 2) / percentile(host_ms, 50)})
+    session.close()
+    return out
+
+
 SERVE_RATES = (5000, 10000, 20000, 50000)  # --serve-all
 SERVE_RATES_DEFAULT = (5000, 20000)
 SERVE_TERMS, SERVE_KS, SERVE_POOL = (1, 16), (10, 100, 1000), 4096
@@ -810,6 +924,7 @@ def main():
     ap.add_argument('--no-mix', action='store_true', help='skip the batched 256-query mix')
     ap.add_argument('--mix-train-queries', type=int, default=120_000)
     ap.add_argument('--no-blockmax', action='store_true', help='skip the 4.2M-doc block-max workload')
+    ap.add_argument('--no-refshape', action='store_true', help="skip the reference's own corpus shape at 10M docs")
     ap.add_argument('--blockmax-train-queries', type=int, default=200_000)
     ap.add_argument('--no-serve', action='store_true', help='skip the serving loop (Poisson arrivals)')
     ap.add_argument('--serve-all', action='store_true', help='serving loop at 5k, 10k, 20k and 50k queries/s')
@@ -938,21 +1053,24 @@ def main():
     if info['kernel'] in (4, 5) and not args.no_serve and world == 1 and not (args.docs or args.vocab):
         serving = serve_leg(pkg, args, spec, index, local, SERVE_RATES if args.serve_all else SERVE_RATES_DEFAULT)
 
-    mix = blockmax = None
+    mix = blockmax = refshape = None
     full_size = info['kernel'] in (4, 5) and not (args.docs or args.vocab)
     session_open = True
-    if full_size and not (args.no_mix and args.no_blockmax):
+    if full_size and not (args.no_mix and args.no_blockmax and args.no_refshape):
         session.close()  # frees the 10M index before the next corpus is resident
         session_open = False
+    if full_size and not args.no_refshape:
+        refshape = refshape_leg(pkg, args, local, world, flush, stream, rank)
     if full_size and not args.no_mix:
         mix = mix_leg(pkg, args, local, world, flush, stream, rank)
     if full_size and not args.no_blockmax:
         blockmax = blockmax_leg(pkg, args, local, world, flush, stream, rank)
 
-    cpu = None
+    cpu = cpu_bm25s = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         res = cpu_search_leg(index, sets, K, budget_s=20.0, max_steps=40)
         cpu = {k2: res[k2] for k2 in ('value', 'unit', 'cores', 'kind', 'sample')}
+        cpu_bm25s = cpu_bm25s_leg(index, spec.k1, sets, want)
 
     if rank == 0:
         line = {
@@ -990,10 +1108,14 @@ def main():
             line['batched_mix'] = mix
         if blockmax is not None:
             line['blockmax_c4'] = blockmax
+        if refshape is not None:
+            line['reference_shape'] = refshape
         if serving is not None:
             line['serving'] = serving
         if cpu is not None:
             line['cpu_baseline'] = cpu
+        if cpu_bm25s is not None:
+            line['cpu_baseline_bm25s'] = cpu_bm25s
         print(json.dumps(line), flush=True)
     if session_open:
         session.close()

@@ -52,7 +52,8 @@ class LazyIndex:
 
 @dataclass
 class CorpusSpec:
-    """Seeded synthetic corpus shape: Zipf(s) token ranks, lognormal lengths (mean, sigma)."""
+    """Seeded synthetic corpus shape: Zipf(s) token ranks (s = 0: uniform), lognormal lengths (mean,
+    sigma), or uniform integer lengths in [mean - |sigma|, mean + |sigma|] when sigma < 0."""
 
     docs: int
     vocab: int
@@ -64,12 +65,16 @@ class CorpusSpec:
     b: float = 0.75
 
 
-# Workload shapes: 8192 docs / V 30k; 10M docs / V 1M; 8.8M passages / V 2.5M; 4.2M docs / V 1M.
+# Workload shapes: 8192 docs / V 30k; 10M docs / V 1M; 8.8M passages / V 2.5M; 4.2M docs / V 1M; and
+# the reference's own benchmark corpus shape (standalone/large_corpus.py:58-62: tokens uniform over
+# 1024 terms, lengths uniform in 16..48, seed 20261014, its builder's k1 1.2 and b 0.75) at 10M docs.
 CONFIG_SHAPES = {
     'synthetic_8192': CorpusSpec(docs=8192, vocab=30000),
     'synthetic_10m': CorpusSpec(docs=10_000_000, vocab=1_000_000),
     'passages_8p8m': CorpusSpec(docs=8_800_000, vocab=2_500_000, zipf_s=1.05, len_mean=56.0),
     'blockmax_4p2m': CorpusSpec(docs=4_200_000, vocab=1_000_000, len_mean=80.0),
+    'reference_10m': CorpusSpec(docs=10_000_000, vocab=1024, zipf_s=0.0, len_mean=32.0, len_sigma=-16.0,
+                                seed=20261014, k1=1.2, b=0.75),
 }
 
 

@@ -12,9 +12,11 @@
  *     norm = f32(k1 * (1 - b + b * len / avgdl))           large_corpus.py:174
  * evaluated in double and rounded once, as the reference does.
  *
- * The document stream differs from the reference's uniform one: token ranks
- * follow Zipf(s) over V terms (term id = rank - 1) and lengths follow
- * round(lognormal(ln(mean) - sigma^2/2, sigma)), at least 1.  Every random draw
+ * The document stream: token ranks follow Zipf(s) over V terms (term id =
+ * rank - 1; s = 0 draws every term alike, the reference's uniform stream of
+ * large_corpus.py:58-62) and lengths follow round(lognormal(ln(mean) -
+ * sigma^2/2, sigma)), at least 1 -- or, for sigma < 0, a uniform integer in
+ * [mean - |sigma|, mean + |sigma|] (mean 32, sigma -16: the reference's 16..48).  Every random draw
  * is a counter-based hash of (seed, document, position), so the corpus does not
  * depend on the thread count and pass 2 replays pass 1 exactly.
  */
@@ -55,6 +57,13 @@ typedef struct {
 
 static int32_t doc_length(const synth_t *s, int64_t d)
 {
+    if (s->len_sigma < 0) {  /* uniform integer lengths in [mean - |sigma|, mean + |sigma|] */
+        const int64_t lo = (int64_t)floor(s->len_mean + s->len_sigma + 0.5);
+        const int64_t hi = (int64_t)floor(s->len_mean - s->len_sigma + 0.5);
+        const uint64_t x = draw(s->seed, (uint64_t)d, 0xFFFFFFFF00000001ull);
+        const int64_t len = lo + (int64_t)(x % (uint64_t)(hi - lo + 1));
+        return (int32_t)(len < 1 ? 1 : (len > SYNTH_MAX_LEN ? SYNTH_MAX_LEN : len));
+    }
     const double mu = log(s->len_mean) - 0.5 * s->len_sigma * s->len_sigma;
     const double u1 = unit53(draw(s->seed, (uint64_t)d, 0xFFFFFFFF00000001ull));
     const double u2 = unit53(draw(s->seed, (uint64_t)d, 0xFFFFFFFF00000002ull));
@@ -200,7 +209,8 @@ void synth_destroy(void *handle)
 void *synth_create(int64_t docs, int64_t vocab, double zipf_s, double len_mean, double len_sigma, uint64_t seed,
                    int threads)
 {
-    if (docs < 1 || docs > INT32_MAX || vocab < 1 || vocab >= INT32_MAX || len_mean <= 0 || len_sigma < 0)
+    if (docs < 1 || docs > INT32_MAX || vocab < 1 || vocab >= INT32_MAX || len_mean <= 0 ||
+        (len_sigma < 0 && len_mean + len_sigma < 1))
         return NULL;
     synth_t *s = (synth_t *)calloc(1, sizeof(synth_t));
     if (!s)

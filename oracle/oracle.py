@@ -10,6 +10,7 @@ product library never loads it.
 """
 
 import ctypes
+import os
 import subprocess
 from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_int32, c_int64, c_size_t, c_void_p
 from pathlib import Path
@@ -20,7 +21,8 @@ HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / 'liboracle.so'
 REF_SO = HERE / '_ref' / 'libref_cpu.so'
 REF_TEST = HERE / '_ref' / 'cpu_index_search_tests'
-REFERENCE_ROOT = Path('/root/reference')
+# where the reference's sources are read from when its CPU search is compiled (override: REFERENCE_ROOT)
+REFERENCE_ROOT = Path(os.environ.get('REFERENCE_ROOT', '/root/reference'))
 
 
 def build(with_reference=None):

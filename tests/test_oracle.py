@@ -106,3 +106,21 @@ def test_merge_of_document_shards(pkg, oracle_mod):
             lists_i.append(i[0])
         ms, mi = oracle_mod.merge(np.stack(lists_s), np.stack(lists_i), 10)
         assert_same_topk(ms[None], mi[None], gs[qi:qi + 1], gi[qi:qi + 1])
+
+
+def test_bm25s_port_scores_equal_oracle(pkg, oracle_mod):
+    """The numba restatement of bm25s's retrieve (the timed bm25s CPU baseline) returns the oracle's top-K
+    scores for every query (its ids may differ only among tied scores: bm25s does not rank ties)."""
+    from oracle import bm25s_port
+    if not bm25s_port.available():
+        pytest.skip('numba not installed')
+    spec = pkg.CorpusSpec(docs=20_000, vocab=4_000, seed=12, k1=1.2)
+    index = pkg.synthetic_index(spec)
+    data = oracle_mod.contributions(index, spec.k1)
+    qo, w = pkg.synthetic_queries(index.offsets, 12, 1, 6, 9)
+    for k in (1, 10, 50):
+        bs, bi = bm25s_port.retrieve(index.offsets, index.docs, data, index.num_docs, qo, w, k, 2)
+        rs, ri = oracle_mod.search(index.offsets, index.docs, data, index.num_docs, qo, w, k)
+        assert np.array_equal(np.sort(bs, axis=1), np.sort(rs, axis=1)), k
+        untied = np.array([len(set(r)) == r.size for r in rs])
+        assert np.array_equal(np.sort(bi[untied], axis=1), np.sort(ri[untied], axis=1)), k

@@ -59,3 +59,20 @@ def test_index_files_round_trip(pkg, tmp_path):
     back = pkg.read_index_dir(tmp_path)
     for f in ('offsets', 'docs', 'tf', 'norm', 'idf'):
         assert np.array_equal(getattr(idx, f), getattr(back, f))
+
+
+def test_reference_shaped_corpus(pkg):
+    """The reference's benchmark corpus shape (standalone/large_corpus.py:58-62): tokens uniform over
+    1024 terms, lengths uniform in 16..48, k1 1.2; deterministic for any thread count."""
+    import dataclasses
+    spec = dataclasses.replace(pkg.CONFIG_SHAPES['reference_10m'], docs=40_000)
+    assert (spec.vocab, spec.zipf_s, spec.k1, spec.b, spec.seed) == (1024, 0.0, 1.2, 0.75, 20261014)
+    a = pkg.synthetic_index(spec, threads=1)
+    b = pkg.synthetic_index(spec, threads=4)
+    assert np.array_equal(a.offsets, b.offsets) and np.array_equal(a.docs, b.docs)
+    assert a.doc_len.min() == 16 and a.doc_len.max() == 48
+    assert abs(a.doc_len.mean() - 32.0) < 0.3
+    counts = np.bincount(a.doc_len - 16, minlength=33)
+    assert counts.min() > 0.8 * counts.mean()  # every length in 16..48 about equally often
+    df = np.diff(a.offsets)
+    assert df.min() > 0.85 * df.mean() and df.max() < 1.15 * df.mean()  # no term favoured
