@@ -833,12 +833,19 @@ def run_doc_sharded(args):
     want = [oracle.search(index.offsets, index.docs, data, index.num_docs, *qs, K) for qs in sets] \
         if rank == 0 else None
     del data
-    parity = True
+    host_ok = []
+    first_diff = None
     for i, qs in enumerate(sets):
         got = session.search(qs, K)
         if want is not None:
-            parity &= same_bits(got, want[i])
-    stream = torch.cuda.current_stream()
+            host_ok.append(same_bits(got, want[i]))
+            if not host_ok[-1] and first_diff is None:
+                bad_q = [j for j in range(Q) if not same_bits((got[0][j], got[1][j]), (want[i][0][j], want[i][1][j]))]
+                first_diff = {'batch': i, 'queries': bad_q, 'got': [got[0][bad_q[0]].tolist(), got[1][bad_q[0]].tolist()],
+                              'want': [want[i][0][bad_q[0]].tolist(), want[i][1][bad_q[0]].tolist()]}
+    parity = all(host_ok)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     dev_sets = [(torch.from_numpy(o).cuda(), torch.from_numpy(w).cuda()) for o, w in sets]
     flush = torch.empty(64 << 20, dtype=torch.float32, device='cuda')
     for i in range(args.warmup):
@@ -869,6 +876,7 @@ def run_doc_sharded(args):
                        'parallelism': f'doc-sharded x{world} (NCCL all-gather of the local top-K, merge kernel)',
                        'l2': 'flushed between steps (256 MiB write)'},
             'parity': {'bit_exact': bool(parity and bad == 0), 'checked_searches': checked + len(sets),
+                       'host_searches_exact': host_ok, 'timed_mismatched': bad, 'first_difference': first_diff,
                        'against': 'unsharded oracle'},
         }), flush=True)
     session.close()

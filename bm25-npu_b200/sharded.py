@@ -128,6 +128,10 @@ class ShardedSession:
                                     dtype=np.int32)
         self.bases = torch.from_numpy(self._bases_host).to(self.device)
         self._bufs = {}  # gather and output buffers per (q, k), reused across Searches
+        # device Searches run on a stream of their own, fenced against the caller's current stream on
+        # both sides (the caller's may be the legacy default stream, whose handle the engine would read
+        # as "the session's own stream")
+        self._stream = torch.cuda.Stream(self.device) if self.device.type == 'cuda' else None
 
     def local(self, queries, k):
         """This rank's top-K over its own documents (local ids), host arrays."""
@@ -176,8 +180,9 @@ class ShardedSession:
         return out_s.cpu().numpy(), out_i.cpu().numpy()
 
     def search_device(self, d_offsets, d_words, q, k, learned=False):
-        """Device query batch (torch int64 offsets, int32 words) -> global (scores, ids) [q, k] tensors; the
-        local search writes into this rank's slot of the gather buffers' inputs, no allocation per call."""
+        """Device query batch (torch int64 offsets, int32 words) -> global (scores, ids) [q, k] tensors (this
+        session's buffers, valid until its next Search of the same shape), ordered after the caller's
+        current stream's prior work and before its later work; no allocation per call."""
         import torch
         if self.session is None:
             raise InnerError(n.BM25_ERR_ILLEGAL_OPERATION, 'search_device needs the engine as local search')
@@ -188,14 +193,19 @@ class ShardedSession:
                                torch.empty((q, k), dtype=torch.int32, device=dev),
                                torch.empty(q, dtype=torch.int32, device=dev))
         ls, li, ex = self._bufs[key]
-        stream = torch.cuda.current_stream(dev).cuda_stream
-        if learned:
-            self.session.search_learned_device(d_offsets.data_ptr(), d_words.data_ptr(), q, k, ls.data_ptr(),
-                                               li.data_ptr(), ex.data_ptr(), stream)
-        else:
-            self.session.search_device(d_offsets.data_ptr(), d_words.data_ptr(), q, k, ls.data_ptr(),
-                                       li.data_ptr(), stream)
-        return self.gather_merge(ls, li)
+        caller = torch.cuda.current_stream(dev)
+        self._stream.wait_stream(caller)  # the query batch is ready
+        with torch.cuda.stream(self._stream):
+            stream = self._stream.cuda_stream
+            if learned:
+                self.session.search_learned_device(d_offsets.data_ptr(), d_words.data_ptr(), q, k, ls.data_ptr(),
+                                                   li.data_ptr(), ex.data_ptr(), stream)
+            else:
+                self.session.search_device(d_offsets.data_ptr(), d_words.data_ptr(), q, k, ls.data_ptr(),
+                                           li.data_ptr(), stream)
+            out = self.gather_merge(ls, li)
+        caller.wait_stream(self._stream)  # the caller sees the merged lists
+        return out
 
     def close(self):
         if self.session is not None:

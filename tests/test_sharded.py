@@ -192,10 +192,18 @@ def _nccl_single_rank(port, index, data, offsets, words, k, out):
     host = session.search((offsets, words), k)
     d_o = torch.from_numpy(offsets).cuda()
     d_w = torch.from_numpy(words).cuda()
-    gs, gi = session.search_device(d_o, d_w, offsets.size - 1, k)
+    # an empty batch between the real ones: each result must be its own batch's, on the legacy
+    # default stream (the caller's current stream here), with no synchronisation in between
+    e_o = torch.zeros(offsets.size, dtype=torch.int64, device='cuda')
+    e_w = torch.zeros(1, dtype=torch.int32, device='cuda')
+    results = []
+    for _ in range(3):
+        gs, gi = session.search_device(d_o, d_w, offsets.size - 1, k)
+        results.append((gs.clone(), gi.clone()))
+        session.search_device(e_o, e_w, offsets.size - 1, k)
     torch.cuda.synchronize()
     out['host'] = host
-    out['device'] = (gs.cpu().numpy(), gi.cpu().numpy())
+    out['device'] = [(a.cpu().numpy(), b.cpu().numpy()) for a, b in results]
     session.close()
     dist.destroy_process_group()
 
@@ -217,4 +225,5 @@ def test_sharded_session_on_the_gpu(pkg, oracle_mod, corpus, cuda_ok):
         p.join(300)
         assert p.exitcode == 0
         assert_same_topk(*out['host'], *want, 'search')
-        assert_same_topk(*out['device'], *want, 'search_device')
+        for r, got in enumerate(out['device']):
+            assert_same_topk(*got, *want, f'search_device {r}')
