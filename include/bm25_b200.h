@@ -55,7 +55,9 @@ typedef struct bm25_options {
     int32_t prune;           /* nonzero: build the 128-document block-max index and the term statistics of
                                 the pruned and learned Searches (tile-group kernel only) */
     int64_t candidate_capacity; /* max_k > 32: candidates kept per query (0 = automatic, 512 K and at least
-                                   2^18); a query that overflows it is searched again from its final bound */
+                                   2^18); a query that overflows it is searched again from its final bound.
+                                   A Search whose K-th score is tied by more documents than this overflows
+                                   every retry pass and fails with BM25_ERR_INNER_ERROR (device status 32) */
     float prune_route;       /* pruned Searches of 32 queries or more: a query keeping more than this share of
                                 its 128-document blocks is streamed by the tile-group kernel instead
                                 (0 = 0.3; negative = never) */

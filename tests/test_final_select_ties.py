@@ -76,3 +76,19 @@ def test_tied_scores_large_k(pkg, oracle_mod, cuda_ok):
             want = oracle_mod.search(indptr, indices, data, N, offsets, words, k)
             assert_same_topk(*s.search((offsets, words), k), *want, f'k={k}')
             assert s.device_status() == 0
+
+
+@pytest.mark.gpu
+def test_ties_beyond_the_candidate_buffer_are_reported(pkg, cuda_ok):
+    """K > 32 keeps every document at or above the running bound in a buffer of candidate_capacity per
+    query.  When more documents than that tie at the K-th score (term 0: 9,363 documents, all 1.0; K =
+    1000, 2,048 slots), every retry pass starts from that score and overflows again: the Search reports a
+    device error (candidate overflow, status bit 32) instead of a wrong answer, as bm25_b200.h states."""
+    indptr, indices, data = tied_corpus()
+    offsets, words = pack([[0]])
+    with pkg.Bm25Session.from_csc(indptr, indices, data, N, query_capacity=1, word_capacity=4, max_k=1000,
+                                  candidate_capacity=2048) as s:
+        with pytest.raises(pkg.InnerError) as err:
+            s.search((offsets, words), 1000)
+        status = int(str(err.value).split('status=')[1].split()[0].rstrip('.,;'))
+        assert status & 32, str(err.value)
