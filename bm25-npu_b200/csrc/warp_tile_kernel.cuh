@@ -54,7 +54,7 @@ constexpr int kWtTile = 1024;        // documents per tile (one warp's row)
 constexpr int kWtWarps = 8;
 constexpr int kWtThreads = kWtWarps * 32;
 constexpr int kWtWindow = 128;       // postings per window (4 per lane)
-constexpr int kWtLead = 4;           // words whose first window is loaded before any add
+constexpr int kWtLead = 3;           // words whose first window is loaded before any add
 constexpr int kPlanRowChunk = 2048;  // plan row entries per PlanRowsKernel CTA (grid.y)
 constexpr int kTermTopK = 32;        // largest posting scores kept per term
 
