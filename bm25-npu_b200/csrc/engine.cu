@@ -1183,12 +1183,15 @@ class Engine {
                 sa.item_count = d_item_count_;
                 sa.item_cap = item_cap_;
             }
-            // plain Searches of one K <= 32 in a warp-tile session: plan rows of the words without a
-            // directory row, then the warp-tile kernel.  Every other Search -- pruned, a K per query or
-            // K > 32 (no starting bound from the term statistics: the warp-tile kernel's wider first
-            // wave of claims would append far more candidates) -- takes the (query word, tile) plan and
-            // the tile-group kernel.
-            const bool warp_tile = plan_.kernel == BM25_KERNEL_WARP_TILE && !tau && !kq && k <= bm25k::kMaxSmallK;
+            // A warp-tile session runs the warp-tile kernel for plain Searches of one K <= 32 and for
+            // every pass that streams from a bound already set (the routed queries of a pruned Search,
+            // from their learned bound; retry passes, from their proven one); it needs the plan rows of
+            // the words without a directory row.  The first pass of a pruned Search is block-scored and
+            // that of a batch with a K per query or K > 32 runs the tile-group kernel (no starting bound
+            // from the term statistics there: the warp-tile kernel's wider first wave of claims would
+            // append far more candidates); both take the (query word, tile) plan.
+            const bool wt_session = plan_.kernel == BM25_KERNEL_WARP_TILE;
+            const bool warp_tile = wt_session && !tau && !kq && k <= bm25k::kMaxSmallK;
             sa.plan_rows = plan_rows_;
             sa.prefetch = 1;
             sa.wait_budget = opts_.wait_budget_cycles;
@@ -1197,15 +1200,20 @@ class Engine {
             sa.dense_row = d_dense_row_;
             sa.dense_stride = dense_stride_;
             sa.inject = d_inject_;
-            if (warp_tile)
+            if (warp_tile) {
                 bm25k::PlanRowsKernel<<<bm25k::PlanRowsGrid(opts_.word_capacity, plan_.tiles, sms_),
                                         bm25k::kPlanThreads, 0, s>>>(sa);
-            else if (learned)
-                LaunchOverlapped(bm25k::PlanKernel, bm25k::PlanGrid(opts_.word_capacity, plan_.tiles, sms_),
-                                 bm25k::kPlanThreads, 0, s, sa);
-            else
-                bm25k::PlanKernel<<<bm25k::PlanGrid(opts_.word_capacity, plan_.tiles, sms_), bm25k::kPlanThreads, 0,
-                                    s>>>(sa);
+            } else {
+                if (learned)
+                    LaunchOverlapped(bm25k::PlanKernel, bm25k::PlanGrid(opts_.word_capacity, plan_.tiles, sms_),
+                                     bm25k::kPlanThreads, 0, s, sa);
+                else
+                    bm25k::PlanKernel<<<bm25k::PlanGrid(opts_.word_capacity, plan_.tiles, sms_), bm25k::kPlanThreads,
+                                        0, s>>>(sa);
+                if (wt_session)  // for the streaming passes; set up while the plan kernel runs
+                    LaunchOverlapped(bm25k::PlanRowsKernel, bm25k::PlanRowsGrid(opts_.word_capacity, plan_.tiles, sms_),
+                                     bm25k::kPlanThreads, 0, s, sa);
+            }
             Cuda(cudaGetLastError(), "plan kernel launch");
             const long long claims = (long long)q * ((plan_.tiles + bm25k::kWgWarps - 1) / bm25k::kWgWarps);
             const int wg_grid = (int)std::max<long long>(1, std::min<long long>(tg_grid_, claims));
@@ -1219,7 +1227,7 @@ class Engine {
             }
             auto tile_group = [&](const bm25k::StreamArgs &args) {
                 const bool lean = !args.retry && !args.kq && k <= bm25k::kMaxSmallK;
-                if (warp_tile) {
+                if (warp_tile || (wt_session && args.retry)) {
                     if (!args.retry)  // right after the plan rows: set up while they are built
                         LaunchOverlapped(lean ? bm25k::WarpTileKernel<kWtClaimTiles, true>
                                               : bm25k::WarpTileKernel<kWtClaimTiles, false>,

@@ -455,8 +455,10 @@ __global__ void __launch_bounds__(kPlanThreads) PlanRowsKernel(const StreamArgs 
     }
     const int n_ent = a.tiles + 1;
     const int e0 = (int)blockIdx.y * kPlanRowChunk, e1 = min(n_ent, e0 + kPlanRowChunk);
-    if (e0 >= e1)
+    if (e0 >= e1) {
+        WaitPrerequisites();
         return;
+    }
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (long long w = blockIdx.x; w < total; w += gridDim.x) {
         const int term = __ldg(a.words + w);
@@ -515,6 +517,9 @@ __global__ void __launch_bounds__(kPlanThreads) PlanRowsKernel(const StreamArgs 
         }
         __syncthreads();  // ent, lim and wmin are rewritten for the next word
     }
+    // launched overlapped after the plan kernel (a pruned or batched Search): complete only after it,
+    // so that every later kernel sees that plan too
+    WaitPrerequisites();
 }
 
 // Grid of PlanRowsKernel for a batch capacity of `words` query words.
