@@ -892,6 +892,29 @@ class Engine {
             bm25k::TermStatsKernel<<<grid, 256, 0, stream_>>>((const long long *)d_indptr_, d_data_, vocab_,
                                                                d_term_top_, d_term_mean_);
             Cuda(cudaGetLastError(), "term statistics kernel launch");
+            if (plan_.kernel == BM25_KERNEL_WARP_TILE) {
+                // scores at ranks 64 .. 1024 of every term with more than 32 postings: the warp-tile
+                // kernel's starting bounds for K above 32
+                d_term_rank_ = static_cast<float *>(Alloc(vocab_ * bm25k::kRankCount * sizeof(float),
+                                                          "cudaMalloc term ranks"));
+                Cuda(cudaMemsetAsync(d_term_rank_, 0, vocab_ * bm25k::kRankCount * sizeof(float), stream_),
+                     "cudaMemset term ranks");
+                std::vector<int32_t> long_terms;
+                for (int64_t t = 0; t < vocab_; ++t)
+                    if (dfs[t] > 32)
+                        long_terms.push_back((int32_t)t);
+                if (!long_terms.empty()) {
+                    int32_t *d_lt = static_cast<int32_t *>(Alloc(long_terms.size() * sizeof(int32_t),
+                                                                 "cudaMalloc rank terms"));
+                    Cuda(cudaMemcpy(d_lt, long_terms.data(), long_terms.size() * sizeof(int32_t),
+                                    cudaMemcpyHostToDevice),
+                         "rank terms upload");
+                    bm25k::TermRanksKernel<<<(int)std::min<size_t>(long_terms.size(), 148 * 4), bm25k::kLargeThreads,
+                                             0, stream_>>>((const long long *)d_indptr_, d_data_, d_lt,
+                                                           (int)long_terms.size(), d_term_rank_);
+                    Cuda(cudaGetLastError(), "term rank kernel launch");
+                }
+            }
             Cuda(cudaStreamSynchronize(stream_), "term statistics kernel");
         }
         if (opts_.prune) {
@@ -1196,6 +1219,7 @@ class Engine {
             sa.prefetch = 1;
             sa.wait_budget = opts_.wait_budget_cycles;
             sa.term_top = plan_.kernel == BM25_KERNEL_WARP_TILE ? d_term_top_ : nullptr;
+            sa.term_rank = d_term_rank_;
             sa.dense = d_dense_;
             sa.dense_row = d_dense_row_;
             sa.dense_stride = dense_stride_;
@@ -1535,6 +1559,7 @@ class Engine {
     bm25k::PlanEntry *plan_entries_ = nullptr;
     int *plan_rows_ = nullptr;
     float *d_dense_ = nullptr;  // dense rows of the most frequent terms (warp-tile kernel)
+    float *d_term_rank_ = nullptr;  // [vocab][5] scores at ranks 64 .. 1024 (warp-tile kernel)
     int32_t *d_dense_row_ = nullptr;
     int64_t dense_rows_ = 0, dense_stride_ = 0;
     size_t tg_smem_ = 0;  // tile-group kernel: dynamic shared memory and grid

@@ -156,6 +156,7 @@ struct StreamArgs {
     // frequency): the warp-tile kernel starts a K <= 32 query's running bound at the largest K-th
     // score of its words, which K documents reach (nullptr: start at 0)
     const float *term_top;
+    const float *term_rank;  // [vocab][5] scores at ranks 64 .. 1024: starting bounds for K in 33 .. 1024
     // [dense row][dense_stride] per-document scores of the terms kept dense (0 where absent);
     // dense_row [vocab]: a term's dense row or -1
     const float *dense;
@@ -1297,6 +1298,67 @@ __device__ void BlockBitonic(int p, const Before &before, const Swap &swap)
             }
             __syncthreads();
         }
+}
+
+// Each listed term's posting scores at ranks 64, 128, 256, 512 and 1024 (largest first; 0 past the
+// term's document frequency): ranks [term][kRankCount].  One CTA per term: a list of at most 1024
+// postings is sorted whole in shared memory; a longer one takes its 1024-th largest score by three
+// radix passes, then sorts the scores above it (fewer than 1024; the rest of the ranks tie at it).
+constexpr int kRankCount = 5;
+__global__ void __launch_bounds__(kLargeThreads) TermRanksKernel(const long long *indptr, const float *data,
+                                                                 const int *terms, int n_terms, float *ranks)
+{
+    __shared__ LargeShared sh;
+    const int tid = threadIdx.x;
+    for (int ti = blockIdx.x; ti < n_terms; ti += gridDim.x) {
+        const int t = terms[ti];
+        const long long s = indptr[t];
+        const int df = (int)(indptr[t + 1] - s);
+        const float *v = data + s;
+        float top = 0.0f;  // the 1024-th largest score when the list is longer
+        if (tid == 0)
+            sh.sel_count = 0u;
+        __syncthreads();
+        if (df <= kLargeMaxK) {
+            for (int i = tid; i < kLargeMaxK; i += kLargeThreads)
+                sh.sel_s[i] = i < df ? fmaxf(v[i], 0.0f) : -1.0f;
+            if (tid == 0)
+                sh.sel_count = (unsigned)df;
+        } else {
+            auto key_of = [&](int i, unsigned *key) {
+                *key = __float_as_uint(fmaxf(__ldg(v + i), 0.0f)) & 0x7fffffffu;
+                return true;
+            };
+            unsigned rest = 0;
+            const unsigned kth = RadixSelect31(sh, df, key_of, (unsigned)kLargeMaxK, &rest);
+            top = __uint_as_float(kth);
+            for (int i = tid; i < kLargeMaxK; i += kLargeThreads)
+                sh.sel_s[i] = -1.0f;
+            __syncthreads();
+            for (int i = tid; i < df; i += kLargeThreads) {
+                const float x = fmaxf(__ldg(v + i), 0.0f);
+                if (x > top)
+                    sh.sel_s[atomicAdd(&sh.sel_count, 1u)] = x;  // fewer than 1024 are above the 1024-th
+            }
+        }
+        __syncthreads();
+        BlockBitonic(
+            kLargeMaxK, [&](int i, int j) { return sh.sel_s[i] > sh.sel_s[j]; },
+            [&](int i, int j) {
+                const float x = sh.sel_s[i];
+                sh.sel_s[i] = sh.sel_s[j];
+                sh.sel_s[j] = x;
+            });
+        if (tid < kRankCount) {
+            const int r = 64 << tid;  // rank r: sel_s[r - 1] when above the 1024-th, else that score
+            const unsigned above = df <= kLargeMaxK ? (unsigned)df : sh.sel_count;
+            float x = 0.0f;
+            if (r <= df)
+                x = (unsigned)r <= above ? sh.sel_s[r - 1] : top;
+            ranks[(long long)t * kRankCount + tid] = x;
+        }
+        __syncthreads();  // sh is reused for the next term
+    }
 }
 
 __global__ void __launch_bounds__(kLargeThreads) FinalSelectLargeKernel(const StreamArgs a)

@@ -34,10 +34,11 @@
 //     score (contributions are non-negative, so a document's final sum is the
 //     largest it takes); a tile whose largest score is below the bound only
 //     clears its row.
-// A K <= 32 query's running bound starts at the largest, over its words, of the
-// word's K-th largest posting score (term statistics kept at create): K
-// documents hold that word with at least that score, and a non-negative FP32
-// sum is at least each of its terms, so K documents reach it.  Without it the
+// A query's running bound starts at the largest, over its words, of the word's
+// K-th largest posting score (K <= 32; for K up to 1024, its score at the
+// smallest rank 64, 128, ..., 1024 not below K) from term statistics kept at
+// create: that many documents hold the word with at least that score, and a
+// non-negative FP32 sum is at least each of its terms, so K documents reach it.  Without it the
 // first wave of claims (every warp's first tiles) would run with no bound and
 // select and append in full.
 // No producer warp, no mbarrier, no wait on another warp: the only latencies
@@ -121,6 +122,8 @@ __device__ __forceinline__ void WtWordOffsets(const StreamArgs &a, long long w, 
     }
     if (a.term_top && k <= kTermTopK)
         seed = fmaxf(seed, __ldg(a.term_top + (long long)term * kTermTopK + (k - 1)));
+    else if (a.term_rank && k <= 1024)  // the score at the smallest rank 64 << j >= k: K documents reach it
+        seed = fmaxf(seed, __ldg(a.term_rank + (long long)term * 5 + (31 - __clz(k - 1)) - 5));
     if (a.dense_row)
         drow = __ldg(a.dense_row + term);
     const int base = (int)__ldg(a.indptr + term);
