@@ -612,6 +612,7 @@ class Engine {
         bm25k::LearnedArgs la{};
         la.indptr = (const long long *)d_indptr_;
         la.top = d_term_top_;
+        la.rank = d_term_rank_;
         la.mean = d_term_mean_;
         la.vocab = (int)vocab_;
         la.qoffsets = (const long long *)qoffsets;

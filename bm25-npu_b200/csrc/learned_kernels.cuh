@@ -10,7 +10,9 @@
 //   word with at least that score, and every FP32 sum of non-negative
 //   contributions is at least each of its terms -- rounded addition is
 //   monotone -- so K documents reach it and it never makes a query fall back);
-//   0 for K > 32; -1 when the query's words hold fewer than K postings in all
+//   for K in 33..1024 the same with the word's score at the smallest rank 64,
+//   128, ..., 1024 not below K (term ranks, warp-tile sessions; else 0); -1
+//   when the query's words hold fewer than K postings in all
 //   (fewer than K documents can match: such a query is not pruned).
 // LearnedBoundKernel -- features -> threshold MLP (log of the K-th score) ->
 //   tau = max(exp(prediction - margin), safe bound); without a model tau is the
@@ -54,6 +56,7 @@ __global__ void TermStatsKernel(const long long *indptr, const float *data, long
 struct LearnedArgs {
     const long long *indptr;
     const float *top;   // [vocab][kTermTop]
+    const float *rank;  // [vocab][5] scores at ranks 64 .. 1024 (safe bounds for K above 32), or nullptr
     const float *mean;  // [vocab]
     int vocab;
     const long long *qoffsets;
@@ -87,6 +90,7 @@ __device__ __forceinline__ float QueryFeaturesWarp(const LearnedArgs &a, int q, 
     const int n = (int)nl;
     const int k = a.kq ? min(max(a.kq[q], 1), a.k) : a.k, kk = min(k, kTermTop), h = (kk - 1) / 2;
     long long postings = 0;
+    float max_rank = 0.0f;  // K > 32: the largest, over the words, score at the smallest rank >= K
     float sum_top = 0.0f, sum_kth = 0.0f, max_kth = 0.0f, sum_mean = 0.0f, sum_ldf = 0.0f;
     float min_ldf = FLT_MAX, max_half = 0.0f, sum_half = 0.0f;
     int valid = 0, oov = 0;
@@ -105,6 +109,8 @@ __device__ __forceinline__ float QueryFeaturesWarp(const LearnedArgs &a, int q, 
         }
         const float *t = a.top + (long long)w * kTermTop;
         const float mx = t[0], kth = t[kk - 1], half = t[h];
+        if (a.rank && k > kTermTop && k <= 1024)
+            max_rank = fmaxf(max_rank, a.rank[(long long)w * 5 + (31 - __clz(k - 1)) - 5]);
         const long long df = a.indptr[w + 1] - a.indptr[w];
         postings += df;
         const float ldf = log1pf((float)df);
@@ -130,6 +136,7 @@ __device__ __forceinline__ float QueryFeaturesWarp(const LearnedArgs &a, int q, 
         sum_top += __shfl_xor_sync(kFull, sum_top, o);
         sum_kth += __shfl_xor_sync(kFull, sum_kth, o);
         max_kth = fmaxf(max_kth, __shfl_xor_sync(kFull, max_kth, o));
+        max_rank = fmaxf(max_rank, __shfl_xor_sync(kFull, max_rank, o));
         sum_mean += __shfl_xor_sync(kFull, sum_mean, o);
         sum_ldf += __shfl_xor_sync(kFull, sum_ldf, o);
         min_ldf = fminf(min_ldf, __shfl_xor_sync(kFull, min_ldf, o));
@@ -189,7 +196,7 @@ __device__ __forceinline__ float QueryFeaturesWarp(const LearnedArgs &a, int q, 
     __syncwarp();
     if (postings < k)
         return -1.0f;
-    return k <= kTermTop ? max_kth : 0.0f;
+    return k <= kTermTop ? max_kth : max_rank;
 }
 
 // One warp per query.
