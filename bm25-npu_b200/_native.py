@@ -88,8 +88,8 @@ SIGNATURES = {
                             POINTER(Options), POINTER(c_void_p)]),
     'bm25_create_lazy': (c_int, [POINTER(c_int64), POINTER(c_int32), POINTER(c_float), POINTER(c_float),
                                  POINTER(c_float), c_int64, c_int64, c_float, POINTER(Options), POINTER(c_void_p)]),
-    'bm25_search': (c_int, [c_void_p, POINTER(c_int64), POINTER(c_int32), c_int64, c_int32, POINTER(c_float),
-                            POINTER(c_int32)]),
+    # the per-Search call takes plain addresses (numpy's .ctypes.data): no pointer objects on the hot path
+    'bm25_search': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p]),
     'bm25_search_device': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p]),
     'bm25_device_status': (c_int, [c_void_p, POINTER(c_uint32)]),
     'bm25_close': (c_int, [c_void_p]),

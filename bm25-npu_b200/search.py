@@ -165,9 +165,13 @@ class Bm25Session:
             scores, ids = out
         if words.size == 0:
             words = np.zeros(1, dtype=np.int32)
-        status = self._lib.bm25_search(self._handle, n.ptr(offsets, c_int64), n.ptr(words, c_int32), q, k,
-                                       n.ptr(scores, c_float), n.ptr(ids, c_int32))
-        _raise(self._lib, status, self._handle)
+        if not (scores.flags.c_contiguous and ids.flags.c_contiguous and scores.dtype == np.float32
+                and ids.dtype == np.int32 and scores.size >= q * k and ids.size >= q * k):
+            raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'out must be C-contiguous float32 and int32 arrays of q*k')
+        status = self._lib.bm25_search(self._handle, offsets.ctypes.data, words.ctypes.data, q, k,
+                                       scores.ctypes.data, ids.ctypes.data)
+        if status:
+            _raise(self._lib, status, self._handle)
         return scores, ids
 
     def search_pruned(self, queries, k, tau):
