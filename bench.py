@@ -937,6 +937,7 @@ def main():
     ap.add_argument('--no-serve', action='store_true', help='skip the serving loop (Poisson arrivals)')
     ap.add_argument('--serve-all', action='store_true', help='serving loop at 5k, 10k, 20k and 50k queries/s')
     ap.add_argument('--serve-seconds', type=float, default=1.0)
+    ap.add_argument('--no-tune', action='store_true', help='keep the default runtime tuning (no autotune)')
     args = ap.parse_args()
     if args.impl == 'reference':
         return run_reference(args)
@@ -967,6 +968,19 @@ def main():
                                         prune=args.kernel in (4, 5) and not args.no_learned)
     info = session.info()
     log(f'engine ready in {time.perf_counter() - t:.1f}s: {info}')
+    tuning = None
+    if info['kernel'] == 5 and not args.no_tune:
+        # runtime knobs timed on a sample batch of the same shape (not one of the timed batches);
+        # every combination is bit-checked against the first, and the fastest is kept
+        t = time.perf_counter()
+        sample = pkg.synthetic_queries(index.offsets, Q, TERMS, TERMS, SEED_A + 77 + 1000 * rank)
+        best, table = pkg.autotune.tune(session, sample, K, space={'claim_tiles': (2, 4, 8),
+                                                                   'tail_claims': (1, 2, 4)}, reps=8)
+        tuning = {'chosen': {key: best[key] for key in ('claim_tiles', 'tail_claims')},
+                  'sample': f'one batch of {Q} x {TERMS} words (its own seed), 8 timed Searches per setting',
+                  'ms': {f"{c['claim_tiles']}x{c['tail_claims']}": round(ms, 4) for c, ms in table},
+                  'seconds': round(time.perf_counter() - t, 2)}
+        log(f'tuning: {tuning}')
 
     # Parity of both batches against the CPU oracle (outside every timer).
     parity = None
@@ -1110,6 +1124,8 @@ def main():
             'clocks': clock_info,
             'parity': parity,
         }
+        if tuning is not None:
+            line['tuning'] = tuning
         if learned is not None:
             line['learned_pruned'] = learned
         if mix is not None:

@@ -51,6 +51,18 @@ class Options(ctypes.Structure):
     ]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [
+        ('claim_tiles', c_int32),
+        ('tail_claims', c_int32),
+        ('ring_stages', c_int32),
+        ('ring_chunk', c_int32),
+        ('candidate_cap', c_int64),
+        ('prune_route', c_float),
+        ('reserved', c_int32),
+    ]
+
+
 class Info(ctypes.Structure):
     _fields_ = [
         ('num_docs', c_int64),
@@ -99,6 +111,8 @@ SIGNATURES = {
     'bm25_kernel_timing': (c_int, [c_void_p, c_int32]),
     'bm25_test_inject': (c_int, [c_void_p, c_int32]),
     'bm25_prepare_batch_graphs': (c_int, [c_void_p, c_int32, c_int32]),
+    'bm25_get_tuning': (c_int, [c_void_p, POINTER(Tuning)]),
+    'bm25_set_tuning': (c_int, [c_void_p, POINTER(Tuning)]),
     'bm25_kernel_times': (c_int, [c_void_p, POINTER(c_float), c_int64, POINTER(c_int64)]),
     'bm25_search_pruned_device': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p,
                                           c_void_p, c_void_p, c_void_p]),

@@ -1,12 +1,15 @@
-"""Autotuner for the tile-group engine: picks tile size, ring stage size and ring depth
-(and, for K > 32, the candidate capacity) by timing device-resident Searches of a sample
-batch on the caller's index and GPU.
+"""Autotuners: pick the engine's speed knobs by timing device-resident Searches of a
+sample batch on the caller's index and GPU.  A configuration changes speed, never
+results: every one is checked bit for bit against the first.
 
-Every configuration is a separate session over the same index (the index is uploaded
-once per configuration); each is timed with CUDA events on its launching stream over
-`reps` Searches after `warmup`, with the L2 flushed between Searches, and its results are
-checked bit for bit against the first configuration's -- a configuration changes speed,
-never results.
+tune() works on a live session (bm25_set_tuning: warp-tile claim sizes, tile-group ring
+shape, candidate capacity, learned routing cut) without re-uploading the index; this is
+what a server or the benchmark runs before it serves.  autotune() also chooses what is
+fixed when a session is created (tile size): every configuration is a separate session
+over the same index.
+
+Each configuration is timed with CUDA events on its launching stream over `reps`
+Searches after `warmup`, with the L2 flushed between Searches (a write of 256 MiB).
 """
 
 import itertools
@@ -31,27 +34,35 @@ def candidates(space=None, max_k=10):
     return [dict(zip(keys, values)) for values in itertools.product(*(space[k] for k in keys))]
 
 
-def _time(session, queries, k, reps, warmup, flush):
+def _time(session, queries, k, reps, warmup, flush, learned=False):
     import torch
     offsets, words = queries
     q = offsets.size - 1
-    dev = torch.device('cuda', torch.cuda.current_device())
+    dev = flush.device
     d_off = torch.from_numpy(np.ascontiguousarray(offsets, dtype=np.int64)).to(dev)
     d_w = torch.from_numpy(np.ascontiguousarray(words if len(words) else np.zeros(1), dtype=np.int32)).to(dev)
     d_s = torch.empty((q, k), dtype=torch.float32, device=dev)
     d_i = torch.empty((q, k), dtype=torch.int32, device=dev)
+    d_x = torch.empty(q, dtype=torch.int32, device=dev)
     stream = torch.cuda.Stream(dev)
+
+    def one():
+        if learned:
+            session.search_learned_device(d_off.data_ptr(), d_w.data_ptr(), q, k, d_s.data_ptr(), d_i.data_ptr(),
+                                          d_x.data_ptr(), stream.cuda_stream)
+        else:
+            session.search_device(d_off.data_ptr(), d_w.data_ptr(), q, k, d_s.data_ptr(), d_i.data_ptr(),
+                                  stream.cuda_stream)
+
     ms = []
     with torch.cuda.stream(stream):
         for _ in range(warmup):
-            session.search_device(d_off.data_ptr(), d_w.data_ptr(), q, k, d_s.data_ptr(), d_i.data_ptr(),
-                                  stream.cuda_stream)
+            one()
         for _ in range(reps):
             flush.zero_()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            session.search_device(d_off.data_ptr(), d_w.data_ptr(), q, k, d_s.data_ptr(), d_i.data_ptr(),
-                                  stream.cuda_stream)
+            one()
             b.record(stream)
             b.synchronize()
             ms.append(a.elapsed_time(b))
@@ -90,4 +101,54 @@ def autotune(indptr, indices, data, num_docs, queries, k, *, space=None, reps=20
     if not table:
         raise InvalidParam(0, 'no configuration of the search space could be created')
     best = min(table, key=lambda row: row[1])[0]
+    return best, table
+
+
+def tuning_space(session, k, learned=False):
+    """The runtime knobs that matter for this session's kernel and K (dict of value tuples)."""
+    info = session.info()
+    space = {}
+    if info['kernel'] == 5:  # warp tile
+        space['claim_tiles'] = (2, 4, 8)
+        space['tail_claims'] = (1, 2, 4)
+    if info['kernel'] in (4, 5):  # tile group (also the warp-tile sessions' K > 32 batches)
+        space['ring_stages'] = (2, 3, 4)
+        space['ring_chunk'] = (1024, 2048)
+    if info['max_k'] > 32:
+        space['candidate_cap'] = (0, max(info['max_k'], 64 * k))
+    if learned:
+        space['prune_route'] = (0.2, 0.3, 0.45)
+    return space
+
+
+def tune(session, queries, k, *, space=None, learned=False, reps=10, warmup=3, keep=True):
+    """Times every combination of `space` (default tuning_space) on a live session with the sample
+    batch `queries` (offsets, words) and K `k`, through search_device (search_learned_device when
+    `learned`); checks that every combination returns the first one's results bit for bit; sets the
+    fastest on the session when `keep` (else restores the tuning it had).
+
+    Returns (best tuning dict, table of (changes, median ms per Search))."""
+    import torch
+    if space is None:
+        space = tuning_space(session, k, learned)
+    keys = sorted(space)
+    combos = [dict(zip(keys, values)) for values in itertools.product(*(space[key] for key in keys))] or [{}]
+    start = session.tuning()
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=f'cuda:{torch.cuda.current_device()}')
+    offsets, words = (np.asarray(queries[0], np.int64), np.asarray(queries[1], np.int32))
+    table, ref = [], None
+    for changes in combos:
+        try:
+            session.set_tuning(**{**start, **changes})
+        except InvalidParam:
+            continue  # e.g. a ring too deep for one SM's shared memory
+        ms, scores, ids = _time(session, (offsets, words), k, reps, warmup, flush, learned)
+        if ref is None:
+            ref = (scores, ids)
+        elif not (np.array_equal(ids, ref[1]) and np.array_equal(scores.view(np.uint32), ref[0].view(np.uint32))):
+            session.set_tuning(**start)
+            raise RuntimeError(f'tuning {changes} changed the results')
+        table.append((changes, ms))
+    best = {**start, **min(table, key=lambda row: row[1])[0]} if table else start
+    session.set_tuning(**(best if keep else start))
     return best, table

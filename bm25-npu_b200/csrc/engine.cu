@@ -81,8 +81,21 @@ static bool TileFamily(int kernel) { return kernel == BM25_KERNEL_TILE_GROUP || 
 
 static_assert(bm25k::kTermTop == bm25k::kTermTopK, "one layout of the per-term top scores");
 
-// Tiles per claim of the warp-tile kernel.
+// Tiles per claim of the warp-tile kernel: the default, and the sizes a tuning may pick.
 constexpr int kWtClaimTiles = 4;
+
+// The warp-tile kernel with kC tiles per claim (2, 4 or 8).
+template <bool kLean> static void (*WarpTileFor(int claim_tiles))(const bm25k::StreamArgs)
+{
+    switch (claim_tiles) {
+    case 2:
+        return bm25k::WarpTileKernel<2, kLean>;
+    case 8:
+        return bm25k::WarpTileKernel<8, kLean>;
+    default:
+        return bm25k::WarpTileKernel<4, kLean>;
+    }
+}
 
 // Test hook: the next host-buffer Search of any session fails as a device error (bm25_test_inject
 // with no handle).
@@ -213,6 +226,7 @@ class Engine {
         }
         Cuda(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming), "cudaEventCreate");
         MakePlan();
+        tuning_.prune_route = o.prune_route;
     }
 
     ~Engine() { Release(); }
@@ -499,6 +513,67 @@ class Engine {
         } catch (...) {
             failed_ = true;
             throw;
+        }
+    }
+
+    // Runtime tuning (bm25_set_tuning): validated, applied to the launch parameters, and the
+    // instantiated graphs (which hold the old ones by value) dropped.
+    void GetTuning(bm25_tuning *t) const
+    {
+        *t = tuning_;
+        t->ring_stages = plan_.stages;
+        t->ring_chunk = plan_.chunk;
+    }
+    void SetTuning(const bm25_tuning &t)
+    {
+        RequireUsable();
+        Check(t.claim_tiles == 2 || t.claim_tiles == 4 || t.claim_tiles == 8, "claim_tiles must be 2, 4 or 8");
+        Check(t.tail_claims >= 0 && t.tail_claims <= 8, "tail_claims must be in [0, 8]");
+        Check(std::isfinite(t.prune_route), "prune_route must be finite");
+        const bool ring = TileFamily(plan_.kernel);
+        int stages = plan_.stages, chunk = plan_.chunk;
+        if (ring) {
+            Check(t.ring_stages >= 2 && t.ring_stages <= bm25k::kMaxStages, "ring_stages must be in [2, 8]");
+            Check(t.ring_chunk >= bm25k::kWgChunkMin && t.ring_chunk <= bm25k::kWgChunkMax && t.ring_chunk % 4 == 0,
+                  "ring_chunk must be a multiple of 4 in [512, 4096]");
+            stages = t.ring_stages;
+            chunk = t.ring_chunk;
+        }
+        long long cap = 0;
+        if (opts_.max_k > bm25k::kMaxSmallK && t.candidate_cap != 0) {
+            cap = (t.candidate_cap + 3) & ~3LL;
+            Check(cap >= opts_.max_k && cap <= cand_cap_, "candidate_cap must be in [max_k, candidate_capacity]");
+        }
+        Cuda(cudaSetDevice(device_), "cudaSetDevice");
+        size_t tg_smem = tg_smem_;
+        int tg_grid = tg_grid_;
+        if (ring && (stages != plan_.stages || chunk != plan_.chunk)) {
+            tg_smem = bm25k::TileGroupSmem(stages, chunk, plan_.tile_docs);
+            const void *kernel = bm25k::TileGroupKernelFor(plan_.tile_docs);
+            int per_sm = 0;
+            RaiseSmemCap(kernel, tg_smem);
+            RaiseSmemCap(bm25k::TileGroupKernelFor(plan_.tile_docs, true), tg_smem);
+            Cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, bm25k::kWgThreads, tg_smem),
+                 "occupancy");
+            Check(per_sm >= 1, "ring_stages x ring_chunk exceed the shared memory of one SM");
+            tg_grid = per_sm * sms_;
+        }
+        Cuda(cudaStreamWaitEvent(stream_, done_, 0), "cudaStreamWaitEvent");
+        Cuda(cudaStreamSynchronize(stream_), "tuning");
+        for (auto &g : graphs_)
+            cudaGraphExecDestroy(g.second.exec);
+        graphs_.clear();
+        tuning_ = t;
+        tuning_.candidate_cap = cap;
+        plan_.stages = stages;
+        plan_.chunk = chunk;
+        if (ring) {
+            tg_smem_ = tg_smem;
+            tg_grid_ = tg_grid;
+            if (plan_.kernel == BM25_KERNEL_TILE_GROUP) {
+                smem_bytes_ = tg_smem;
+                plan_.grid = tg_grid;
+            }
         }
     }
 
@@ -993,8 +1068,10 @@ class Engine {
                 per_tile = opts_.max_k;
                 if (plan_.kernel == BM25_KERNEL_WARP_TILE) {
                     smem_bytes_ = bm25k::WarpTileSmem();
-                    for (const bool lean : {true, false})
-                        RaiseSmemCap(bm25k::WarpTileKernelFor<kWtClaimTiles>(lean), smem_bytes_);
+                    for (const int c : {2, 4, 8}) {
+                        RaiseSmemCap(reinterpret_cast<const void *>(WarpTileFor<true>(c)), smem_bytes_);
+                        RaiseSmemCap(reinterpret_cast<const void *>(WarpTileFor<false>(c)), smem_bytes_);
+                    }
                     kernel = bm25k::WarpTileKernelFor<kWtClaimTiles>(false);
                     threads = bm25k::kWtThreads;
                 }
@@ -1151,7 +1228,11 @@ class Engine {
             sa.cand_count = cand_count_;
             sa.cand_scores = cand_scores_;
             sa.cand_ids = cand_ids_;
-            sa.cand_cap = cand_cap_;
+            // a tuned capacity (bm25_set_tuning) is a narrower stride over the same rows, for batches of
+            // one K > 32 only: a query of those that overflows it is searched again (a K <= 32 query's
+            // final select has no retry and counts on the allocated worst case)
+            sa.cand_cap = tuning_.candidate_cap > 0 && k > bm25k::kMaxSmallK && !kq ? tuning_.candidate_cap
+                                                                                    : cand_cap_;
             sa.ctrl = ctrl_;
             sa.stages = plan_.stages;
             sa.chunk = plan_.chunk;
@@ -1177,7 +1258,7 @@ class Engine {
             }
             // routing (pruned batches of 32 queries or more): the queries whose bounds keep too many
             // blocks are streamed by the tile-group kernel, the others scored block by block
-            const float route = opts_.prune_route == 0.0f ? 0.3f : opts_.prune_route;
+            const float route = tuning_.prune_route == 0.0f ? 0.3f : tuning_.prune_route;
             const bool routing = tau != nullptr && q >= 32 && route > 0.0f && route < 1.0f;
             if (routing) {
                 sa.qkept = d_qkept_;
@@ -1242,24 +1323,23 @@ class Engine {
             Cuda(cudaGetLastError(), "plan kernel launch");
             const long long claims = (long long)q * ((plan_.tiles + bm25k::kWgWarps - 1) / bm25k::kWgWarps);
             const int wg_grid = (int)std::max<long long>(1, std::min<long long>(tg_grid_, claims));
-            const long long wt_claims = (long long)q * ((plan_.tiles + kWtClaimTiles - 1) / kWtClaimTiles);
+            const int ct = tuning_.claim_tiles;
+            const long long wt_claims = (long long)q * ((plan_.tiles + ct - 1) / ct);
             const int wt_grid = (int)std::max<long long>(
                 1, std::min<long long>(plan_.grid, (wt_claims + bm25k::kWtWarps - 1) / bm25k::kWtWarps));
             {
-                // single-tile claims for the last tiles: about two per warp of the launch
-                const long long tail = (2LL * wt_grid * bm25k::kWtWarps + q - 1) / q;
-                sa.wt_bulk = (int)std::max<long long>(0, (plan_.tiles - tail) / kWtClaimTiles);
+                // single-tile claims for the last tiles: tail_claims per warp of the launch
+                const long long tail = ((long long)tuning_.tail_claims * wt_grid * bm25k::kWtWarps + q - 1) / q;
+                sa.wt_bulk = (int)std::max<long long>(0, (plan_.tiles - tail) / ct);
             }
             auto tile_group = [&](const bm25k::StreamArgs &args) {
                 const bool lean = !args.retry && !args.kq && k <= bm25k::kMaxSmallK;
                 if (warp_tile || (wt_session && args.retry)) {
                     if (!args.retry)  // right after the plan rows: set up while they are built
-                        LaunchOverlapped(lean ? bm25k::WarpTileKernel<kWtClaimTiles, true>
-                                              : bm25k::WarpTileKernel<kWtClaimTiles, false>,
-                                         wt_grid, bm25k::kWtThreads, smem_bytes_, s, args);
+                        LaunchOverlapped(lean ? WarpTileFor<true>(ct) : WarpTileFor<false>(ct), wt_grid,
+                                         bm25k::kWtThreads, smem_bytes_, s, args);
                     else
-                        bm25k::WarpTileKernel<kWtClaimTiles, false><<<wt_grid, bm25k::kWtThreads, smem_bytes_, s>>>(
-                            args);
+                        WarpTileFor<false>(ct)<<<wt_grid, bm25k::kWtThreads, smem_bytes_, s>>>(args);
                 } else if (plan_.tile_docs == 2048) {
                     if (lean)
                         bm25k::TileGroupKernel<2048, true><<<wg_grid, bm25k::kWgThreads, tg_smem_, s>>>(args);
@@ -1528,6 +1608,7 @@ class Engine {
     cudaEvent_t done_ = nullptr;
     size_t free_at_start_ = 0;
     Plan plan_;
+    bm25_tuning tuning_{kWtClaimTiles, 2, 0, 0, 0, 0.0f, 0};
     std::vector<void *> allocations_;
     int64_t device_bytes_ = 0, index_bytes_ = 0;
     int64_t *d_indptr_ = nullptr;
@@ -1975,6 +2056,36 @@ void bm25_destroy(bm25_handle *h)
         return;
     bm25_close(h);
     delete h;
+}
+
+int bm25_get_tuning(bm25_handle *h, bm25_tuning *t)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            bm25b200::Check(t != nullptr, "Null tuning");
+            h->engine->GetTuning(t);
+        },
+        h->error, h->code);
+}
+
+int bm25_set_tuning(bm25_handle *h, const bm25_tuning *t)
+{
+    if (!h)
+        return BM25_ERR_ILLEGAL_OPERATION;
+    std::lock_guard<std::mutex> guard(h->mutex);
+    return Invoke(
+        [&] {
+            if (!h->engine)
+                throw bm25b200::InvalidState("BM25 is not initialized");
+            bm25b200::Check(t != nullptr, "Null tuning");
+            h->engine->SetTuning(*t);
+        },
+        h->error, h->code);
 }
 
 int bm25_prepare_batch_graphs(bm25_handle *h, int32_t max_batch, int32_t learned)

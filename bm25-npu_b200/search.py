@@ -309,6 +309,22 @@ class Bm25Session:
         _raise(self._lib, self._lib.bm25_prepare_batch_graphs(self._handle, int(max_batch), int(bool(learned))),
                self._handle)
 
+    def tuning(self):
+        """The session's runtime tuning (bm25_get_tuning) as a dict."""
+        t = n.Tuning()
+        _raise(self._lib, self._lib.bm25_get_tuning(self._handle, ctypes.byref(t)), self._handle)
+        return {name: getattr(t, name) for name, _ in n.Tuning._fields_ if name != 'reserved'}
+
+    def set_tuning(self, **changes):
+        """Changes some runtime tuning fields (bm25_set_tuning): speed only, never results; the
+        session's instantiated graphs are dropped."""
+        t = self.tuning()
+        unknown = set(changes) - set(t)
+        if unknown:
+            raise InvalidParam(n.BM25_ERR_INVALID_PARAM, f'unknown tuning fields {sorted(unknown)}')
+        t.update(changes)
+        _raise(self._lib, self._lib.bm25_set_tuning(self._handle, ctypes.byref(n.Tuning(**t))), self._handle)
+
     def inject(self, what):
         """Test hook (bm25_test_inject): the next ``search`` fails as a device error, either on the host
         (BM25_INJECT_HOST_FAILURE) or by a stalled ring producer whose consumers' bounded waits run out

@@ -395,6 +395,33 @@ int bm25_build_index(const int64_t *doc_offsets, const int32_t *tokens, int64_t 
                      float *doc_norm, float *idf, int64_t *postings);
 int bm25_build_last_error(char *buffer, size_t length);
 
+/*
+ * Runtime tuning of a session (no counterpart in the reference): knobs that change speed,
+ * never results, settable on a live session without re-uploading the index (the
+ * autotuner, bm25-npu_b200/autotune.py, times them on a sample batch and keeps the
+ * fastest).  Setting them drops the session's instantiated graphs.
+ *   claim_tiles      warp-tile kernel: tiles per claim, 2, 4 or 8
+ *   tail_claims      warp-tile kernel: single-tile claims per warp at the end, 0..8
+ *   ring_stages      tile-group kernel: ring depth, 2..8
+ *   ring_chunk       tile-group kernel: postings per ring stage, a multiple of 4 in 512..4096
+ *                    (stages and chunk must fit one SM's shared memory)
+ *   candidate_cap    max_k > 32: candidates kept per query in a Search of one K > 32, from
+ *                    max_k up to the session's candidate_capacity (0 = all of it); rounded
+ *                    up to a multiple of 4; a query that overflows it is searched again
+ *   prune_route      as bm25_options.prune_route
+ */
+typedef struct bm25_tuning {
+    int32_t claim_tiles;
+    int32_t tail_claims;
+    int32_t ring_stages;
+    int32_t ring_chunk;
+    int64_t candidate_cap;
+    float prune_route;
+    int32_t reserved;
+} bm25_tuning;
+int bm25_get_tuning(bm25_handle *handle, bm25_tuning *tuning);
+int bm25_set_tuning(bm25_handle *handle, const bm25_tuning *tuning);
+
 /* Engine facts for reports and tests. */
 typedef struct bm25_info {
     int64_t num_docs, vocab, postings;
