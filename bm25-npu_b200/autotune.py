@@ -115,7 +115,7 @@ def tuning_space(session, k, learned=False):
         space['ring_stages'] = (2, 3, 4)
         space['ring_chunk'] = (1024, 2048)
     if info['max_k'] > 32:
-        space['candidate_cap'] = (0, max(info['max_k'], 64 * k))
+        space['candidate_cap'] = (0, max(2048, 8 * info['max_k'], 64 * k))
     if learned:
         space['prune_route'] = (0.2, 0.3, 0.45)
     return space

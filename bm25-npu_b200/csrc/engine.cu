@@ -541,8 +541,12 @@ class Engine {
         }
         long long cap = 0;
         if (opts_.max_k > bm25k::kMaxSmallK && t.candidate_cap != 0) {
+            // the retry passes start from a bound that may sit below the K-th score (the running bounds
+            // of concurrent warps), so the buffer keeps some slack over K: at least 8 max_k and 2048
             cap = (t.candidate_cap + 3) & ~3LL;
-            Check(cap >= opts_.max_k && cap <= cand_cap_, "candidate_cap must be in [max_k, candidate_capacity]");
+            const long long least = std::min<long long>(cand_cap_, std::max<long long>(2048, 8LL * opts_.max_k));
+            Check(cap >= least && cap <= cand_cap_,
+                  "candidate_cap must be in [max(2048, 8 max_k), candidate_capacity]");
         }
         Cuda(cudaSetDevice(device_), "cudaSetDevice");
         size_t tg_smem = tg_smem_;
@@ -1126,10 +1130,13 @@ class Engine {
             // Searches it hands to the tile-group kernel
             plan_entries_ = static_cast<bm25k::PlanEntry *>(Alloc(
                 std::max<size_t>(1, opts_.word_capacity) * tiles_z * sizeof(bm25k::PlanEntry), "cudaMalloc plan"));
-            if (plan_.kernel == BM25_KERNEL_WARP_TILE)
+            if (plan_.kernel == BM25_KERNEL_WARP_TILE) {
                 plan_rows_ = static_cast<int *>(Alloc(std::max<size_t>(1, opts_.word_capacity) * (tiles_z + 1) *
                                                           sizeof(int),
                                                       "cudaMalloc plan rows"));
+                word_rec_ = static_cast<int2 *>(
+                    Alloc(std::max<size_t>(1, opts_.word_capacity) * sizeof(int2), "cudaMalloc word records"));
+            }
             Cuda(cudaMemset(ctrl_, 0, sizeof(bm25k::StreamCtrl)), "cudaMemset");
             d_stats_ = static_cast<unsigned long long *>(Alloc(bm25k::kStats * sizeof(unsigned long long), "cudaMalloc stats"));
             Cuda(cudaMemset(d_stats_, 0, bm25k::kStats * sizeof(unsigned long long)), "cudaMemset");
@@ -1298,6 +1305,7 @@ class Engine {
             const bool wt_session = plan_.kernel == BM25_KERNEL_WARP_TILE;
             const bool warp_tile = wt_session && !tau && !kq && k <= bm25k::kMaxSmallK;
             sa.plan_rows = plan_rows_;
+            sa.word_rec = word_rec_;
             sa.prefetch = 1;
             sa.wait_budget = opts_.wait_budget_cycles;
             sa.term_top = plan_.kernel == BM25_KERNEL_WARP_TILE ? d_term_top_ : nullptr;
@@ -1640,6 +1648,7 @@ class Engine {
     long long cand_cap_ = 0;
     bm25k::PlanEntry *plan_entries_ = nullptr;
     int *plan_rows_ = nullptr;
+    int2 *word_rec_ = nullptr;  // warp-tile sessions: per query word (seed bits, dense row)
     float *d_dense_ = nullptr;  // dense rows of the most frequent terms (warp-tile kernel)
     float *d_term_rank_ = nullptr;  // [vocab][5] scores at ranks 64 .. 1024 (warp-tile kernel)
     int32_t *d_dense_row_ = nullptr;

@@ -147,10 +147,13 @@ struct StreamArgs {
     // a batch with a K per query (tile-group kernel): nullptr when every query takes a.k
     const int *kq;               // [Q] K of each query (a.k is their maximum)
     const long long *kout;       // [Q] first output slot of each query (packed rows)
-    // warp-tile kernel: [word][tiles + 1] first posting (relative to indptr[term]) of each tile for
-    // the query words without a directory row (PlanRowsKernel); prefetch != 0: each claim's posting
-    // runs are prefetched into L2 when the claim is taken
+    // warp-tile kernel, both written by PlanRowsKernel for every query word w of the Search:
+    // plan_rows [word][tiles + 1] the position in the posting arrays of the word's first posting in
+    // each tile (tiles + 1: the list's end), so a claim reads its bounds with one load per tile bound;
+    // word_rec [word] (starting-bound seed as float bits, dense row or -1).  prefetch != 0: each
+    // claim's posting runs are prefetched into L2 when the claim is taken
     int *plan_rows;
+    int2 *word_rec;
     int prefetch;
     // [vocab][32] each term's 32 largest posting scores (descending, 0 past its document
     // frequency): the warp-tile kernel starts a K <= 32 query's running bound at the largest K-th

@@ -102,43 +102,21 @@ __device__ __forceinline__ void PrefetchL2(const void *p, unsigned bytes)
 }
 
 // Posting positions of query word w at the bounds of the claim's tiles t0 .. t0 + nt (j > nt
-// repeats the last bound): off[j] = first posting of the word's list in tile t0 + j.  Words outside the vocabulary
-// have no postings (a negative one is flagged).
-// seed: raised to the word's k-th largest posting score (k <= 32 and term statistics present).
-// drow: the term's dense row, or -1.
+// repeats the last bound): off[j] = first posting of the word's list in tile t0 + j, from the word's
+// plan row; seed raised to the word's starting-bound seed, drow = its dense row or -1 (both from
+// its word record).  Both are written by PlanRowsKernel before this kernel reads them, so a claim
+// resolves its words with one round of independent loads.
 template <int kC>
-__device__ __forceinline__ void WtWordOffsets(const StreamArgs &a, long long w, int t0, int nt, int *off,
-                                              unsigned &bad, int k, float &seed, int &drow)
+__device__ __forceinline__ void WtWordRow(const StreamArgs &a, long long w, int t0, int nt, int *off, float &seed,
+                                          int &drow)
 {
-    const int term = __ldg(a.words + w);
-    drow = -1;
-    if (term < 0 || term >= a.vocab) {
-        if (term < 0)
-            bad |= kStatusBadWord;
+    const int *row = a.plan_rows + w * a.dir_stride + t0;
 #pragma unroll
-        for (int j = 0; j <= kC; ++j)
-            off[j] = 0;
-        return;
-    }
-    if (a.term_top && k <= kTermTopK)
-        seed = fmaxf(seed, __ldg(a.term_top + (long long)term * kTermTopK + (k - 1)));
-    else if (a.term_rank && k <= 1024)  // the score at the smallest rank 64 << j >= k: K documents reach it
-        seed = fmaxf(seed, __ldg(a.term_rank + (long long)term * 5 + (31 - __clz(k - 1)) - 5));
-    if (a.dense_row)
-        drow = __ldg(a.dense_row + term);
-    const int base = (int)__ldg(a.indptr + term);
-    const int r = a.dir_row ? __ldg(a.dir_row + term) : -1;
-    if (r >= 0) {
-        const int *row = a.dir + (long long)r * a.dir_stride;
-#pragma unroll
-        for (int j = 0; j <= kC; ++j)
-            off[j] = base + __ldg(row + t0 + min(j, nt));
-    } else {
-        const int *row = a.plan_rows + w * a.dir_stride;  // written by the kernel before this one
-#pragma unroll
-        for (int j = 0; j <= kC; ++j)
-            off[j] = base + __ldcg(row + t0 + min(j, nt));
-    }
+    for (int j = 0; j <= kC; ++j)
+        off[j] = __ldcg(row + min(j, nt));
+    const int2 r = __ldcg(a.word_rec + w);
+    seed = fmaxf(seed, __int_as_float(r.x));
+    drow = r.y;
 }
 
 // L2 prefetch of postings [lo, hi) of both arrays, widened to 16-byte boundaries (the arrays are
@@ -239,6 +217,7 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
     float *row = reinterpret_cast<float *>(wt_smem) + (size_t)warp * kWtTile;
     float4 *row4 = reinterpret_cast<float4 *>(row);
     WtShared &sh = *reinterpret_cast<WtShared *>(wt_smem + (size_t)kWtWarps * kWtTile * sizeof(float));
+    int *offB = &sh.offB[warp][0][0];  // [32][kWtMaxC + 1]
     WarpSel &ws = sh.wsel[warp];
 #pragma unroll
     for (int j = 0; j < kWtTile / 128; ++j)
@@ -285,34 +264,34 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
         float seed = 0.0f;
         int drowA = -1;
         if (lane < nw)
-            WtWordOffsets<kC>(a, qb + lane, t0, nt, offA, bad, k, seed, drowA);
+            WtWordRow<kC>(a, qb + lane, t0, nt, offA, seed, drowA);
         if (a.prefetch)
             PrefetchRun(a, offA[0], offA[kC], drowA, t0, nt);
         const unsigned denseA = __ballot_sync(kFull, drowA >= 0);
         unsigned denseB = 0;
         if (nw > 32) {  // uniform: words 32..63 go to shared memory
-            int offB[kC + 1];
+            int offR[kC + 1];
 #pragma unroll
             for (int j = 0; j <= kC; ++j)
-                offB[j] = 0;
+                offR[j] = 0;
             int drowB = -1;
             if (lane + 32 < nw)
-                WtWordOffsets<kC>(a, qb + lane + 32, t0, nt, offB, bad, k, seed, drowB);
+                WtWordRow<kC>(a, qb + lane + 32, t0, nt, offR, seed, drowB);
             if (a.prefetch)
-                PrefetchRun(a, offB[0], offB[kC], drowB, t0, nt);
+                PrefetchRun(a, offR[0], offR[kC], drowB, t0, nt);
 #pragma unroll
             for (int j = 0; j <= kC; ++j)
-                sh.offB[warp][lane][j] = offB[j];
+                offB[lane * (kWtMaxC + 1) + j] = offR[j];
             sh.drowB[warp][lane] = drowB;
             denseB = __ballot_sync(kFull, drowB >= 0);
             __syncwarp();
         }
-        // the largest K-th posting score of the query's words (0 for K > 32)
+        // the largest starting-bound seed of the query's words (0 without term statistics)
         seed = __uint_as_float(__reduce_max_sync(kFull, __float_as_uint(seed)));  // non-negative: bit order
         {
             unsigned posts = (unsigned)(offA[kC] - offA[0]);
             if (nw > 32)
-                posts += (unsigned)(sh.offB[warp][lane][kC] - sh.offB[warp][lane][0]);
+                posts += (unsigned)(offB[lane * (kWtMaxC + 1) + kC] - offB[lane * (kWtMaxC + 1)]);
             posts = __reduce_add_sync(kFull, posts);
             if (lane == 0) {
                 sh.counters[warp][0] += 1u;
@@ -374,8 +353,8 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
                     drow = __shfl_sync(kFull, drowA, s);
                     dense = (denseA >> s) & 1u;
                 } else {
-                    b = sh.offB[warp][s - 32][j];
-                    e = sh.offB[warp][s - 32][j + 1];
+                    b = offB[(s - 32) * (kWtMaxC + 1) + j];
+                    e = offB[(s - 32) * (kWtMaxC + 1) + j + 1];
                     drow = sh.drowB[warp][s - 32];
                     dense = (denseB >> (s - 32)) & 1u;
                 }
@@ -388,7 +367,7 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
             }
             bool any = lane < nw && offA[1] > offA[0];
             if (nw > 32)
-                any |= lane + 32 < nw && sh.offB[warp][lane][j + 1] > sh.offB[warp][lane][j];
+                any |= lane + 32 < nw && offB[lane * (kWtMaxC + 1) + j + 1] > offB[lane * (kWtMaxC + 1) + j];
             const bool W = __any_sync(kFull, any);
             __syncwarp();
             const float thr = fmaxf(fmaxf(seed, __uint_as_float(__shfl_sync(kFull, thr_bits, 0))),
@@ -433,15 +412,19 @@ inline const void *WarpTileKernelFor(bool lean)
                 : reinterpret_cast<const void *>(&WarpTileKernel<kC, false>);
 }
 
-// ---- plan rows of the words without a directory row -------------------------------------------
+// ---- plan rows and word records of a Search's query words ---------------------------------------
 //
-// rows[w][t] = (first posting of word w's list with document >= t * tile_docs) - indptr[term], for
-// t in [0, tiles] (the same values a directory row holds).  CTA (x, y) covers row entries
-// [y * kPlanRowChunk, (y + 1) * kPlanRowChunk) of words x, x + gridDim.x, ...; a word with a
-// directory row or outside the vocabulary is skipped (the search kernel does not read its plan row).
-// Two warps find the chunk's first and last posting (32-way searches), the chunk's postings mark
-// the entry of their tile when they are the first there, and a suffix minimum fills the entries of
-// the tiles without postings with the next marked one: O(postings + tiles) per word.
+// rows[w][t] = position of the first posting of word w's list with document >= t * tile_docs, for
+// t in [0, tiles] (indptr[term] plus the directory row's entry where the term has one); a word
+// outside the vocabulary gets an empty row (all 0), and a negative one is flagged.  CTA (x, y)
+// covers row entries [y * kPlanRowChunk, (y + 1) * kPlanRowChunk) of words x, x + gridDim.x, ...
+// A word with a directory row copies it; for the others two warps find the chunk's first and last
+// posting (32-way searches), the chunk's postings mark the entry of their tile when they are the
+// first there, and a suffix minimum fills the entries of the tiles without postings with the next
+// marked one: O(postings + tiles) per word.
+// The CTAs of chunk 0 also write each word's record: its dense row, and its seed -- the word's
+// posting score at rank K of its query (term_top for K <= 32, else the smallest stored rank 64,
+// 128, ..., 1024 not below K), which K documents reach (0 without term statistics).
 __global__ void __launch_bounds__(kPlanThreads) PlanRowsKernel(const StreamArgs a)
 {
     __shared__ int ent[kPlanRowChunk];
@@ -465,11 +448,47 @@ __global__ void __launch_bounds__(kPlanThreads) PlanRowsKernel(const StreamArgs 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (long long w = blockIdx.x; w < total; w += gridDim.x) {
         const int term = __ldg(a.words + w);
-        if (term < 0 || term >= a.vocab)
-            continue;  // flagged by the search kernel; it reads no row for it
-        if (a.dir_row && __ldg(a.dir_row + term) >= 0)
-            continue;  // read from the directory
+        int *out = a.plan_rows + w * a.dir_stride;
+        const bool known = term >= 0 && term < a.vocab;
+        if (blockIdx.y == 0 && tid == 0) {
+            float seed = 0.0f;
+            int drow = -1;
+            if (known) {
+                // the word's query: the last q with qoffsets[q] <= w (a malformed batch is flagged by
+                // the search kernel and fails as a whole)
+                int lo = 0, hi = a.q - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (__ldg(a.qoffsets + mid) <= w)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
+                }
+                const int k = QueryK(a, lo);
+                if (a.term_top && k <= kTermTopK)
+                    seed = __ldg(a.term_top + (long long)term * kTermTopK + (k - 1));
+                else if (a.term_rank && k <= 1024)
+                    seed = __ldg(a.term_rank + (long long)term * 5 + (31 - __clz(k - 1)) - 5);
+                if (a.dense_row)
+                    drow = __ldg(a.dense_row + term);
+            } else if (term < 0) {
+                atomicOr(a.status, kStatusBadWord);
+            }
+            a.word_rec[w] = make_int2(__float_as_int(seed), drow);
+        }
+        if (!known) {  // no postings
+            for (int t = e0 + tid; t < e1; t += kPlanThreads)
+                out[t] = 0;
+            continue;
+        }
         const long long s = __ldg(a.indptr + term), e = __ldg(a.indptr + term + 1);
+        const int r = a.dir_row ? __ldg(a.dir_row + term) : -1;
+        if (r >= 0) {  // the directory row, made absolute
+            const int *src = a.dir + (long long)r * a.dir_stride;
+            for (int t = e0 + tid; t < e1; t += kPlanThreads)
+                out[t] = (int)s + __ldg(src + t);
+            continue;
+        }
         if (warp < 2) {
             const long long target = (long long)(warp == 0 ? e0 : e1) * a.tile_docs;
             const long long p = WarpLowerBoundGlobal(a.indices, s, e, target, lane);
@@ -511,12 +530,11 @@ __global__ void __launch_bounds__(kPlanThreads) PlanRowsKernel(const StreamArgs 
         const int after = __shfl_down_sync(kFull, x, 1);
         if (lane < 31)
             carry = min(carry, after);
-        int *out = a.plan_rows + w * a.dir_stride;
 #pragma unroll
         for (int u = 0; u < kPer; ++u) {
             const int t = e0 + tid * kPer + u;
             if (t < e1)
-                out[t] = min(v[u], carry);
+                out[t] = (int)s + min(v[u], carry);
         }
         __syncthreads();  // ent, lim and wmin are rewritten for the next word
     }

@@ -58,6 +58,17 @@ def _raise(lib, status, handle):
     raise _ERRORS.get(status, Bm25Error)(status, message or f'BM25 status {status}', code)
 
 
+def _outputs(q, k, out):
+    """(scores [q, k] f32, ids [q, k] i32, exact [q] i32): new arrays, or `out` checked."""
+    if out is None:
+        return np.empty((q, k), dtype=np.float32), np.empty((q, k), dtype=np.int32), np.empty(q, dtype=np.int32)
+    scores, ids, exact = out
+    for a, dt, size in ((scores, np.float32, q * k), (ids, np.int32, q * k), (exact, np.int32, q)):
+        if not (a.flags.c_contiguous and a.dtype == dt and a.size >= size):
+            raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'out must be C-contiguous float32/int32 arrays of q*k, q*k, q')
+    return scores, ids, exact
+
+
 def pack_queries(queries):
     """List of word-id lists -> (offsets int64 [Q+1], words int32), common/bm25/search_inputs.h:23-42."""
     offsets = np.zeros(len(queries) + 1, dtype=np.int64)
@@ -188,15 +199,13 @@ class Bm25Session:
         tau = np.ascontiguousarray(tau, dtype=np.float32)
         if tau.shape != (q,):
             raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'tau must hold one bound per query')
-        scores = np.empty((q, k), dtype=np.float32)
-        ids = np.empty((q, k), dtype=np.int32)
-        exact = np.empty(q, dtype=np.int32)
+        scores, ids, exact = _outputs(q, k, None)
         if words.size == 0:
             words = np.zeros(1, dtype=np.int32)
-        status = self._lib.bm25_search_pruned(self._handle, n.ptr(offsets, c_int64), n.ptr(words, c_int32),
-                                              n.ptr(tau, c_float), q, k, n.ptr(scores, c_float),
-                                              n.ptr(ids, c_int32), n.ptr(exact, c_int32))
-        _raise(self._lib, status, self._handle)
+        status = self._lib.bm25_search_pruned(self._handle, offsets.ctypes.data, words.ctypes.data, tau.ctypes.data,
+                                              q, k, scores.ctypes.data, ids.ctypes.data, exact.ctypes.data)
+        if status:
+            _raise(self._lib, status, self._handle)
         return scores, ids, exact
 
     def search_pruned_device(self, qoffsets_ptr, words_ptr, tau_ptr, q, k, scores_ptr, ids_ptr, exact_ptr,
@@ -228,14 +237,16 @@ class Bm25Session:
             words = np.zeros(1, dtype=np.int32)
         if learned:
             exact = np.empty(q, dtype=np.int32)
-            status = self._lib.bm25_search_batch_learned(self._handle, n.ptr(offsets, c_int64), n.ptr(words, c_int32),
-                                                         n.ptr(ks, c_int32), q, n.ptr(scores, c_float),
-                                                         n.ptr(ids, c_int32), n.ptr(exact, c_int32))
-            _raise(self._lib, status, self._handle)
+            status = self._lib.bm25_search_batch_learned(self._handle, offsets.ctypes.data, words.ctypes.data,
+                                                         ks.ctypes.data, q, scores.ctypes.data, ids.ctypes.data,
+                                                         exact.ctypes.data)
+            if status:
+                _raise(self._lib, status, self._handle)
             return scores, ids, koff, exact
-        status = self._lib.bm25_search_batch(self._handle, n.ptr(offsets, c_int64), n.ptr(words, c_int32),
-                                             n.ptr(ks, c_int32), q, n.ptr(scores, c_float), n.ptr(ids, c_int32))
-        _raise(self._lib, status, self._handle)
+        status = self._lib.bm25_search_batch(self._handle, offsets.ctypes.data, words.ctypes.data, ks.ctypes.data,
+                                             q, scores.ctypes.data, ids.ctypes.data)
+        if status:
+            _raise(self._lib, status, self._handle)
         return scores, ids, koff
 
     def search_batch_device(self, qoffsets_ptr, words_ptr, ks_ptr, kout_ptr, q, kmax, scores_ptr, ids_ptr,
@@ -256,22 +267,22 @@ class Bm25Session:
             status = self._lib.bm25_set_threshold_model(self._handle, n.ptr(params, c_float), c_float(model.margin))
         _raise(self._lib, status, self._handle)
 
-    def search_learned(self, queries, k):
-        """Exact top-k with learned starting bounds; returns (scores, ids, exact) as search_pruned."""
+    def search_learned(self, queries, k, *, out=None):
+        """Exact top-k with learned starting bounds; returns (scores, ids, exact) as search_pruned.
+        out: optional (scores, ids, exact) arrays to write (C-contiguous, q*k, q*k and q)."""
         if isinstance(queries, tuple):
             offsets = np.ascontiguousarray(queries[0], dtype=np.int64)
             words = np.ascontiguousarray(queries[1], dtype=np.int32)
         else:
             offsets, words = pack_queries(queries)
         q = offsets.size - 1
-        scores = np.empty((q, k), dtype=np.float32)
-        ids = np.empty((q, k), dtype=np.int32)
-        exact = np.empty(q, dtype=np.int32)
+        scores, ids, exact = _outputs(q, k, out)
         if words.size == 0:
             words = np.zeros(1, dtype=np.int32)
-        status = self._lib.bm25_search_learned(self._handle, n.ptr(offsets, c_int64), n.ptr(words, c_int32), q, k,
-                                               n.ptr(scores, c_float), n.ptr(ids, c_int32), n.ptr(exact, c_int32))
-        _raise(self._lib, status, self._handle)
+        status = self._lib.bm25_search_learned(self._handle, offsets.ctypes.data, words.ctypes.data, q, k,
+                                               scores.ctypes.data, ids.ctypes.data, exact.ctypes.data)
+        if status:
+            _raise(self._lib, status, self._handle)
         return scores, ids, exact
 
     def search_learned_device(self, qoffsets_ptr, words_ptr, q, k, scores_ptr, ids_ptr, exact_ptr, stream_ptr=None):

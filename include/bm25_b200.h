@@ -406,8 +406,9 @@ int bm25_build_last_error(char *buffer, size_t length);
  *   ring_chunk       tile-group kernel: postings per ring stage, a multiple of 4 in 512..4096
  *                    (stages and chunk must fit one SM's shared memory)
  *   candidate_cap    max_k > 32: candidates kept per query in a Search of one K > 32, from
- *                    max_k up to the session's candidate_capacity (0 = all of it); rounded
- *                    up to a multiple of 4; a query that overflows it is searched again
+ *                    max(2048, 8 max_k) up to the session's candidate_capacity (0 = all of
+ *                    it); rounded up to a multiple of 4; a query that overflows it is
+ *                    searched again (ties beyond it are reported as with candidate_capacity)
  *   prune_route      as bm25_options.prune_route
  */
 typedef struct bm25_tuning {

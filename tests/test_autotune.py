@@ -57,7 +57,7 @@ def test_tuning_space_follows_the_kernel(pkg):
     assert set(space) == {'claim_tiles', 'tail_claims', 'ring_stages', 'ring_chunk'}
     space = pkg.autotune.tuning_space(_FakeSession(4, 1000), 100, learned=True)
     assert set(space) == {'ring_stages', 'ring_chunk', 'candidate_cap', 'prune_route'}
-    assert space['candidate_cap'] == (0, 6400)
+    assert space['candidate_cap'] == (0, 8000)
     assert pkg.autotune.tuning_space(_FakeSession(0, 10), 10) == {}
 
 
@@ -80,16 +80,17 @@ def test_set_tuning_checks_and_keeps_results(pkg, oracle_mod, cuda_ok):
                                   word_capacity=64, max_k=100) as s:
         start = s.tuning()
         assert start['claim_tiles'] == 4 and start['tail_claims'] == 2 and start['candidate_cap'] == 0
-        for bad in ({'claim_tiles': 3}, {'tail_claims': 9}, {'ring_stages': 1}, {'ring_chunk': 1000},
-                    {'candidate_cap': 50}, {'prune_route': float('nan')}):
+        for bad in ({'claim_tiles': 3}, {'tail_claims': 9}, {'ring_stages': 1}, {'ring_chunk': 1002},
+                    {'ring_chunk': 256}, {'candidate_cap': 50}, {'candidate_cap': 2044},
+                    {'prune_route': float('nan')}):
             with pytest.raises(pkg.InvalidParam):
                 s.set_tuning(**bad)
             assert s.tuning() == start, bad
         s.search_batch((qo, w), np.full(16, 10, np.int32))
         assert s.info()['graphs_cached'] >= 1
         for changes in ({'claim_tiles': 2, 'tail_claims': 0}, {'claim_tiles': 8, 'tail_claims': 4},
-                        {'ring_stages': 2, 'ring_chunk': 1024}, {'candidate_cap': 100},
-                        {'candidate_cap': 101}):
+                        {'ring_stages': 2, 'ring_chunk': 1024}, {'candidate_cap': 2048},
+                        {'candidate_cap': 2050}):
             s.set_tuning(**changes)
             assert s.info()['graphs_cached'] == 0
             got = s.tuning()
