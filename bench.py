@@ -483,6 +483,10 @@ def mix_leg(pkg, args, local, world, flush, stream, rank):
                      'val_fallback': model.report['val_fallback']}}
     steps = max(3, args.steps // 4)
     totals = [int(ks.sum()) for _, _, ks in batches]
+    sample_qo, sample_w = pkg.synthetic_queries(index.offsets, MIX_Q, lo, hi, 880077 + 1000 * rank)
+    sample_ks = np.random.default_rng(777 + 1000 * rank).choice(MIX_KS, MIX_Q).astype(np.int32)
+    out['tuning'] = route_tuning(pkg, session, model, (sample_qo, sample_w, sample_ks), kmax)
+    log(f"mix tuning: {out['tuning']}")
     for label, learned in (('plain', False), ('learned', True)):
         session.set_threshold_model(model if learned else None)
 
@@ -552,6 +556,24 @@ def oracle_packed(index, data, qo, w, ks, kset):
             ps[koff[i]:koff[i + 1]] = rs[j]
             pi[koff[i]:koff[i + 1]] = ri[j]
     return ps, pi
+
+
+ROUTE_CUTS = (0.3, 0.45, 0.6, 0.8, 1.0)
+
+
+def route_tuning(pkg, session, model, sample, kmax):
+    """The learned routing cut (share of a query's blocks kept above which the query is streamed;
+    1.0: none is), timed on a sample batch with a K per query (its own seed, not a timed batch),
+    every cut bit-checked against the first; the fastest is kept on the session."""
+    t = time.perf_counter()
+    session.set_threshold_model(model)
+    qo, w, ks = sample
+    best, table = pkg.autotune.tune(session, (qo, w), kmax, space={'prune_route': ROUTE_CUTS}, learned=True,
+                                    ks=ks, reps=5)
+    return {'chosen': {'prune_route': best['prune_route']}, 'ms': {str(c['prune_route']): round(ms, 4)
+                                                                   for c, ms in table},
+            'sample': f'one batch of {qo.size - 1} queries (its own seed), 5 timed Searches per cut',
+            'seconds': round(time.perf_counter() - t, 2)}
 
 
 def same_bits(got, want):
@@ -629,6 +651,10 @@ def blockmax_leg(pkg, args, local, world, flush, stream, rank):
                      'val_fallback': model.report['val_fallback']}}
     steps = n_batches  # one pass over the held-out set
     totals = [int(ks.sum()) for _, _, ks in batches]
+    sample_qo, sample_w = pkg.synthetic_queries(index.offsets, BLOCKMAX_Q, lo, hi, 420077 + 1000 * rank)
+    sample_ks = np.random.default_rng(477 + 1000 * rank).choice(BLOCKMAX_KS, BLOCKMAX_Q).astype(np.int32)
+    out['tuning'] = route_tuning(pkg, session, model, (sample_qo, sample_w, sample_ks), kmax)
+    log(f"block-max tuning: {out['tuning']}")
     for label, learned in (('plain', False), ('learned', True)):
         session.set_threshold_model(model if learned else None)
 

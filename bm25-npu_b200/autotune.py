@@ -34,20 +34,32 @@ def candidates(space=None, max_k=10):
     return [dict(zip(keys, values)) for values in itertools.product(*(space[k] for k in keys))]
 
 
-def _time(session, queries, k, reps, warmup, flush, learned=False):
+def _time(session, queries, k, reps, warmup, flush, learned=False, ks=None):
+    """Median ms of a device Search of `queries` with K k, or (ks given: a K per query, k their
+    largest) of a batch Search; returns (ms, scores, ids)."""
     import torch
     offsets, words = queries
     q = offsets.size - 1
     dev = flush.device
     d_off = torch.from_numpy(np.ascontiguousarray(offsets, dtype=np.int64)).to(dev)
     d_w = torch.from_numpy(np.ascontiguousarray(words if len(words) else np.zeros(1), dtype=np.int32)).to(dev)
-    d_s = torch.empty((q, k), dtype=torch.float32, device=dev)
-    d_i = torch.empty((q, k), dtype=torch.int32, device=dev)
+    rows = q * k if ks is None else int(np.sum(ks))
+    d_s = torch.empty(rows, dtype=torch.float32, device=dev)
+    d_i = torch.empty(rows, dtype=torch.int32, device=dev)
     d_x = torch.empty(q, dtype=torch.int32, device=dev)
+    if ks is not None:
+        d_ks = torch.from_numpy(np.ascontiguousarray(ks, dtype=np.int32)).to(dev)
+        kout = np.zeros(q, dtype=np.int64)
+        np.cumsum(ks[:-1], out=kout[1:])
+        d_kout = torch.from_numpy(kout).to(dev)
     stream = torch.cuda.Stream(dev)
 
     def one():
-        if learned:
+        if ks is not None:
+            session.search_batch_device(d_off.data_ptr(), d_w.data_ptr(), d_ks.data_ptr(), d_kout.data_ptr(), q, k,
+                                        d_s.data_ptr(), d_i.data_ptr(), d_x.data_ptr() if learned else None,
+                                        learned=learned, stream_ptr=stream.cuda_stream)
+        elif learned:
             session.search_learned_device(d_off.data_ptr(), d_w.data_ptr(), q, k, d_s.data_ptr(), d_i.data_ptr(),
                                           d_x.data_ptr(), stream.cuda_stream)
         else:
@@ -117,15 +129,16 @@ def tuning_space(session, k, learned=False):
     if info['max_k'] > 32:
         space['candidate_cap'] = (0, max(2048, 8 * info['max_k'], 64 * k))
     if learned:
-        space['prune_route'] = (0.2, 0.3, 0.45)
+        space['prune_route'] = (0.3, 0.6, 1.0)
     return space
 
 
-def tune(session, queries, k, *, space=None, learned=False, reps=10, warmup=3, keep=True):
+def tune(session, queries, k, *, space=None, learned=False, ks=None, reps=10, warmup=3, keep=True):
     """Times every combination of `space` (default tuning_space) on a live session with the sample
     batch `queries` (offsets, words) and K `k`, through search_device (search_learned_device when
-    `learned`); checks that every combination returns the first one's results bit for bit; sets the
-    fastest on the session when `keep` (else restores the tuning it had).
+    `learned`; search_batch_device when `ks` gives a K per query, k their largest); checks that every
+    combination returns the first one's results bit for bit; sets the fastest on the session when
+    `keep` (else restores the tuning it had).
 
     Returns (best tuning dict, table of (changes, median ms per Search))."""
     import torch
@@ -142,7 +155,7 @@ def tune(session, queries, k, *, space=None, learned=False, reps=10, warmup=3, k
             session.set_tuning(**{**start, **changes})
         except InvalidParam:
             continue  # e.g. a ring too deep for one SM's shared memory
-        ms, scores, ids = _time(session, (offsets, words), k, reps, warmup, flush, learned)
+        ms, scores, ids = _time(session, (offsets, words), k, reps, warmup, flush, learned, ks)
         if ref is None:
             ref = (scores, ids)
         elif not (np.array_equal(ids, ref[1]) and np.array_equal(scores.view(np.uint32), ref[0].view(np.uint32))):

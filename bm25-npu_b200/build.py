@@ -21,6 +21,7 @@ ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
 ENGINE_SOURCES = ['engine.cu', 'mlp.cu', 'serve.cpp', 'builder.cu']
 ENGINE_HEADERS = ['tile_kernels.cuh', 'stream_kernel.cuh', 'tile_group_kernel.cuh', 'warp_tile_kernel.cuh', 'block_kernels.cuh',
+                  'block_tile_kernel.cuh',
                   'learned_kernels.cuh', 'mlp.cuh', 'merge_kernel.cuh']
 
 

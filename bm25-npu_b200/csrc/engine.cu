@@ -10,6 +10,7 @@
 // D2H.  Search = validate + pack, graph replay, synchronise, validate result.
 #include "bm25_b200.h"
 #include "block_kernels.cuh"
+#include "block_tile_kernel.cuh"
 #include "learned_kernels.cuh"
 #include "merge_kernel.cuh"
 #include "stream_kernel.cuh"
@@ -1076,6 +1077,7 @@ class Engine {
                         RaiseSmemCap(reinterpret_cast<const void *>(WarpTileFor<true>(c)), smem_bytes_);
                         RaiseSmemCap(reinterpret_cast<const void *>(WarpTileFor<false>(c)), smem_bytes_);
                     }
+                    RaiseSmemCap(reinterpret_cast<const void *>(&bm25k::BlockTileKernel), smem_bytes_);
                     kernel = bm25k::WarpTileKernelFor<kWtClaimTiles>(false);
                     threads = bm25k::kWtThreads;
                 }
@@ -1265,7 +1267,9 @@ class Engine {
             }
             // routing (pruned batches of 32 queries or more): the queries whose bounds keep too many
             // blocks are streamed by the tile-group kernel, the others scored block by block
-            const float route = tuning_.prune_route == 0.0f ? 0.3f : tuning_.prune_route;
+            const float route = tuning_.prune_route != 0.0f ? tuning_.prune_route
+                                : plan_.kernel == BM25_KERNEL_WARP_TILE ? 1.0f
+                                                                        : 0.3f;
             const bool routing = tau != nullptr && q >= 32 && route > 0.0f && route < 1.0f;
             if (routing) {
                 sa.qkept = d_qkept_;
@@ -1361,6 +1365,16 @@ class Engine {
                         bm25k::TileGroupKernel<1024><<<wg_grid, bm25k::kWgThreads, tg_smem_, s>>>(args);
                 }
             };
+            // the kept blocks of a pruned pass: the warp-tile style scorer in a warp-tile session
+            // (1024-document tiles, its counter and shared memory), else the staging block scorer
+            auto block_score = [&](const bm25k::StreamArgs &args) {
+                if (wt_session)
+                    LaunchOverlapped(bm25k::BlockTileKernel, plan_.grid, bm25k::kWtThreads, smem_bytes_, s, args);
+                else if (plan_.tile_docs == 2048)
+                    LaunchOverlapped(bm25k::BlockScoreKernel<2048>, bs_grid_, bm25k::kBsThreads, bs_smem_, s, args);
+                else
+                    LaunchOverlapped(bm25k::BlockScoreKernel<1024>, bs_grid_, bm25k::kBsThreads, bs_smem_, s, args);
+            };
             auto final_select = [&](const bm25k::StreamArgs &args) {
                 if (k <= bm25k::kMaxSmallK || kq)
                     LaunchOverlapped(bm25k::FinalSelectKernel, q, bm25k::kFinalThreads, 0, s, args);
@@ -1380,10 +1394,7 @@ class Engine {
                     Cuda(cudaGetLastError(), "route kernel launch");
                 }
                 MarkKernel(0, s);
-                if (plan_.tile_docs == 2048)
-                    LaunchOverlapped(bm25k::BlockScoreKernel<2048>, bs_grid_, bm25k::kBsThreads, bs_smem_, s, sa);
-                else
-                    LaunchOverlapped(bm25k::BlockScoreKernel<1024>, bs_grid_, bm25k::kBsThreads, bs_smem_, s, sa);
+                block_score(sa);
                 Cuda(cudaGetLastError(), "block score kernel launch");
                 MarkKernel(1, s);
                 if (routing) {  // the routed queries, streamed from their starting bound
@@ -1427,13 +1438,11 @@ class Engine {
                     ra.item_count = d_item_count_ + 2;
                     ra.safe = learned ? d_safe_ : nullptr;
                     const dim3 bgrid((plan_.tiles + bm25k::kBbThreads - 1) / bm25k::kBbThreads, q);
-                    if (plan_.tile_docs == 2048) {
+                    if (plan_.tile_docs == 2048)
                         LaunchOverlapped(bm25k::BlockBoundKernel<2048>, bgrid, bm25k::kBbThreads, 0, s, ra);
-                        LaunchOverlapped(bm25k::BlockScoreKernel<2048>, bs_grid_, bm25k::kBsThreads, bs_smem_, s, ra);
-                    } else {
+                    else
                         LaunchOverlapped(bm25k::BlockBoundKernel<1024>, bgrid, bm25k::kBbThreads, 0, s, ra);
-                        LaunchOverlapped(bm25k::BlockScoreKernel<1024>, bs_grid_, bm25k::kBsThreads, bs_smem_, s, ra);
-                    }
+                    block_score(ra);
                 } else {
                     ra.items = nullptr;
                     ra.wrow = nullptr;

@@ -59,8 +59,10 @@ typedef struct bm25_options {
                                    A Search whose K-th score is tied by more documents than this overflows
                                    every retry pass and fails with BM25_ERR_INNER_ERROR (device status 32) */
     float prune_route;       /* pruned Searches of 32 queries or more: a query keeping more than this share of
-                                its 128-document blocks is streamed by the tile-group kernel instead
-                                (0 = 0.3; negative = never) */
+                                its 128-document blocks is streamed instead of block-scored (0 = the
+                                kernel's default: never for the warp-tile kernel, whose block scorer reads
+                                each word's run of kept blocks at the streaming rate; 0.3 for the others;
+                                negative or >= 1 = never) */
     int64_t wait_budget_cycles; /* SM clock cycles a bounded wait of the ring kernels (0 and 4) spends
                                    before it gives up and the Search reports a device error
                                    (0 = 4e9, about 2 s) */
