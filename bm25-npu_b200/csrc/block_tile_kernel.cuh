@@ -9,9 +9,10 @@
 //     [first posting of the first kept block, end of the last kept block) -- the postings
 //     of dropped blocks between two kept ones are read as well (one contiguous run per
 //     word, no per-block bookkeeping);
-//   * the first window (128 postings) of each of the first kWtLead words is loaded at once
-//     straight into registers, the rest two windows at a time, and added word by word
-//     (query-word order, a __syncwarp between words) into the warp's private FP32 row;
+//   * the words go in groups of kWtLead: the first window (128 postings) of every word of a
+//     group is loaded at once straight into registers, the rest two windows at a time, and
+//     the group's words are added one by one (query-word order, a __syncwarp between words)
+//     into the warp's private FP32 row, so an item waits for memory about once per group;
 //   * the kept blocks are selected against the query's running bound (TileSelectAppend
 //     with the mask) and the row is cleared.
 // A document of a dropped block holds at most a partial sum, below its block's bound and so
@@ -103,35 +104,34 @@ __global__ void __launch_bounds__(kWtThreads, 3) BlockTileKernel(const StreamArg
                 BtWordRange(a, qb + s0 + lane, t, mask, lo, hi);
             any |= hi > lo;
             read += (unsigned long long)max(0, hi - lo);
-            int lid[kWtLead][4];
-            float lval[kWtLead][4];
+            // words in groups of kWtLead: the first window of every word of a group is loaded at once,
+            // then the group's words are added in query order
+            for (int g = 0; g < nw; g += kWtLead) {  // uniform
+                int lid[kWtLead][4];
+                float lval[kWtLead][4];
 #pragma unroll
-            for (int s = 0; s < kWtLead; ++s) {
-                const int b = __shfl_sync(kFull, lo, s), e = __shfl_sync(kFull, hi, s);
+                for (int u = 0; u < kWtLead; ++u) {
+                    const int b = __shfl_sync(kFull, lo, g + u), e = __shfl_sync(kFull, hi, g + u);
 #pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    const int p = b + lane + 32 * v;
-                    lid[s][v] = -1;
-                    lval[s][v] = 0.0f;
-                    if (s < nw && p < e) {
-                        lid[s][v] = LdStreamI32(a.indices + p);
-                        lval[s][v] = LdStreamF32(a.data + p);
+                    for (int v = 0; v < 4; ++v) {
+                        const int p = b + lane + 32 * v;
+                        lid[u][v] = -1;
+                        lval[u][v] = 0.0f;
+                        if (g + u < nw && p < e) {
+                            lid[u][v] = LdStreamI32(a.indices + p);
+                            lval[u][v] = LdStreamF32(a.data + p);
+                        }
                     }
                 }
-            }
 #pragma unroll
-            for (int s = 0; s < kWtLead; ++s) {
-                if (s >= nw)
-                    break;  // uniform
-                __syncwarp();  // the previous word's adds are in the row before this word's
-                const int b = __shfl_sync(kFull, lo, s), e = __shfl_sync(kFull, hi, s);
-                WtScatter(lid[s], lval[s], base_doc, row, rmax, bad);
-                WtWordWindows(a, b + kWtWindow, e, base_doc, row, lane, rmax, bad);
-            }
-            for (int s = kWtLead; s < nw; ++s) {
-                __syncwarp();
-                const int b = __shfl_sync(kFull, lo, s), e = __shfl_sync(kFull, hi, s);
-                WtWordWindows(a, b, e, base_doc, row, lane, rmax, bad);
+                for (int u = 0; u < kWtLead; ++u) {
+                    if (g + u >= nw)
+                        break;  // uniform
+                    __syncwarp();  // the previous word's adds are in the row before this word's
+                    const int b = __shfl_sync(kFull, lo, g + u), e = __shfl_sync(kFull, hi, g + u);
+                    WtScatter(lid[u], lval[u], base_doc, row, rmax, bad);
+                    WtWordWindows(a, b + kWtWindow, e, base_doc, row, lane, rmax, bad);
+                }
             }
         }
         __syncwarp();
