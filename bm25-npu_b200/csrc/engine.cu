@@ -1308,6 +1308,11 @@ class Engine {
             // append far more candidates); both take the (query word, tile) plan.
             const bool wt_session = plan_.kernel == BM25_KERNEL_WARP_TILE;
             const bool warp_tile = wt_session && !tau && !kq && k <= bm25k::kMaxSmallK;
+            // the streaming passes after a first pass (retries, routed queries) run the warp-tile kernel
+            // too, on plan rows built beside the plan -- except in a pruned Search that routes nothing:
+            // there only the few queries of the retry lists stream, and the tile-group kernel takes
+            // them from the plan alone, so the plan rows are not built
+            const bool wt_streams = wt_session && (tau == nullptr || routing);
             sa.plan_rows = plan_rows_;
             sa.word_rec = word_rec_;
             sa.prefetch = 1;
@@ -1328,7 +1333,7 @@ class Engine {
                 else
                     bm25k::PlanKernel<<<bm25k::PlanGrid(opts_.word_capacity, plan_.tiles, sms_), bm25k::kPlanThreads,
                                         0, s>>>(sa);
-                if (wt_session)  // for the streaming passes; set up while the plan kernel runs
+                if (wt_streams)  // for the streaming passes; set up while the plan kernel runs
                     LaunchOverlapped(bm25k::PlanRowsKernel, bm25k::PlanRowsGrid(opts_.word_capacity, plan_.tiles, sms_),
                                      bm25k::kPlanThreads, 0, s, sa);
             }
@@ -1346,7 +1351,7 @@ class Engine {
             }
             auto tile_group = [&](const bm25k::StreamArgs &args) {
                 const bool lean = !args.retry && !args.kq && k <= bm25k::kMaxSmallK;
-                if (warp_tile || (wt_session && args.retry)) {
+                if (warp_tile || (wt_streams && args.retry)) {
                     if (!args.retry)  // right after the plan rows: set up while they are built
                         LaunchOverlapped(lean ? WarpTileFor<true>(ct) : WarpTileFor<false>(ct), wt_grid,
                                          bm25k::kWtThreads, smem_bytes_, s, args);
