@@ -119,8 +119,15 @@ __global__ void __launch_bounds__(kBbThreads) BlockBoundKernel(const StreamArgs 
                 r[u] = -2;
                 pe[u] = PlanEntry{0, 0};
                 if (s0 + u < n) {
-                    r[u] = __ldcg(a.wrow + qb + s0 + u);  // written by PlanKernel
-                    pe[u] = a.plan[(qb + s0 + u) * a.tiles + t];
+                    const long long w = qb + s0 + u;
+                    if (a.rows_plan) {  // written by PlanRowsKernel
+                        const int *row = a.plan_rows + w * a.dir_stride + t;
+                        r[u] = __ldcg(&a.word_rec[w].z);
+                        pe[u] = PlanEntry{__ldcg(row), __ldcg(row + 1)};
+                    } else {  // written by PlanKernel
+                        r[u] = __ldcg(a.wrow + w);
+                        pe[u] = a.plan[w * a.tiles + t];
+                    }
                 }
             }
             float m[kPf][kNb];

@@ -32,10 +32,18 @@ namespace bm25k {
 // [lo, hi).  A word outside the vocabulary has an empty plan entry.
 __device__ __forceinline__ void BtWordRange(const StreamArgs &a, long long w, int t, unsigned mask, int &lo, int &hi)
 {
-    const PlanEntry pe = a.plan[w * a.tiles + t];
-    const int r = __ldcg(a.wrow + w);  // written by PlanKernel; -1 short list, -2 not a term
-    lo = (int)pe.b;
-    hi = (int)pe.e;
+    int r;  // -1 short list, -2 not a term
+    if (a.rows_plan) {  // written by PlanRowsKernel
+        const int *row = a.plan_rows + w * a.dir_stride + t;
+        lo = __ldcg(row);
+        hi = __ldcg(row + 1);
+        r = __ldcg(&a.word_rec[w].z);
+    } else {  // written by PlanKernel
+        const PlanEntry pe = a.plan[w * a.tiles + t];
+        lo = (int)pe.b;
+        hi = (int)pe.e;
+        r = __ldcg(a.wrow + w);
+    }
     if (r >= 0 && lo < hi) {
         const uint4 o = __ldg(reinterpret_cast<const uint4 *>(a.boff + ((long long)r * a.tiles + t) * 8));
         const unsigned off[4] = {o.x, o.y, o.z, o.w};

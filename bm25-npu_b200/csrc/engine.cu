@@ -1136,8 +1136,8 @@ class Engine {
                 plan_rows_ = static_cast<int *>(Alloc(std::max<size_t>(1, opts_.word_capacity) * (tiles_z + 1) *
                                                           sizeof(int),
                                                       "cudaMalloc plan rows"));
-                word_rec_ = static_cast<int2 *>(
-                    Alloc(std::max<size_t>(1, opts_.word_capacity) * sizeof(int2), "cudaMalloc word records"));
+                word_rec_ = static_cast<int4 *>(
+                    Alloc(std::max<size_t>(1, opts_.word_capacity) * sizeof(int4), "cudaMalloc word records"));
             }
             Cuda(cudaMemset(ctrl_, 0, sizeof(bm25k::StreamCtrl)), "cudaMemset");
             d_stats_ = static_cast<unsigned long long *>(Alloc(bm25k::kStats * sizeof(unsigned long long), "cudaMalloc stats"));
@@ -1309,10 +1309,11 @@ class Engine {
             const bool wt_session = plan_.kernel == BM25_KERNEL_WARP_TILE;
             const bool warp_tile = wt_session && !tau && !kq && k <= bm25k::kMaxSmallK;
             // the streaming passes after a first pass (retries, routed queries) run the warp-tile kernel
-            // too, on plan rows built beside the plan -- except in a pruned Search that routes nothing:
-            // there only the few queries of the retry lists stream, and the tile-group kernel takes
-            // them from the plan alone, so the plan rows are not built
-            const bool wt_streams = wt_session && (tau == nullptr || routing);
+            // too, on the plan rows; a pruned Search of a warp-tile session takes its block path's
+            // ranges from the plan rows as well and builds no (query word, tile) plan
+            const bool wt_streams = wt_session;
+            const bool rows_only = wt_session && tau != nullptr;
+            sa.rows_plan = rows_only ? 1 : 0;
             sa.plan_rows = plan_rows_;
             sa.word_rec = word_rec_;
             sa.prefetch = 1;
@@ -1326,6 +1327,10 @@ class Engine {
             if (warp_tile) {
                 bm25k::PlanRowsKernel<<<bm25k::PlanRowsGrid(opts_.word_capacity, plan_.tiles, sms_),
                                         bm25k::kPlanThreads, 0, s>>>(sa);
+            } else if (rows_only) {
+                // after the learned bounds kernel: set up while it runs (it writes nothing the rows read)
+                LaunchOverlapped(bm25k::PlanRowsKernel, bm25k::PlanRowsGrid(opts_.word_capacity, plan_.tiles, sms_),
+                                 bm25k::kPlanThreads, 0, s, sa);
             } else {
                 if (learned)
                     LaunchOverlapped(bm25k::PlanKernel, bm25k::PlanGrid(opts_.word_capacity, plan_.tiles, sms_),
@@ -1662,7 +1667,7 @@ class Engine {
     long long cand_cap_ = 0;
     bm25k::PlanEntry *plan_entries_ = nullptr;
     int *plan_rows_ = nullptr;
-    int2 *word_rec_ = nullptr;  // warp-tile sessions: per query word (seed bits, dense row)
+    int4 *word_rec_ = nullptr;  // warp-tile sessions: per query word (seed bits, dense row, directory row)
     float *d_dense_ = nullptr;  // dense rows of the most frequent terms (warp-tile kernel)
     float *d_term_rank_ = nullptr;  // [vocab][5] scores at ranks 64 .. 1024 (warp-tile kernel)
     int32_t *d_dense_row_ = nullptr;

@@ -150,10 +150,14 @@ struct StreamArgs {
     // warp-tile kernel, both written by PlanRowsKernel for every query word w of the Search:
     // plan_rows [word][tiles + 1] the position in the posting arrays of the word's first posting in
     // each tile (tiles + 1: the list's end), so a claim reads its bounds with one load per tile bound;
-    // word_rec [word] (starting-bound seed as float bits, dense row or -1).  prefetch != 0: each
-    // claim's posting runs are prefetched into L2 when the claim is taken
+    // word_rec [word] (starting-bound seed as float bits, dense row or -1, directory row: -1 a
+    // short list, -2 not a term, 0).  prefetch != 0: each claim's posting runs are prefetched into
+    // L2 when the claim is taken.  rows_plan != 0: the block path (BlockBoundKernel, BlockTileKernel)
+    // takes a word's range in a tile from its plan row and its directory row from its record, and
+    // PlanKernel does not run (a warp-tile session's pruned Search)
     int *plan_rows;
-    int2 *word_rec;
+    int4 *word_rec;
+    int rows_plan;
     int prefetch;
     // [vocab][32] each term's 32 largest posting scores (descending, 0 past its document
     // frequency): the warp-tile kernel starts a K <= 32 query's running bound at the largest K-th

@@ -12,8 +12,9 @@
 //     not end waiting on a few warps with long claims of a dense query;
 //   * the warp resolves the claim itself: lane s holds query word s's posting
 //     position at each of the claim's kC + 1 tile bounds, read from the word's
-//     directory row (long lists, built at create) or from its plan row (short
-//     lists, PlanRowsKernel), and issues one L2 prefetch per word for the
+//     plan row (PlanRowsKernel: the directory row made absolute for a long list,
+//     built from the postings for a short one) with its word record (seed, dense
+//     row) in one round of loads, and issues one L2 prefetch per word for the
 //     postings of all kC tiles (cp.async.bulk.prefetch.L2: no shared memory, no
 //     registers held while the bytes are in flight);
 //   * per tile the warp loads its postings straight from global memory into
@@ -114,7 +115,7 @@ __device__ __forceinline__ void WtWordRow(const StreamArgs &a, long long w, int 
 #pragma unroll
     for (int j = 0; j <= kC; ++j)
         off[j] = __ldcg(row + min(j, nt));
-    const int2 r = __ldcg(a.word_rec + w);
+    const int4 r = __ldcg(a.word_rec + w);
     seed = fmaxf(seed, __int_as_float(r.x));
     drow = r.y;
 }
@@ -422,9 +423,11 @@ inline const void *WarpTileKernelFor(bool lean)
 // posting (32-way searches), the chunk's postings mark the entry of their tile when they are the
 // first there, and a suffix minimum fills the entries of the tiles without postings with the next
 // marked one: O(postings + tiles) per word.
-// The CTAs of chunk 0 also write each word's record: its dense row, and its seed -- the word's
-// posting score at rank K of its query (term_top for K <= 32, else the smallest stored rank 64,
-// 128, ..., 1024 not below K), which K documents reach (0 without term statistics).
+// The CTAs of chunk 0 also write each word's record: its seed -- the word's posting score at rank
+// K of its query (term_top for K <= 32, else the smallest stored rank 64, 128, ..., 1024 not
+// below K), which K documents reach (0 without term statistics) --, its dense row, and its
+// directory row (-1: a short list; -2: not a term).  One CTA also empties the block path's work
+// lists of the Search (when it has them), as PlanKernel does where it runs.
 __global__ void __launch_bounds__(kPlanThreads) PlanRowsKernel(const StreamArgs a)
 {
     __shared__ int ent[kPlanRowChunk];
@@ -433,6 +436,8 @@ __global__ void __launch_bounds__(kPlanThreads) PlanRowsKernel(const StreamArgs 
     constexpr int kPer = kPlanRowChunk / kPlanThreads;
     static_assert(kPlanRowChunk % kPlanThreads == 0, "whole entries per thread");
     AllowDependents();  // the search kernel sets up its shared memory meanwhile
+    if (a.rows_plan && a.item_count && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < 4)
+        a.item_count[threadIdx.x] = 0u;
     long long total = __ldg(a.qoffsets + a.q);
     if (total < 0 || total > a.word_cap) {
         if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
@@ -452,19 +457,23 @@ __global__ void __launch_bounds__(kPlanThreads) PlanRowsKernel(const StreamArgs 
         const bool known = term >= 0 && term < a.vocab;
         if (blockIdx.y == 0 && tid == 0) {
             float seed = 0.0f;
-            int drow = -1;
+            int drow = -1, dr = -2;
             if (known) {
-                // the word's query: the last q with qoffsets[q] <= w (a malformed batch is flagged by
-                // the search kernel and fails as a whole)
-                int lo = 0, hi = a.q - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (__ldg(a.qoffsets + mid) <= w)
-                        lo = mid;
-                    else
-                        hi = mid - 1;
+                dr = a.dir_row ? __ldg(a.dir_row + term) : -1;
+                int k = a.k;
+                if (a.kq) {
+                    // a K per query: the word's query is the last q with qoffsets[q] <= w (a malformed
+                    // batch is flagged by the search kernel and fails as a whole)
+                    int lo = 0, hi = a.q - 1;
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (__ldg(a.qoffsets + mid) <= w)
+                            lo = mid;
+                        else
+                            hi = mid - 1;
+                    }
+                    k = QueryK(a, lo);
                 }
-                const int k = QueryK(a, lo);
                 if (a.term_top && k <= kTermTopK)
                     seed = __ldg(a.term_top + (long long)term * kTermTopK + (k - 1));
                 else if (a.term_rank && k <= 1024)
@@ -474,7 +483,7 @@ __global__ void __launch_bounds__(kPlanThreads) PlanRowsKernel(const StreamArgs 
             } else if (term < 0) {
                 atomicOr(a.status, kStatusBadWord);
             }
-            a.word_rec[w] = make_int2(__float_as_int(seed), drow);
+            a.word_rec[w] = make_int4(__float_as_int(seed), drow, dr, 0);
         }
         if (!known) {  // no postings
             for (int t = e0 + tid; t < e1; t += kPlanThreads)
