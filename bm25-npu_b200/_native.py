@@ -173,6 +173,23 @@ def engine_library():
     return _engine
 
 
+_hostcall = None
+
+
+def hostcall():
+    """The host-buffer Search entry points over the buffer protocol (_hostcall, built beside the
+    engine), or ImportError."""
+    global _hostcall
+    if _hostcall is None:
+        engine_library()  # the engine first, from this package
+        import importlib
+        try:
+            _hostcall = importlib.import_module(__package__ + '._hostcall')
+        except ImportError as e:
+            raise ImportError(f'BM25 host call module not built in {PACKAGE} (run bm25-npu_b200/build.py): {e}')
+    return _hostcall
+
+
 _synth = None
 
 

@@ -3,6 +3,7 @@
   libbm25_b200.so   CUDA engine + C ABI (nvcc, sm_100a only)
   libbm25_synth.so  seeded synthetic corpus -> resident-index arrays (gcc + OpenMP)
   libbm25_facade.so C++ SDK facade (include/AscendIndexBm25.h) over the C ABI (g++)
+  _hostcall*.so     Python entry points of the host-buffer Searches over the C ABI (gcc, CPython C API)
 
 Run as ``python bm25-npu_b200/build.py`` or through ``__graft_entry__.build()``.
 """
@@ -86,8 +87,23 @@ def build_runner(force=False):
     return target
 
 
+def build_hostcall(force=False):
+    """_hostcall: the Python entry points of the host-buffer Searches (csrc/hostcall.c, CPython C API)."""
+    import sysconfig
+    target = PACKAGE / ('_hostcall' + sysconfig.get_config_var('EXT_SUFFIX'))
+    src = CSRC / 'hostcall.c'
+    engine = build_engine(force)
+    deps = [src, INCLUDE / 'bm25_b200.h', engine, Path(__file__)]
+    if not force and not _stale(target, deps):
+        return target
+    _run(['gcc', '-O2', '-std=c11', '-fPIC', '-shared', '-Wall', '-I', sysconfig.get_paths()['include'], '-I', INCLUDE,
+          '-o', target, src, '-L', PACKAGE, '-lbm25_b200', "-Wl,-rpath,$ORIGIN"])
+    return target
+
+
 def build_all(force=False):
-    return build_engine(force), build_synth(force), build_facade(force), build_runner(force)
+    return (build_engine(force), build_synth(force), build_facade(force), build_runner(force),
+            build_hostcall(force))
 
 
 if __name__ == '__main__':

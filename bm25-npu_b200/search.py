@@ -109,7 +109,9 @@ class Bm25Session:
 
     def __init__(self, handle, num_docs, max_k):
         self._lib = n.engine_library()
+        self._call = n.hostcall()
         self._handle = handle
+        self._handle_int = (handle.value if isinstance(handle, c_void_p) else handle) or 0
         self.num_docs = num_docs
         self.max_k = max_k
 
@@ -176,11 +178,10 @@ class Bm25Session:
             scores, ids = out
         if words.size == 0:
             words = np.zeros(1, dtype=np.int32)
-        if not (scores.flags.c_contiguous and ids.flags.c_contiguous and scores.dtype == np.float32
-                and ids.dtype == np.int32 and scores.size >= q * k and ids.size >= q * k):
-            raise InvalidParam(n.BM25_ERR_INVALID_PARAM, 'out must be C-contiguous float32 and int32 arrays of q*k')
-        status = self._lib.bm25_search(self._handle, offsets.ctypes.data, words.ctypes.data, q, k,
-                                       scores.ctypes.data, ids.ctypes.data)
+        try:  # type and length checks of the arrays, then bm25_search with the GIL released
+            status = self._call.search(self._handle_int, offsets, words, q, k, scores, ids)
+        except ValueError as e:
+            raise InvalidParam(n.BM25_ERR_INVALID_PARAM, str(e)) from None
         if status:
             _raise(self._lib, status, self._handle)
         return scores, ids
@@ -279,8 +280,10 @@ class Bm25Session:
         scores, ids, exact = _outputs(q, k, out)
         if words.size == 0:
             words = np.zeros(1, dtype=np.int32)
-        status = self._lib.bm25_search_learned(self._handle, offsets.ctypes.data, words.ctypes.data, q, k,
-                                               scores.ctypes.data, ids.ctypes.data, exact.ctypes.data)
+        try:
+            status = self._call.search_learned(self._handle_int, offsets, words, q, k, scores, ids, exact)
+        except ValueError as e:
+            raise InvalidParam(n.BM25_ERR_INVALID_PARAM, str(e)) from None
         if status:
             _raise(self._lib, status, self._handle)
         return scores, ids, exact
@@ -372,6 +375,7 @@ class Bm25Session:
             _raise(self._lib, self._lib.bm25_close(self._handle), self._handle)
             self._lib.bm25_destroy(self._handle)
             self._handle = None
+            self._handle_int = 0  # a later call reaches the ABI with no handle: ILLEGAL_OPERATION
 
     def __enter__(self):
         return self
