@@ -79,6 +79,8 @@ __global__ void __launch_bounds__(kWtThreads, 3) BlockTileKernel(const StreamArg
     AllowDependents();
     WaitPrerequisites();  // the work list of the block bound kernel
     const unsigned count = (unsigned)min((long long)__ldcg(a.item_count), a.item_cap);
+    if (count == 0)
+        return;  // no item (an empty retry list), the same for every warp: the counter is left untouched
     unsigned bad = 0;
     unsigned long long read = 0;
 

@@ -227,6 +227,8 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
     AllowDependents();    // the final select may be placed as this kernel's CTAs retire
     WaitPrerequisites();  // plan rows (and a retry pass's fail list) of the kernels before this one
     const unsigned nq = !kLean && a.retry ? __ldcg(a.fail_in_count) : (unsigned)a.q;
+    if (nq == 0)
+        return;  // an empty retry list, the same for every warp: the work counter is left untouched
     const unsigned bulk = (unsigned)min(a.wt_bulk, a.tiles / kC);
     const unsigned claims_bulk = nq * bulk;
     const unsigned claims = claims_bulk + nq * (unsigned)(a.tiles - (int)bulk * kC);
