@@ -166,15 +166,10 @@ __global__ void __launch_bounds__(kWtThreads, 3) BlockTileKernel(const StreamArg
     if (lane == 0) {
         if (bad)
             atomicOr(a.status, bad);
-        if (a.stats && read)
-            atomicAdd(a.stats + kStatPostingsRead, read);
-        // the last warp to run dry resets the work counter for the next pass
-        const unsigned d = atomicAdd(&a.ctrl->done, 1u);
-        if (d == gridDim.x * kWtWarps - 1) {
-            a.ctrl->next = 0u;
-            a.ctrl->done = 0u;
-        }
+        sh.counters[warp][0] = sh.counters[warp][1] = 0u;
+        sh.counters[warp][2] = (unsigned)read;
     }
+    WtRetire(a, sh, kStatPostingsRead);
 }
 
 } // namespace bm25k

@@ -208,6 +208,37 @@ __device__ __forceinline__ void WtDenseAdd(const StreamArgs &a, int drow, int ba
     }
 }
 
+// End of a warp-tile style kernel: the CTA's counters (claims, tiles, postings: statistic stat2)
+// go to the Search's statistics and the CTA counts itself done, one thread for the CTA (the warps
+// all finish at about the same time, and per-warp atomics on these few addresses would queue up
+// behind one another at the launch's end); the last CTA to finish resets the work counter for the
+// next pass.
+__device__ __forceinline__ void WtRetire(const StreamArgs &a, WtShared &sh, int stat2 = kStatPostingsCopied)
+{
+    __syncthreads();  // every warp has taken its last claim and written its counters
+    if (threadIdx.x != 0)
+        return;
+    unsigned long long c[3] = {0ull, 0ull, 0ull};
+#pragma unroll
+    for (int w = 0; w < kWtWarps; ++w)
+#pragma unroll
+        for (int x = 0; x < 3; ++x)
+            c[x] += sh.counters[w][x];
+    if (a.stats) {
+        if (c[0])
+            atomicAdd(a.stats + kStatClaims, c[0]);
+        if (c[1])
+            atomicAdd(a.stats + kStatTilesScanned, c[1]);
+        if (c[2])
+            atomicAdd(a.stats + stat2, c[2]);
+    }
+    const unsigned d = atomicAdd(&a.ctrl->done, 1u);
+    if (d == gridDim.x - 1) {
+        a.ctrl->next = 0u;
+        a.ctrl->done = 0u;
+    }
+}
+
 // kC: tiles per claim.  kLean: the plain first pass with one K <= 32 for every query.
 template <int kC, bool kLean>
 __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs a)
@@ -391,21 +422,9 @@ __global__ void __launch_bounds__(kWtThreads, 3) WarpTileKernel(const StreamArgs
     }
 
     bad = __reduce_or_sync(kFull, bad);
-    if (lane == 0) {
-        if (bad)
-            atomicOr(a.status, bad);
-        if (a.stats && sh.counters[warp][0]) {
-            atomicAdd(a.stats + kStatClaims, (unsigned long long)sh.counters[warp][0]);
-            atomicAdd(a.stats + kStatTilesScanned, (unsigned long long)sh.counters[warp][1]);
-            atomicAdd(a.stats + kStatPostingsCopied, (unsigned long long)sh.counters[warp][2]);
-        }
-        // the last warp to run dry resets the work counter for the next pass
-        const unsigned d = atomicAdd(&a.ctrl->done, 1u);
-        if (d == gridDim.x * kWtWarps - 1) {
-            a.ctrl->next = 0u;
-            a.ctrl->done = 0u;
-        }
-    }
+    if (lane == 0 && bad)
+        atomicOr(a.status, bad);
+    WtRetire(a, sh);
 }
 
 template <int kC>
