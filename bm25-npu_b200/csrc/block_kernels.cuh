@@ -34,10 +34,13 @@ constexpr int kBsWarps = 8;
 constexpr int kBsThreads = kBsWarps * 32;
 constexpr int kBbThreads = 128;
 
-// Block offsets and maxima of directory row r in tile t (thread per (row, tile)).
+// Block offsets and maxima of directory row r in tile t (thread per (row, tile)).  A maximum is
+// stored rounded up to FP16 (never below the FP32 value: still a bound, half the bytes the block
+// bound kernel reads per (word, tile)); a maximum past FP16's range becomes +inf, which keeps the
+// block.
 __global__ void BuildBlockIndexKernel(const long long *indptr, const int *indices, const float *data,
                                       const int *dir_terms, const int *dir, long long rows, int tiles, long long stride,
-                                      int tile_docs, unsigned short *boff, float *bmax)
+                                      int tile_docs, unsigned short *boff, __half *bmax)
 {
     const int nb = tile_docs / kBlockDocs;
     const long long total = rows * (long long)tiles;
@@ -49,24 +52,24 @@ __global__ void BuildBlockIndexKernel(const long long *indptr, const int *indice
         const int *d = dir + r * stride;
         const long long b = s + d[t], e = s + d[t + 1];
         unsigned short *o = boff + i * nb;
-        float *m = bmax + i * nb;
+        __half *m = bmax + i * nb;
         int blk = 0;
         float mx = 0.0f;
         o[0] = 0;
         for (long long p = b; p < e; ++p) {
             const int bi = min(nb - 1, max(0, (indices[p] - t * tile_docs) / kBlockDocs));
             while (blk < bi) {
-                m[blk] = mx;
+                m[blk] = __float2half_ru(mx);
                 mx = 0.0f;
                 ++blk;
                 o[blk] = (unsigned short)(p - b);
             }
             mx = fmaxf(mx, data[p]);  // fmaxf(0, negative) = 0: a negative score is bounded by 0
         }
-        m[blk] = mx;
+        m[blk] = __float2half_ru(mx);
         for (int j = blk + 1; j < nb; ++j) {
             o[j] = (unsigned short)(e - b);
-            m[j] = 0.0f;
+            m[j] = __float2half(0.0f);
         }
     }
 }
@@ -136,16 +139,18 @@ __global__ void __launch_bounds__(kBbThreads) BlockBoundKernel(const StreamArgs 
 #pragma unroll
                 for (int j = 0; j < kNb; ++j)
                     m[u][j] = 0.0f;
-                if (r[u] >= 0 && pe[u].b < pe[u].e) {
-                    const float4 *src =
-                        reinterpret_cast<const float4 *>(a.bmax + ((long long)r[u] * a.tiles + t) * kNb);
+                if (r[u] >= 0 && pe[u].b < pe[u].e) {  // 8 FP16 maxima per 16-byte load
+                    const uint4 *src =
+                        reinterpret_cast<const uint4 *>(a.bmax + ((long long)r[u] * a.tiles + t) * kNb);
 #pragma unroll
-                    for (int j = 0; j < kNb / 4; ++j) {
-                        const float4 v = __ldg(src + j);
-                        m[u][4 * j] = v.x;
-                        m[u][4 * j + 1] = v.y;
-                        m[u][4 * j + 2] = v.z;
-                        m[u][4 * j + 3] = v.w;
+                    for (int j = 0; j < kNb / 8; ++j) {
+                        const uint4 v = __ldg(src + j);
+                        const unsigned h[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                        for (int x = 0; x < 4; ++x) {  // the lower half of each word is the earlier block
+                            m[u][8 * j + 2 * x] = __half2float(__ushort_as_half((unsigned short)(h[x] & 0xffffu)));
+                            m[u][8 * j + 2 * x + 1] = __half2float(__ushort_as_half((unsigned short)(h[x] >> 16)));
+                        }
                     }
                 }
             }

@@ -952,7 +952,7 @@ class Engine {
                 // 128-document block index of the directory rows: offsets (uint16) and maxima
                 const size_t cells = (size_t)rows * tiles * (plan_.tile_docs / bm25k::kBlockDocs);
                 d_boff_ = static_cast<unsigned short *>(Alloc(cells * sizeof(unsigned short), "cudaMalloc block offsets"));
-                d_bmax_ = static_cast<float *>(Alloc(cells * sizeof(float), "cudaMalloc block maxima"));
+                d_bmax_ = static_cast<__half *>(Alloc(cells * sizeof(__half), "cudaMalloc block maxima"));
                 const long long pairs = rows * (long long)tiles;
                 bm25k::BuildBlockIndexKernel<<<(int)std::min<long long>((pairs + 255) / 256, 148 * 64), 256, 0,
                                                stream_>>>((const long long *)d_indptr_, d_indices_, d_data_, d_terms,
@@ -1646,7 +1646,7 @@ class Engine {
     size_t word_offset_ = 0, tau_offset_ = 0, ks_offset_ = 0, kout_offset_ = 0, in_bytes_ = 0, out_bytes_ = 0,
            smem_bytes_ = 0;
     unsigned short *d_boff_ = nullptr;
-    float *d_bmax_ = nullptr;
+    __half *d_bmax_ = nullptr;
     uint4 *d_items_ = nullptr;
     int *d_wrow_ = nullptr;
     float *d_safe_ = nullptr;

@@ -46,6 +46,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cuda_fp16.h>
 
 namespace bm25k {
 
@@ -121,7 +122,9 @@ struct StreamArgs {
     unsigned *status;
     // pruned Search (block kernels): nullptr on the plain path
     const unsigned short *boff;  // [dir row][tile][block] posting offset of the block from the tile's start
-    const float *bmax;           // [dir row][tile][block] largest posting score of the row's term in the block
+    // [dir row][tile][block] largest posting score of the row's term in the block, rounded up to FP16
+    // (a larger value is still a bound: rounded FP32 addition is monotone)
+    const __half *bmax;
     const float *tau;            // [Q] starting bound guesses
     const float *safe;           // [Q] safe bounds (learned Searches; a retry's bound), or nullptr
     int *exact;                  // [Q] 1 where K candidates reached tau

@@ -23,9 +23,25 @@ def block_bounds(indptr, indices, data, words, block_docs, blocks):
     return out
 
 
+def round_up_fp16(x):
+    """x rounded up to FP16 (as the engine stores its block maxima), back in FP32."""
+    h = np.asarray(x, np.float32).astype(np.float16)
+    low = h.astype(np.float32) < x
+    h[low] = np.nextafter(h[low], np.float16(np.inf))
+    return h.astype(np.float32)
+
+
+def test_round_up_fp16_never_lowers():
+    x = np.random.default_rng(3).random(10_000, dtype=np.float32) * np.float32(40.0)
+    r = round_up_fp16(x)
+    assert np.all(r >= x) and np.all(r <= x * np.float32(1.001))
+
+
 @pytest.mark.parametrize('block_docs', [128, 1024])
-def test_block_bound_covers_every_document(pkg, oracle_mod, block_docs):
-    """FP32 sums of per-block maxima in query-word order bound every document's FP32 sum in the block."""
+@pytest.mark.parametrize('stored', ['fp32', 'fp16_up'])
+def test_block_bound_covers_every_document(pkg, oracle_mod, block_docs, stored):
+    """FP32 sums of per-block maxima in query-word order bound every document's FP32 sum in the block,
+    with the maxima in FP32 or rounded up to FP16 (the engine's block index)."""
     spec = pkg.CorpusSpec(docs=20_000, vocab=3_000, seed=5, k1=1.2)
     index = pkg.synthetic_index(spec)
     data = oracle_mod.contributions(index, spec.k1)
@@ -35,6 +51,8 @@ def test_block_bound_covers_every_document(pkg, oracle_mod, block_docs):
     blocks = (index.num_docs + block_docs - 1) // block_docs
     for q in range(len(rows)):
         wb = block_bounds(index.offsets, index.docs, data, words[offsets[q]:offsets[q + 1]], block_docs, blocks)
+        if stored == 'fp16_up':
+            wb = round_up_fp16(wb)
         bound = np.zeros(blocks, dtype=np.float32)
         for b in wb:  # query-word order, FP32 rounding at every step
             bound = (bound + b).astype(np.float32)
