@@ -140,3 +140,23 @@ def test_batch_with_k_per_query(pkg, oracle_mod, corpus, cuda_ok):
             assert s.device_status() == 0
             assert_same_topk(d_s.cpu().numpy()[None], d_i.cpu().numpy()[None], want_s[None], want_i[None],
                              f'batch device learned={learned}')
+
+
+@pytest.mark.gpu
+def test_tune_batch_with_k_per_query_learned(pkg, oracle_mod, corpus, cuda_ok):
+    """The live-session tuner on a learned batch with a K per query (as the benchmark tunes the routing
+    cut): every cut answers the same bits, the fastest is kept, and the session still answers the
+    oracle's rows afterwards."""
+    index, data = corpus
+    offsets, words = _queries(index, 11, 41)
+    q = offsets.size - 1
+    ks = np.random.default_rng(9).choice([10, 100, 1000], q).astype(np.int32)
+    want_s, want_i = _by_k(oracle_mod, index, data, offsets, words, ks)
+    with pkg.Bm25Session.from_csc(index.offsets, index.docs, data, index.num_docs, query_capacity=64,
+                                  word_capacity=1024, max_k=1000, prune=True) as s:
+        s.set_threshold_model(pkg.learned.ThresholdModel(pkg.learned.init_params(1, 3.0), -1.0))
+        best, table = pkg.autotune.tune(s, (offsets, words), int(ks.max()), space={'prune_route': (0.2, 1.0)},
+                                        learned=True, ks=ks, reps=2)
+        assert len(table) == 2 and best['prune_route'] in (0.2, 1.0) and s.tuning()['prune_route'] == best['prune_route']
+        got_s, got_i, _, _ = s.search_batch((offsets, words), ks, learned=True)
+        assert_same_topk(got_s[None], got_i[None], want_s[None], want_i[None], 'tuned learned batch')
