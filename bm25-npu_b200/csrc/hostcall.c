@@ -10,6 +10,7 @@
  */
 #define PY_SSIZE_T_CLEAN
 #include <Python.h>
+#include <stdint.h>
 #include <string.h>
 
 #include "bm25_b200.h"
@@ -73,8 +74,8 @@ static PyObject *Search(PyObject *self, PyObject *args)
     (void)self;
     if (!PyArg_ParseTuple(args, "KOOnnOO", &handle, &offsets, &words, &q, &k, &scores, &ids))
         return NULL;
-    if (k < 1) {
-        PyErr_SetString(PyExc_ValueError, "k must be positive");
+    if (k < 1 || k > INT32_MAX || q > INT32_MAX) {
+        PyErr_SetString(PyExc_ValueError, "k must be in [1, 2^31) and q below 2^31");
         return NULL;
     }
     Py_buffer ob, wb, sb, ib;
@@ -111,8 +112,8 @@ static PyObject *SearchLearned(PyObject *self, PyObject *args)
     (void)self;
     if (!PyArg_ParseTuple(args, "KOOnnOOO", &handle, &offsets, &words, &q, &k, &scores, &ids, &exact))
         return NULL;
-    if (k < 1) {
-        PyErr_SetString(PyExc_ValueError, "k must be positive");
+    if (k < 1 || k > INT32_MAX || q > INT32_MAX) {
+        PyErr_SetString(PyExc_ValueError, "k must be in [1, 2^31) and q below 2^31");
         return NULL;
     }
     Py_buffer ob, wb, sb, ib, eb;
