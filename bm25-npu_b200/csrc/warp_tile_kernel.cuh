@@ -476,25 +476,21 @@ __global__ void __launch_bounds__(kPlanThreads) PlanRowsKernel(const StreamArgs 
         const int term = __ldg(a.words + w);
         int *out = a.plan_rows + w * a.dir_stride;
         const bool known = term >= 0 && term < a.vocab;
+        // a K per query: the word's query is the number of q in [1, Q] with qoffsets[q] <= w (the last
+        // query starting at or before w), counted by the whole CTA at once (a malformed batch is
+        // flagged by the search kernel and fails as a whole)
+        int wq = 0;
+        if (a.kq && blockIdx.y == 0) {  // uniform
+            for (int base = 1; base <= a.q; base += kPlanThreads)
+                wq += __syncthreads_count(base + tid <= a.q && __ldg(a.qoffsets + base + tid) <= w);
+            wq = min(wq, a.q - 1);
+        }
         if (blockIdx.y == 0 && tid == 0) {
             float seed = 0.0f;
             int drow = -1, dr = -2;
             if (known) {
                 dr = a.dir_row ? __ldg(a.dir_row + term) : -1;
-                int k = a.k;
-                if (a.kq) {
-                    // a K per query: the word's query is the last q with qoffsets[q] <= w (a malformed
-                    // batch is flagged by the search kernel and fails as a whole)
-                    int lo = 0, hi = a.q - 1;
-                    while (lo < hi) {
-                        const int mid = (lo + hi + 1) >> 1;
-                        if (__ldg(a.qoffsets + mid) <= w)
-                            lo = mid;
-                        else
-                            hi = mid - 1;
-                    }
-                    k = QueryK(a, lo);
-                }
+                const int k = a.kq ? QueryK(a, wq) : a.k;
                 if (a.term_top && k <= kTermTopK)
                     seed = __ldg(a.term_top + (long long)term * kTermTopK + (k - 1));
                 else if (a.term_rank && k <= 1024)
