@@ -21,6 +21,13 @@ frequency, K = 10; two batches A/B alternate as in the reference's benchmark.
           K-th scores), then timed as above (device-resident and through
           bm25_search_learned), beside the safe bounds alone; every result checked
           bit for bit against the oracle.
+  tuning  before the timed region, the session's runtime knobs (warp-tile claim
+          size and tail claims) are timed on a sample batch of its own seed and
+          the fastest kept (autotune.tune; every setting bit-checked against the
+          first); the mix and block-max legs tune their learned routing cut the
+          same way.  --no-tune keeps the defaults of the plain leg.
+  batched_mix, blockmax_c4, reference_shape, serving, cpu_baseline_bm25s: the
+          C3, C4, reference-shaped, C5 and bm25s legs (see their functions).
 
 --impl reference times the reference's own CPU search (oracle/_ref, compiled from
 the reference's sources; the oracle's C restatement where that was not built) on
