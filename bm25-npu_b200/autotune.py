@@ -150,18 +150,27 @@ def tune(session, queries, k, *, space=None, learned=False, ks=None, reps=10, wa
     flush = torch.empty(64 << 20, dtype=torch.float32, device=f'cuda:{torch.cuda.current_device()}')
     offsets, words = (np.asarray(queries[0], np.int64), np.asarray(queries[1], np.int32))
     table, ref = [], None
-    for changes in combos:
-        try:
-            session.set_tuning(**{**start, **changes})
-        except InvalidParam:
-            continue  # e.g. a ring too deep for one SM's shared memory
-        ms, scores, ids = _time(session, (offsets, words), k, reps, warmup, flush, learned, ks)
-        if ref is None:
-            ref = (scores, ids)
-        elif not (np.array_equal(ids, ref[1]) and np.array_equal(scores.view(np.uint32), ref[0].view(np.uint32))):
-            session.set_tuning(**start)
-            raise RuntimeError(f'tuning {changes} changed the results')
-        table.append((changes, ms))
-    best = {**start, **min(table, key=lambda row: row[1])[0]} if table else start
-    session.set_tuning(**(best if keep else start))
+    done = False
+    try:
+        for changes in combos:
+            try:
+                session.set_tuning(**{**start, **changes})
+            except InvalidParam:
+                continue  # e.g. a ring too deep for one SM's shared memory
+            ms, scores, ids = _time(session, (offsets, words), k, reps, warmup, flush, learned, ks)
+            if ref is None:
+                ref = (scores, ids)
+            elif not (np.array_equal(ids, ref[1]) and np.array_equal(scores.view(np.uint32),
+                                                                     ref[0].view(np.uint32))):
+                raise RuntimeError(f'tuning {changes} changed the results')
+            table.append((changes, ms))
+        best = {**start, **min(table, key=lambda row: row[1])[0]} if table else start
+        session.set_tuning(**(best if keep else start))
+        done = True
+    finally:
+        if not done:  # a failed run leaves the session as it found it (when it is still usable)
+            try:
+                session.set_tuning(**start)
+            except Exception:
+                pass
     return best, table
