@@ -19,9 +19,9 @@
 // below tau, which the running bound never falls under: it is never selected, and its row
 // entries are cleared with the block.  The result is the same as BlockScoreKernel's, which
 // stages only the kept blocks' postings in shared memory with 4-byte asynchronous copies
-// and pays one exposed memory latency per item; here a typical item waits for memory once
-// for its ranges and once for its postings, and the ranges of the next item are not
-// needed before its postings.
+// and pays one exposed memory latency per item on top of its metadata; here an item waits
+// for its ranges, then for its postings about once per group of words, and a long run reads
+// its first window with the rest of its group.
 #pragma once
 #include "block_kernels.cuh"
 #include "warp_tile_kernel.cuh"
