@@ -450,21 +450,23 @@ class Engine {
             Cuda(cudaGraphLaunch(exec, stream_), "cudaGraphLaunch");
             ++replays_;
             unsigned char *ho = static_cast<unsigned char *>(h_out_);
-            Cuda(cudaMemcpyAsync(ho, d_out_, total * sizeof(float), cudaMemcpyDeviceToHost, stream_), "D2H");
+            // the status word and the scores in one copy, then the ids (and the flags)
+            Cuda(cudaMemcpyAsync(ho, d_out_, kScoreOffset + total * sizeof(float), cudaMemcpyDeviceToHost, stream_),
+                 "D2H");
             const size_t ids = IdOffset(qb, kmax);
             Cuda(cudaMemcpyAsync(ho + ids, d_out_ + ids, total * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_),
                  "D2H");
-            const size_t st = StatusOffset(qb, kmax);
-            Cuda(cudaMemcpyAsync(ho + st, d_out_ + st, 32 + (learned ? (size_t)q * 4 : 0), cudaMemcpyDeviceToHost,
-                                 stream_),
-                 "D2H");
+            if (learned) {
+                const size_t ex = ExactOffset(qb, kmax);
+                Cuda(cudaMemcpyAsync(ho + ex, d_out_ + ex, (size_t)q * 4, cudaMemcpyDeviceToHost, stream_), "D2H");
+            }
             Cuda(cudaEventRecord(done_, stream_), "cudaEventRecord");
             Cuda(cudaStreamSynchronize(stream_), "complete batch Search through result D2H");
             unsigned status = 0;
-            std::memcpy(&status, ho + st, sizeof(unsigned));
+            std::memcpy(&status, ho, sizeof(unsigned));
             if (status)
                 throw DeviceError(0, "Device reported invalid Search state, status=" + std::to_string(status));
-            const float *scores = reinterpret_cast<const float *>(ho);
+            const float *scores = reinterpret_cast<const float *>(ho + kScoreOffset);
             const int32_t *idv = reinterpret_cast<const int32_t *>(ho + ids);
             for (int64_t i = 0; i < q; ++i)
                 for (int64_t r = kout[i]; r < kout[i] + ks[i]; ++r) {
@@ -1021,6 +1023,7 @@ class Engine {
         std::memset(h_in_, 0, in_bytes_);
         d_in_ = static_cast<unsigned char *>(Alloc(in_bytes_, "cudaMalloc input arena"));
         d_out_ = static_cast<unsigned char *>(Alloc(out_bytes_, "cudaMalloc output arena"));
+        Cuda(cudaMemset(d_out_, 0, out_bytes_), "cudaMemset output arena");  // the status word starts 0
         d_dev_status_ = static_cast<unsigned *>(Alloc(sizeof(unsigned), "cudaMalloc status"));
         Cuda(cudaMemset(d_dev_status_, 0, sizeof(unsigned)), "cudaMemset");
         d_inject_ = static_cast<unsigned *>(Alloc(sizeof(unsigned), "cudaMalloc inject word"));
@@ -1480,9 +1483,12 @@ class Engine {
         Cuda(cudaGetLastError(), "search kernel launch");
     }
 
-    size_t IdOffset(int q, int k) const { return Align32((size_t)q * k * 4); }
-    size_t StatusOffset(int q, int k) const { return Align32(IdOffset(q, k) + (size_t)q * k * 4); }
-    size_t ExactOffset(int q, int k) const { return StatusOffset(q, k) + 32; }
+    // Output arena: the status word first (32 bytes, at the same place for every graph), then the
+    // scores, the ids and the exactness flags.  A Search that succeeds leaves the status 0 (any bit
+    // fails the Search and poisons the session), so no graph has to clear it before its kernels.
+    static constexpr size_t kScoreOffset = 32;
+    size_t IdOffset(int q, int k) const { return kScoreOffset + Align32((size_t)q * k * 4); }
+    size_t ExactOffset(int q, int k) const { return IdOffset(q, k) + Align32((size_t)q * k * 4); }
 
     void MarkKernel(int which, cudaStream_t s)
     {
@@ -1531,10 +1537,10 @@ class Engine {
                                        : (mode == kModePruned ? tau_offset_ + (size_t)q * sizeof(float) : tau_offset_),
                                  cudaMemcpyHostToDevice, stream_),
                  "query H2D");
-            unsigned *status = reinterpret_cast<unsigned *>(d_out_ + StatusOffset(q, k));
-            Cuda(cudaMemsetAsync(status, 0, sizeof(unsigned), stream_), "status reset");
+            unsigned *status = reinterpret_cast<unsigned *>(d_out_);  // 0 unless a Search failed
             Launch(q, k, reinterpret_cast<const int64_t *>(d_in_), reinterpret_cast<const int32_t *>(d_in_ + word_offset_),
-                   reinterpret_cast<float *>(d_out_), reinterpret_cast<int32_t *>(d_out_ + IdOffset(q, k)), status,
+                   reinterpret_cast<float *>(d_out_ + kScoreOffset), reinterpret_cast<int32_t *>(d_out_ + IdOffset(q, k)),
+                   status,
                    stream_,
                    mode == kModePruned ? reinterpret_cast<const float *>(d_in_ + tau_offset_)
                                        : (mode == kModeLearned ? d_tau_ : nullptr),
@@ -1543,7 +1549,7 @@ class Engine {
                    mixed ? reinterpret_cast<const int64_t *>(d_in_ + kout_offset_) : nullptr);
             if (!mixed)  // a batch's result size varies per call: copied after the replay
                 Cuda(cudaMemcpyAsync(h_out_, d_out_,
-                                     pruned ? ExactOffset(q, k) + (size_t)q * 4 : StatusOffset(q, k) + 32,
+                                     pruned ? ExactOffset(q, k) + (size_t)q * 4 : ExactOffset(q, k),
                                      cudaMemcpyDeviceToHost, stream_),
                      "top-K D2H");
         } catch (...) {
@@ -1587,10 +1593,10 @@ class Engine {
     {
         const unsigned char *base = static_cast<const unsigned char *>(h_out_);
         unsigned status = 0;
-        std::memcpy(&status, base + StatusOffset((int)q, k), sizeof(unsigned));
+        std::memcpy(&status, base, sizeof(unsigned));
         if (status)
             throw DeviceError(0, "Device reported invalid Search state, status=" + std::to_string(status));
-        const float *scores = reinterpret_cast<const float *>(base);
+        const float *scores = reinterpret_cast<const float *>(base + kScoreOffset);
         const int32_t *ids = reinterpret_cast<const int32_t *>(base + IdOffset((int)q, k));
         const size_t n = (size_t)q * k;
         for (size_t i = 0; i < n; ++i) {
