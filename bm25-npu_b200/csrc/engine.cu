@@ -1304,11 +1304,11 @@ class Engine {
             }
             // A warp-tile session runs the warp-tile kernel for plain Searches of one K <= 32 and for
             // every pass that streams from a bound already set (the routed queries of a pruned Search,
-            // from their learned bound; retry passes, from their proven one); it needs the plan rows of
-            // the words without a directory row.  The first pass of a pruned Search is block-scored and
-            // that of a batch with a K per query or K > 32 runs the tile-group kernel (no starting bound
-            // from the term statistics there: the warp-tile kernel's wider first wave of claims would
-            // append far more candidates); both take the (query word, tile) plan.
+            // from their learned bound; retry passes, from their proven one), all on the plan rows of
+            // the Search's words.  The first pass of a pruned Search is block-scored (block-tile
+            // kernel, also on the plan rows); that of a batch with a K per query or K > 32 runs the
+            // tile-group kernel on the (query word, tile) plan (the warp-tile kernel's wider first
+            // wave of claims would append far more candidates there).
             const bool wt_session = plan_.kernel == BM25_KERNEL_WARP_TILE;
             const bool warp_tile = wt_session && !tau && !kq && k <= bm25k::kMaxSmallK;
             // the streaming passes after a first pass (retries, routed queries) run the warp-tile kernel
